@@ -1,0 +1,284 @@
+/*
+ * psbx.h -- C-ABI of the B200 sparse Krylov library (libpsbx.so).
+ *
+ * The first part exports, with the same names, argument meaning and return
+ * codes, the C glue entry points that PSBLAS 3.9's Fortran GPU types bind to
+ * through iso_c_binding (psb_d_cuda_hlg_sparse_mat, psb_d_cuda_elg_sparse_mat,
+ * psb_d_cuda_csrg_sparse_mat, psb_d_vect_cuda, psb_cuda_env_mod).  Linking
+ * the unmodified Fortran modules against libpsbx.so in place of the
+ * reference's libpsb_cuda routes psb_spmm / psb_geaxpby / psb_gedot /
+ * psb_genrm2 to the kernels of this library.  Each declaration cites the
+ * reference interface it replaces (path within the psblas3 tree).
+ *
+ * The second part (psbx_*) adds entry points that have no one-to-one
+ * counterpart in the reference glue: the device-resident Krylov solver that a
+ * psb_krylov shim calls, the mixed-precision solver, the batched solver and
+ * device-side format builders.  Each says which reference routine it stands
+ * in for.
+ *
+ * Conventions (as in the reference): matrix and vector handles are opaque
+ * void*, owned by the caller and freed with the matching free routine; index
+ * arrays passed in are int32 with firstIndex (normally 1, Fortran); host
+ * arrays are borrowed for the duration of the call only; every call runs on
+ * the library's stream and returns after the host-visible result is ready.
+ * Return codes: 0 success, 1 unsupported / size mismatch, 2 unspecified CUDA
+ * error, 3 out of device memory, plus the solver codes below.
+ * The library is not thread-safe, like the reference's global handle.
+ */
+#ifndef PSBX_H
+#define PSBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status and element codes: cuda/spgpu/core.h:69-80 ------------------ */
+#define SPGPU_SUCCESS        0
+#define SPGPU_UNSUPPORTED    1
+#define SPGPU_UNSPECIFIED    2
+#define SPGPU_OUTOFMEMORY    3
+#define PSBX_TIMEOUT         4   /* a bounded device wait ran out           */
+#define PSBX_BREAKDOWN       5   /* Krylov breakdown (rho/sigma/omega == 0) */
+#define PSBX_NOT_CONVERGED   6   /* itmax reached above tolerance           */
+
+#define SPGPU_TYPE_INT            0
+#define SPGPU_TYPE_FLOAT          1
+#define SPGPU_TYPE_DOUBLE         2
+#define SPGPU_TYPE_COMPLEX_FLOAT  3
+#define SPGPU_TYPE_COMPLEX_DOUBLE 4
+
+/* ======================================================================== */
+/* Environment: cuda/psb_cuda_env_mod.F90:43-175, cuda/cuda_util.c:220-440   */
+/* ======================================================================== */
+int   gpuInit(int dev);                       /* cuda_util.c:220 */
+void  gpuClose(void);                         /* cuda_util.c:244 */
+int   setDevice(int dev);                     /* cuda_util.c:261 */
+int   getDevice(void);                        /* cuda_util.c:289 */
+int   getDeviceCount(void);                   /* cuda_util.c:366 */
+int   getDeviceHasUVA(void);                  /* cuda_util.c:296 */
+int   DeviceHasUVA(void);                     /* cuda_util.c:360 */
+int   getGPUMultiProcessors(void);            /* cuda_util.c:303 */
+int   getGPUMemoryBusWidth(void);             /* cuda_util.c:311 */
+int   getGPUMemoryClockRate(void);            /* cuda_util.c:319 */
+int   getGPUWarpSize(void);                   /* cuda_util.c:327 */
+int   getGPUMaxThreadsPerBlock(void);         /* cuda_util.c:333 */
+int   getGPUMaxThreadsPerMP(void);            /* cuda_util.c:339 */
+int   getGPUMaxRegistersPerBlock(void);       /* cuda_util.c:345 */
+void  cpyGPUNameString(char *cstring);        /* cuda_util.c:352 (>= 256 bytes) */
+void  cudaSync(void);                         /* cuda_util.c:377 */
+void  cudaReset(void);                        /* cuda_util.c:396 */
+void *psb_cudaGetHandle(void);                /* cuda_util.c:414 */
+void  psb_cudaCreateHandle(void);             /* cuda_util.c:419 */
+void  psb_cudaDestroyHandle(void);            /* cuda_util.c:426 */
+void *psb_cudaGetStream(void);                /* cuda_util.c:433 (cudaStream_t) */
+void  psb_cudaSetStream(void *stream);        /* cuda_util.c:438 */
+
+/* ======================================================================== */
+/* Dense multivectors: cuda/vectordev.h:76-86, cuda/dvectordev.h,            */
+/* Fortran side cuda/psb_base_vectordev_mod.F90, psb_d_vectordev_mod.F90     */
+/* Layout: count vectors of size elements, pitch = size when count == 1,     */
+/* else size rounded up to 256 bytes (vectordev.c:40-70).                    */
+/* ======================================================================== */
+int  FallocMultiVecDevice(void **deviceMultiVec, unsigned count,
+                          unsigned size, unsigned elementType);
+void freeMultiVecDevice(void *deviceVec);
+int  getMultiVecDeviceSize(void *deviceVec);
+int  getMultiVecDeviceCount(void *deviceVec);
+int  getMultiVecDevicePitch(void *deviceVec);
+int  writeMultiVecDeviceDouble(void *deviceVec, double *hostVec);
+int  writeMultiVecDeviceDoubleR2(void *deviceVec, double *hostVec, int ld);
+int  readMultiVecDeviceDouble(void *deviceVec, double *hostVec);
+int  readMultiVecDeviceDoubleR2(void *deviceVec, double *hostVec, int ld);
+int  writeMultiVecDeviceFloat(void *deviceVec, float *hostVec);
+int  readMultiVecDeviceFloat(void *deviceVec, float *hostVec);
+/* dvectordev.c:101-112: x(first:last) = val (indexBase-relative) */
+int  setscalMultiVecDeviceDouble(double val, int first, int last,
+                                 int indexBase, void *devVecX);
+/* dvectordev.c:189-198: x = alpha*x over the whole pitch*count */
+int  scalMultiVecDeviceDouble(double alpha, void *devVecA);
+/* dvectordev.c:200-236: reductions over the first n entries of each of the
+ * count vectors; y_res[count] on the host.  Deterministic order on device,
+ * no host-side partial sums. */
+int  nrm2MultiVecDeviceDouble(double *y_res, int n, void *devVecA);
+int  amaxMultiVecDeviceDouble(double *y_res, int n, void *devVecA);
+int  asumMultiVecDeviceDouble(double *y_res, int n, void *devVecA);
+int  dotMultiVecDeviceDouble(double *y_res, int n, void *devVecA, void *devVecB);
+/* dvectordev.c:238-255: y = alpha*x + beta*y (beta == 0: y not read) */
+int  axpbyMultiVecDeviceDouble(int n, double alpha, void *devVecX,
+                               double beta, void *devVecY);
+/* dvectordev.c:257-273: y = alpha*x + beta*y; z = gamma*y + delta*z */
+int  upd_xyzMultiVecDeviceDouble(int n, double alpha, double beta,
+                                 double gamma, double delta, void *devVecX,
+                                 void *devVecY, void *devVecZ);
+/* dvectordev.c:275-292 with the CPU semantics of psi_dxyzw
+ * (base/serial/psi_d_serial_impl.F90:1853-1855):
+ * y = a*x + b*y; z = c*y + d*z; w = e*z + f*w */
+int  xyzwMultiVecDeviceDouble(int n, double a, double b, double c, double d,
+                              double e, double f, void *devVecX, void *devVecY,
+                              void *devVecZ, void *devVecW);
+/* dvectordev.c:294-306: b = alpha*a.*b */
+int  axyMultiVecDeviceDouble(int n, double alpha, void *devVecA, void *devVecB);
+/* dvectordev.c:308-322: z = alpha*a.*b + beta*z (the diagonal prec apply) */
+int  axybzMultiVecDeviceDouble(int n, double alpha, void *devVecA,
+                               void *devVecB, double beta, void *devVecZ);
+/* dvectordev.c:324-345: b = alpha*|a| ; a = alpha*|a| */
+int  absMultiVecDeviceDouble2(int n, double alpha, void *devVecA, void *devVecB);
+int  absMultiVecDeviceDouble(int n, double alpha, void *devVecA);
+
+/* ======================================================================== */
+/* HLL (hacked ELLPACK): cuda/hlldev.h:96-153, cuda/hlldev_mod.F90:37-259    */
+/* Layout (ext/psb_d_hll_mat_mod.f90:38-104): rows in hacks of hksz; hack k  */
+/* stores ja/val column-major with leading dimension hksz starting at        */
+/* hkoffs[k]; irn[i] = stored entries of row i; idiag[i] = 1-based position  */
+/* of the diagonal in row i (0 if none).                                     */
+/* ======================================================================== */
+int  FallocHllDevice(void **deviceMat, unsigned hksize, unsigned rows,
+                     unsigned nzeros, unsigned allocsize, unsigned elementType,
+                     unsigned firstIndex);
+void freeHllDevice(void *deviceMat);
+int  getHllDeviceParams(void *deviceMat, int *hksize, int *rows, int *nzeros,
+                        int *allocsize, int *hackOffsLength, int *firstIndex,
+                        int *avgnzr);
+int  writeHllDeviceDouble(void *deviceMat, double *val, int *ja, int *hkoffs,
+                          int *irn, int *idiag);
+int  readHllDeviceDouble(void *deviceMat, double *val, int *ja, int *hkoffs,
+                         int *irn, int *idiag);
+int  writeHllDeviceFloat(void *deviceMat, float *val, int *ja, int *hkoffs,
+                         int *irn, int *idiag);
+int  readHllDeviceFloat(void *deviceMat, float *val, int *ja, int *hkoffs,
+                        int *irn, int *idiag);
+/* cuda/hlldev.c:420-462: row-sorted COO on the host (1-based), hack offsets
+ * and row lengths precomputed by the caller (psb_d_cuda_cp_hlg_from_coo.F90:
+ * 117-188), scattered into the HLL layout on the device.  Padding follows
+ * psi_cuda_CopyCooToHlg.cuh:59-64 (column of the first entry of row 2). */
+int  psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int noffs,
+                           int isz, int *irn, int *hoffs, int *idisp, int *ja,
+                           double *val, void *deviceMat);
+/* cuda/hlldev.c:185-207: y = alpha*A*x + beta*y (beta == 0: y not read) */
+int  spmvHllDeviceDouble(void *deviceMat, double alpha, void *deviceX,
+                         double beta, void *deviceY);
+int  spmvHllDeviceFloat(void *deviceMat, float alpha, void *deviceX,
+                        float beta, void *deviceY);
+
+/* ======================================================================== */
+/* ELL: cuda/elldev.h, cuda/elldev_mod.F90:37-313.  Device pitch = rows     */
+/* rounded up to 32 (cuda/spgpu/ell.c:33-37); host arrays are pitch x        */
+/* maxRowSize column-major (psb_d_cuda_elg_to_gpu.F90:60-90).                */
+/* ======================================================================== */
+int  FallocEllDevice(void **deviceMat, unsigned rows, unsigned maxRowSize,
+                     unsigned nnzeros, unsigned columns, unsigned elementType,
+                     unsigned firstIndex);
+void freeEllDevice(void *deviceMat);
+void zeroEllDevice(void *deviceMat);
+int  getEllDevicePitch(void *deviceMat);
+int  getEllDeviceMaxRowSize(void *deviceMat);
+int  writeEllDeviceDouble(void *deviceMat, double *val, int *ja, int ldj,
+                          int *irn, int *idiag);
+int  readEllDeviceDouble(void *deviceMat, double *val, int *ja, int ldj,
+                         int *irn, int *idiag);
+/* cuda/elldev.c (psiCopyCooToElgDouble) */
+int  psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ldv,
+                           int nzm, int *irn, int *idisp, int *ja, double *val,
+                           void *deviceMat);
+int  spmvEllDeviceDouble(void *deviceMat, double alpha, void *deviceX,
+                         double beta, void *deviceY);
+
+/* ======================================================================== */
+/* CSR (replaces the cuSPARSE-backed CSRG of cuda/d_cusparse_mod.F90:36-190; */
+/* the matrix handle is the interoperable struct d_Cmat {void *mat;}).       */
+/* ======================================================================== */
+typedef struct psbx_d_Cmat { void *mat; } psbx_d_Cmat;
+int d_CSRGDeviceAlloc(psbx_d_Cmat *Mat, int nr, int nc, int nz);
+int d_CSRGDeviceFree(psbx_d_Cmat *Mat);
+int d_CSRGDeviceGetParms(psbx_d_Cmat *Mat, int *nr, int *nc, int *nz);
+int d_CSRGDeviceSetMatType(psbx_d_Cmat *Mat, int type);
+int d_CSRGDeviceSetMatFillMode(psbx_d_Cmat *Mat, int type);
+int d_CSRGDeviceSetMatDiagType(psbx_d_Cmat *Mat, int type);
+int d_CSRGDeviceSetMatIndexBase(psbx_d_Cmat *Mat, int type); /* 0 or 1 */
+int d_CSRGHost2Device(psbx_d_Cmat *Mat, int m, int n, int nz, int *irp,
+                      int *ja, double *val);
+int d_CSRGDevice2Host(psbx_d_Cmat *Mat, int m, int n, int nz, int *irp,
+                      int *ja, double *val);
+/* y = alpha*A*x + beta*y with x, y MultiVectDevice handles */
+int d_spmvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX,
+                     double beta, void *deviceY);
+
+/* ======================================================================== */
+/* Additions (no one-to-one counterpart in the reference glue)               */
+/* ======================================================================== */
+
+/* Solver options: mirrors psb_c_SolverOptions
+ * (cbind/krylov/psb_krylov_cbind.h:17-27) field for field. */
+typedef struct psbx_SolverOptions {
+  int    iter;    /* out: iterations performed                       */
+  int    itmax;   /* in:  maximum iterations (reference default 1000) */
+  int    itrace;  /* in:  unused (no host printing on the device path) */
+  int    irst;    /* in:  unused by CG / BiCGSTAB                     */
+  int    istop;   /* in:  1 backward error, 2 ||r||/||b||, 3 ||r||/||r0|| */
+  double eps;     /* in:  stopping tolerance                          */
+  double err;     /* out: final error estimate                        */
+} psbx_SolverOptions;
+
+int psbx_DefaultSolverOptions(psbx_SolverOptions *opt);
+
+/* Matrix formats accepted by the solver entry points. */
+#define PSBX_FMT_HLL 0
+#define PSBX_FMT_ELL 1
+#define PSBX_FMT_CSR 2
+
+/* Device-resident psb_krylov('CG'|'BICGSTAB') (krylov/psb_dkrylov.f90:
+ * 179-210 dispatch, psb_dcg.F90:218-295, psb_dcgstab.f90:226-365) with the
+ * diagonal preconditioner (prec/impl/psb_d_diagprec_impl.f90:116):
+ *   mat   HLL / ELL handle, or a psbx_d_Cmat* for CSR (fmt selects)
+ *   dinv  MultiVectDevice with the inverse diagonal, or NULL for no prec
+ *   b, x  MultiVectDevice (x holds x0 on entry, the solution on exit)
+ * Scalars stay on the device; the stop test runs every iteration on the
+ * device; the host reads a status word once per captured batch of
+ * iterations.  Returns 0 (converged or itmax reached, as the reference),
+ * or an error code; opt->iter and opt->err are filled like psb_krylov's
+ * iter and err. */
+int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv,
+                 void *b, void *x, psbx_SolverOptions *opt);
+
+/* psb_d_diag_precbld (prec/impl/psb_d_diagprec_impl.f90:229-292) on the
+ * device: dinv(i) = 1/a_ii, 1 where a_ii == 0 (HLL uses idiag). */
+int psbx_diag_prec_build(void *mat, int fmt, void *dinv);
+
+/* Device-side CSR -> HLL build (the conversion of
+ * ext/impl/psi_d_convert_hll_from_coo.f90:31-122 with the padding of
+ * psi_d_xtr_ell_from_coo.f90:53-60) from a CSR matrix already on the device
+ * (irp/ja 1-based int32, val FP64).  *deviceMat receives a new HLL handle.
+ * perm (device int32[rows] or NULL): when given, hack rows are taken in the
+ * order perm[0..rows-1] (0-based row ids) and the SpMV scatters y through
+ * it; this is the row-sorted HLL variant for skewed row lengths. */
+int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, int nnz,
+                             const int *d_irp, const int *d_ja,
+                             const double *d_val, int hksz, const int *d_perm);
+
+/* Adds an FP32 copy of the values of an FP64 HLL handle (for the FP32 inner
+ * iterations of the mixed-precision solver). */
+int psbx_hll_make_single(void *deviceMat);
+
+/* Wraps caller-owned device memory (double, n entries) as a one-vector
+ * MultiVectDevice without allocating; freeMultiVecDevice on it releases the
+ * descriptor only. */
+int psbx_wrapMultiVecDevice(void **deviceVec, void *devPtr, unsigned size,
+                            unsigned elementType);
+void *psbx_multivec_data(void *deviceVec);
+
+/* Runs y = alpha*A*x + beta*y for an HLL handle on raw device pointers
+ * (x, y: double, y may not alias x) on the library stream, asynchronously. */
+int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x,
+                      double beta, double *y);
+/* Number of kernels launched by the library since load (for accounting). */
+uint64_t psbx_kernel_launches(void);
+/* Last CUDA error string seen by the library (static storage). */
+const char *psbx_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSBX_H */

@@ -1,0 +1,241 @@
+"""CPU oracle for the PSBLAS single-GPU sparse Krylov path.
+
+TEST INFRASTRUCTURE ONLY.  This package restates the reference's CPU path
+(conversion COO->CSR/HLL/ELL, csmv, vector kernels, diagonal preconditioner,
+CG and BiCGSTAB) in plain C (``oracle.c``).  Only ``tests/``, the smoke check
+and the CPU-baseline leg of ``bench.py`` may import it; the product library
+never calls it and has no CPU fallback.
+
+All index arrays are 1-based int32 like the reference Fortran; values FP64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (CPU only)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        I, D, I64, CH = C.c_int, C.c_double, C.c_int64, C.c_char
+        sig = {
+            "or_set_threads": (None, [I]),
+            "or_get_threads": (I, []),
+            "or_coo_fix": (I64, [I, I64, _i32p, _i32p, _f64p]),
+            "or_csr_from_coo": (None, [I, I64, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]),
+            "or_hll_alloc_size": (I64, [I, I64, _i32p, I]),
+            "or_hll_from_coo": (I, [I, I64, _i32p, _i32p, _f64p, I, _i32p, _i32p, _i32p, _f64p, _i32p]),
+            "or_ell_max_row": (I, [I, I64, _i32p]),
+            "or_ell_from_coo": (I, [I, I64, _i32p, _i32p, _f64p, I, I, _i32p, _i32p, _f64p, _i32p]),
+            "or_csr_csmv": (I, [CH, I, I, _i32p, _i32p, _f64p, D, _f64p, D, _f64p]),
+            "or_hll_csmv": (I, [CH, I, I, I, _i32p, _i32p, _i32p, _f64p, D, _f64p, D, _f64p]),
+            "or_ell_csmv": (I, [CH, I, I, I, I, _i32p, _i32p, _f64p, D, _f64p, D, _f64p]),
+            "or_hll_get_diag": (I, [I, I, _i32p, _i32p, _f64p, _i32p, _f64p]),
+            "or_axpby": (None, [I, D, _f64p, D, _f64p]),
+            "or_axpbyz": (None, [I, D, _f64p, D, _f64p, _f64p]),
+            "or_dot": (D, [I, _f64p, _f64p]),
+            "or_nrm2": (D, [I, _f64p]),
+            "or_amax": (D, [I, _f64p]),
+            "or_asum": (D, [I, _f64p]),
+            "or_mlt": (None, [I, D, _f64p, _f64p, D, _f64p]),
+            "or_upd_xyz": (None, [I, D, D, D, D, _f64p, _f64p, _f64p]),
+            "or_xyzw": (None, [I, D, D, D, D, D, D, _f64p, _f64p, _f64p, _f64p]),
+            "or_diag_prec_build": (None, [I, _f64p, _f64p]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        for name in ("or_cg", "or_bicgstab"):
+            f = getattr(L, name)
+            f.restype = I
+            f.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I,
+                          C.POINTER(I), C.POINTER(D), C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().or_set_threads(int(n))
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ---------------------------------------------------------------- assembly
+def coo_fix(nr, ia, ja, val):
+    """Sort by (row, col) stably and add duplicates (psb_d_fix_coo)."""
+    ia, ja, val = _i32(ia).copy(), _i32(ja).copy(), _f64(val).copy()
+    nz = lib().or_coo_fix(int(nr), len(ia), ia, ja, val)
+    return ia[:nz], ja[:nz], val[:nz]
+
+
+def csr_from_coo(nr, ia, ja, val):
+    ia, ja, val = _i32(ia), _i32(ja), _f64(val)
+    irp = np.zeros(nr + 1, np.int32)
+    cja = np.zeros(len(ja), np.int32)
+    cval = np.zeros(len(val), np.float64)
+    lib().or_csr_from_coo(int(nr), len(ia), ia, ja, val, irp, cja, cval)
+    return irp, cja, cval
+
+
+def hll_from_coo(nr, ia, ja, val, hksz=32):
+    """Row-sorted COO -> HLL (psi_d_convert_hll_from_coo)."""
+    ia, ja, val = _i32(ia), _i32(ja), _f64(val)
+    isz = lib().or_hll_alloc_size(int(nr), len(ia), ia, int(hksz))
+    noffs = (nr + hksz - 1) // hksz
+    irn = np.zeros(nr, np.int32)
+    hkoffs = np.zeros(noffs + 1, np.int32)
+    hja = np.zeros(max(isz, 1), np.int32)
+    hval = np.zeros(max(isz, 1), np.float64)
+    idiag = np.zeros(nr, np.int32)
+    lib().or_hll_from_coo(int(nr), len(ia), ia, ja, val, int(hksz), irn, hkoffs, hja, hval, idiag)
+    return dict(irn=irn, hkoffs=hkoffs, ja=hja[:isz], val=hval[:isz], idiag=idiag, hksz=hksz)
+
+
+def ell_from_coo(nr, ia, ja, val, ldv=None):
+    """Row-sorted COO -> ELL (psi_d_convert_ell_from_coo); ldv >= nr rows."""
+    ia, ja, val = _i32(ia), _i32(ja), _f64(val)
+    ldv = nr if ldv is None else int(ldv)
+    nzm = lib().or_ell_max_row(int(nr), len(ia), ia)
+    irn = np.zeros(nr, np.int32)
+    idiag = np.zeros(nr, np.int32)
+    eja = np.zeros(max(ldv * nzm, 1), np.int32)
+    eval_ = np.zeros(max(ldv * nzm, 1), np.float64)
+    lib().or_ell_from_coo(int(nr), len(ia), ia, ja, val, ldv, nzm, irn, eja, eval_, idiag)
+    return dict(irn=irn, ja=eja[: ldv * nzm], val=eval_[: ldv * nzm], idiag=idiag, ldv=ldv, nzm=nzm)
+
+
+# ---------------------------------------------------------------- SpMV
+def csr_csmv(irp, ja, val, alpha, x, beta, y, trans="N", nc=None):
+    nr = len(irp) - 1
+    nc = nr if nc is None else nc
+    y = _f64(y).copy()
+    lib().or_csr_csmv(trans.encode(), nr, int(nc), _i32(irp), _i32(ja), _f64(val),
+                      float(alpha), _f64(x), float(beta), y)
+    return y
+
+
+def hll_csmv(h, nr, alpha, x, beta, y, trans="N", nc=None):
+    nc = nr if nc is None else nc
+    y = _f64(y).copy()
+    lib().or_hll_csmv(trans.encode(), int(nr), int(nc), int(h["hksz"]), h["irn"], h["hkoffs"],
+                      _i32(h["ja"]) if len(h["ja"]) else np.zeros(1, np.int32),
+                      _f64(h["val"]) if len(h["val"]) else np.zeros(1),
+                      float(alpha), _f64(x), float(beta), y)
+    return y
+
+
+def ell_csmv(e, nr, alpha, x, beta, y, trans="N", nc=None):
+    nc = nr if nc is None else nc
+    y = _f64(y).copy()
+    lib().or_ell_csmv(trans.encode(), int(nr), int(nc), int(e["ldv"]), int(e["nzm"]), e["irn"],
+                      _i32(e["ja"]) if len(e["ja"]) else np.zeros(1, np.int32),
+                      _f64(e["val"]) if len(e["val"]) else np.zeros(1),
+                      float(alpha), _f64(x), float(beta), y)
+    return y
+
+
+def hll_get_diag(h, nr):
+    d = np.zeros(nr, np.float64)
+    lib().or_hll_get_diag(int(nr), int(h["hksz"]), h["irn"], h["hkoffs"],
+                          _f64(h["val"]) if len(h["val"]) else np.zeros(1), h["idiag"], d)
+    return d
+
+
+# ---------------------------------------------------------------- vectors
+def axpby(alpha, x, beta, y):
+    y = _f64(y).copy()
+    lib().or_axpby(len(y), float(alpha), _f64(x), float(beta), y)
+    return y
+
+
+def axpbyz(alpha, x, beta, y):
+    z = np.zeros(len(y))
+    lib().or_axpbyz(len(y), float(alpha), _f64(x), float(beta), _f64(y), z)
+    return z
+
+
+def dot(x, y):
+    return lib().or_dot(len(x), _f64(x), _f64(y))
+
+
+def nrm2(x):
+    return lib().or_nrm2(len(x), _f64(x))
+
+
+def amax(x):
+    return lib().or_amax(len(x), _f64(x))
+
+
+def asum(x):
+    return lib().or_asum(len(x), _f64(x))
+
+
+def mlt(alpha, d, x, beta, z):
+    z = _f64(z).copy()
+    lib().or_mlt(len(z), float(alpha), _f64(d), _f64(x), float(beta), z)
+    return z
+
+
+def upd_xyz(alpha, beta, gamma, delta, x, y, z):
+    y, z = _f64(y).copy(), _f64(z).copy()
+    lib().or_upd_xyz(len(y), alpha, beta, gamma, delta, _f64(x), y, z)
+    return y, z
+
+
+def xyzw(a, b, c, d, e, f, x, y, z, w):
+    y, z, w = _f64(y).copy(), _f64(z).copy(), _f64(w).copy()
+    lib().or_xyzw(len(y), a, b, c, d, e, f, _f64(x), y, z, w)
+    return y, z, w
+
+
+def diag_prec_build(diag):
+    d = np.zeros(len(diag))
+    lib().or_diag_prec_build(len(diag), _f64(diag), d)
+    return d
+
+
+# ---------------------------------------------------------------- Krylov
+def krylov(method, irp, ja, val, b, x0=None, dinv=None, eps=1e-6, itmax=1000, istop=2,
+           history=False):
+    """psb_krylov('CG'|'BICGSTAB') restated; returns (x, iter, err[, hist])."""
+    n = len(irp) - 1
+    x = np.zeros(n) if x0 is None else _f64(x0).copy()
+    it, err = C.c_int(0), C.c_double(0.0)
+    hist = np.full(itmax + 1, np.nan) if history else None
+    d = None if dinv is None else _f64(dinv)
+    f = {"CG": lib().or_cg, "BICGSTAB": lib().or_bicgstab}[method.upper()]
+    rc = f(n, _i32(irp), _i32(ja), _f64(val),
+           None if d is None else d.ctypes.data_as(C.c_void_p),
+           _f64(b), x, float(eps), int(itmax), int(istop), C.byref(it), C.byref(err),
+           None if hist is None else hist.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise ValueError(f"oracle krylov failed rc={rc}")
+    if history:
+        return x, it.value, err.value, hist
+    return x, it.value, err.value

@@ -1,0 +1,634 @@
+/*
+ * oracle.c -- CPU restatement of the PSBLAS 3.9 CPU path (test
+ * infrastructure; see oracle.h).  Every function names the reference routine
+ * it restates, by file:line within the psblas3 source tree.
+ *
+ * Compiled with -O2 -fopenmp -ffp-contract=off.  Row-parallel loops keep the
+ * per-row summation order of the reference, so their results do not depend
+ * on the thread count.  Reductions (dot, nrm2, asum) run left to right when
+ * one thread is set; with more threads they sum static per-thread partials in
+ * thread order (deterministic for a fixed count), which is only used for
+ * timing the CPU baseline.
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static int g_threads = 1;
+
+void or_set_threads(int nthreads) { g_threads = nthreads > 0 ? nthreads : 1; }
+int  or_get_threads(void) { return g_threads; }
+
+/* ------------------------------------------------------------------------ */
+/* COO fix: stable sort by (row, col), add duplicates.                       */
+/* base/serial/impl/psb_d_coo_impl.F90:4094 (psb_d_fix_coo, dupl = add,     */
+/* psb_dupl_def_ = psb_dupl_add_ at base/modules/psb_const_mod.F90:225-228). */
+/* Counting sort by column then by row (both stable) gives the (row, col)    */
+/* order with ties kept in insertion order, so duplicates add in that order. */
+/* ------------------------------------------------------------------------ */
+int64_t or_coo_fix(int nr, int64_t nnz, int *ia, int *ja, double *val)
+{
+  if (nnz <= 0) return 0;
+  int nc = 0;
+  for (int64_t k = 0; k < nnz; k++) if (ja[k] > nc) nc = ja[k];
+  int64_t *cnt = (int64_t *)calloc((size_t)(nc > nr ? nc : nr) + 2, sizeof(int64_t));
+  int *ia2 = (int *)malloc(nnz * sizeof(int));
+  int *ja2 = (int *)malloc(nnz * sizeof(int));
+  double *v2 = (double *)malloc(nnz * sizeof(double));
+  /* pass 1: stable by column */
+  for (int64_t k = 0; k < nnz; k++) cnt[ja[k]]++;
+  int64_t s = 0;
+  for (int c = 0; c <= nc; c++) { int64_t t = cnt[c]; cnt[c] = s; s += t; }
+  for (int64_t k = 0; k < nnz; k++) {
+    int64_t p = cnt[ja[k]]++;
+    ia2[p] = ia[k]; ja2[p] = ja[k]; v2[p] = val[k];
+  }
+  /* pass 2: stable by row */
+  memset(cnt, 0, ((size_t)(nc > nr ? nc : nr) + 2) * sizeof(int64_t));
+  for (int64_t k = 0; k < nnz; k++) cnt[ia2[k]]++;
+  s = 0;
+  for (int r = 0; r <= nr; r++) { int64_t t = cnt[r]; cnt[r] = s; s += t; }
+  for (int64_t k = 0; k < nnz; k++) {
+    int64_t p = cnt[ia2[k]]++;
+    ia[p] = ia2[k]; ja[p] = ja2[k]; val[p] = v2[k];
+  }
+  free(cnt); free(ia2); free(ja2); free(v2);
+  /* add duplicates in order */
+  int64_t w = 0;
+  for (int64_t k = 0; k < nnz; k++) {
+    if (w > 0 && ia[w - 1] == ia[k] && ja[w - 1] == ja[k]) {
+      val[w - 1] = val[w - 1] + val[k];
+    } else {
+      ia[w] = ia[k]; ja[w] = ja[k]; val[w] = val[k]; w++;
+    }
+  }
+  return w;
+}
+
+/* COO (row-sorted) -> CSR.  base/serial/impl/psb_d_csr_impl.F90:3154
+ * (psb_d_cp_csr_from_coo): irp(1)=1, irp(i+1)=irp(i)+rowcount(i). */
+void or_csr_from_coo(int nr, int64_t nnz, const int *ia, const int *ja,
+                     const double *val, int *irp, int *cja, double *cval)
+{
+  for (int i = 0; i <= nr; i++) irp[i] = 0;
+  for (int64_t k = 0; k < nnz; k++) irp[ia[k]]++;
+  irp[0] = 1;
+  for (int i = 1; i <= nr; i++) irp[i] += irp[i - 1];
+  memcpy(cja, ja, nnz * sizeof(int));
+  memcpy(cval, val, nnz * sizeof(double));
+}
+
+/* ------------------------------------------------------------------------ */
+/* HLL conversion: ext/impl/psi_d_convert_hll_from_coo.f90:31-122 and        */
+/* ext/impl/psi_d_xtr_ell_from_coo.f90:31-62.                                */
+/*   irn(i)      = number of entries of row i                  (:59-64)     */
+/*   hkoffs(1)=0, hkoffs(j+1)=hkoffs(j)+hksz*max(irn in hack j)  (:69-82)   */
+/*   last hack pre-filled with val=0, ja=nr                      (:94-96)   */
+/*   inside hack: ja(ii,jj) with leading dimension hksz (column major)      */
+/*   padding: ja = last column of the row (jac(1) of the hack if the row is */
+/*   empty), val = 0                                        (xtr:53-60)     */
+/*   idiag(ii) = 1-based position of the diagonal in the row     (xtr:48)   */
+/* idiag is left at 0 for rows without a diagonal (the reference leaves it  */
+/* undefined there; psi_cuda_CopyCooToHlg.cuh:46 writes 0).                 */
+/* ------------------------------------------------------------------------ */
+int64_t or_hll_alloc_size(int nr, int64_t nnz, const int *ia, int hksz)
+{
+  int *irn = (int *)calloc(nr > 0 ? nr : 1, sizeof(int));
+  for (int64_t k = 0; k < nnz; k++) irn[ia[k] - 1]++;
+  int64_t off = 0;
+  for (int i = 0; i < nr; i += hksz) {
+    int ir = (hksz < nr - i) ? hksz : nr - i;
+    int mx = irn[i];
+    for (int k = 1; k < ir; k++) if (irn[i + k] > mx) mx = irn[i + k];
+    off += (int64_t)mx * hksz;
+  }
+  free(irn);
+  return off;
+}
+
+static void xtr_ell_from_coo(int i0, int nrh, int mxrwl, const int *iac,
+                             const int *jac, const double *valc, int *hja,
+                             double *hval, const int *irn, int *idiag, int ld)
+{
+  int64_t kc = 0;
+  for (int ii = 0; ii < nrh; ii++) {
+    int nc = irn[ii];
+    int ic = 0;
+    for (int jj = 0; jj < nc; jj++) {
+      int ir = iac[kc];
+      ic = jac[kc];
+      if (ir == ic) idiag[ii] = jj + 1;
+      hja[(int64_t)jj * ld + ii] = ic;
+      hval[(int64_t)jj * ld + ii] = valc[kc];
+      kc++;
+    }
+    if (nc == 0) ic = jac[0];
+    for (int jj = nc; jj < mxrwl; jj++) {
+      hja[(int64_t)jj * ld + ii] = ic;
+      hval[(int64_t)jj * ld + ii] = 0.0;
+    }
+  }
+  (void)i0;
+}
+
+int or_hll_from_coo(int nr, int64_t nnz, const int *ia, const int *ja,
+                    const double *val, int hksz, int *irn, int *hkoffs,
+                    int *hja, double *hval, int *idiag)
+{
+  for (int i = 0; i < nr; i++) { irn[i] = 0; idiag[i] = 0; }
+  for (int64_t k = 0; k < nnz; k++) irn[ia[k] - 1]++;
+  int noffs = (nr + hksz - 1) / hksz;
+  hkoffs[0] = 0;
+  int j = 0;
+  for (int i = 0; i < nr; i += hksz) {
+    int ir = (hksz < nr - i) ? hksz : nr - i;
+    int mx = irn[i];
+    for (int k = 1; k < ir; k++) if (irn[i + k] > mx) mx = irn[i + k];
+    hkoffs[j + 1] = hkoffs[j] + mx * hksz;
+    j++;
+  }
+  if (noffs > 0) {
+    int64_t isz = hkoffs[noffs];
+    int64_t nzm = hkoffs[noffs] - hkoffs[noffs - 1];
+    for (int64_t k = isz - nzm; k < isz; k++) { hval[k] = 0.0; hja[k] = nr; }
+  }
+  int64_t kc = 0, k = 0;
+  for (int i = 0; i < nr; i += hksz) {
+    int ir = (hksz < nr - i) ? hksz : nr - i;
+    int hk = i / hksz;
+    int64_t isz = hkoffs[hk + 1] - hkoffs[hk];
+    int mxrwl = (int)(isz / hksz);
+    int64_t nza = 0;
+    for (int t = 0; t < ir; t++) nza += irn[i + t];
+    if (isz > 0)
+      xtr_ell_from_coo(i, ir, mxrwl, ia + kc, ja + kc, val + kc, hja + k,
+                       hval + k, irn + i, idiag + i, hksz);
+    k += isz;
+    kc += nza;
+  }
+  return 0;
+}
+
+/* ELL conversion: ext/impl/psi_d_convert_ell_from_coo.f90:31-86 (nzm = max
+ * row length, ldv rows per column, padding as xtr_ell_from_coo).  Rows
+ * nr+1..ldv are filled with val=0, ja=1 (the reference leaves them undefined
+ * and never reads them). */
+int or_ell_max_row(int nr, int64_t nnz, const int *ia)
+{
+  int *irn = (int *)calloc(nr > 0 ? nr : 1, sizeof(int));
+  for (int64_t k = 0; k < nnz; k++) irn[ia[k] - 1]++;
+  int mx = 0;
+  for (int i = 0; i < nr; i++) if (irn[i] > mx) mx = irn[i];
+  free(irn);
+  return mx;
+}
+
+int or_ell_from_coo(int nr, int64_t nnz, const int *ia, const int *ja,
+                    const double *val, int ldv, int nzm, int *irn, int *eja,
+                    double *eval, int *idiag)
+{
+  if (ldv < nr) return 1;
+  for (int i = 0; i < nr; i++) { irn[i] = 0; idiag[i] = 0; }
+  for (int64_t k = 0; k < nnz; k++) irn[ia[k] - 1]++;
+  for (int64_t c = 0; c < nzm; c++)
+    for (int i = nr; i < ldv; i++) { eja[c * ldv + i] = 1; eval[c * ldv + i] = 0.0; }
+  if (nnz > 0 && nzm > 0)
+    xtr_ell_from_coo(0, nr, nzm, ia, ja, val, eja, eval, irn, idiag, ldv);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* SpMV.  Non-transposed rows follow the inner form of the reference:       */
+/*   ext/impl/psb_d_hll_csmv.f90:291-371 (psb_d_hll_csmv_inner),            */
+/*   ext/impl/psb_d_ell_csmv.f90:91-200,                                    */
+/*   base/serial/impl/psb_d_csr_impl.F90:113-270 (psb_d_csr_csmv_inner):    */
+/*   acc = 0; acc = acc + val*x(ja) over the row's stored entries in order; */
+/*   alpha == 0: y = beta*y (y = 0 when beta == 0), x not read;             */
+/*   beta == 0: y = alpha*acc, y not read; otherwise y = alpha*acc+beta*y.  */
+/* The reference's special cases alpha,beta in {+1,-1} give the same bits   */
+/* as this generic form for finite data.                                    */
+/* Transposed: y = beta*y first, then y(ja) += alpha*val*x(row)             */
+/* (psb_d_hll_csmv.f90:70-105; psb_d_csr_impl.F90:271-330).                 */
+/* ------------------------------------------------------------------------ */
+static inline double finish_row(double alpha, double acc, double beta, double yold)
+{
+  if (beta == 0.0) return alpha * acc;
+  return alpha * acc + beta * yold;
+}
+
+static void scale_y(int m, double beta, double *y)
+{
+  if (beta == 0.0) { for (int i = 0; i < m; i++) y[i] = 0.0; }
+  else if (beta != 1.0) { for (int i = 0; i < m; i++) y[i] = beta * y[i]; }
+}
+
+int or_csr_csmv(char trans, int nr, int nc, const int *irp, const int *ja,
+                const double *val, double alpha, const double *x, double beta,
+                double *y)
+{
+  int tra = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
+  int m = tra ? nc : nr;
+  if (alpha == 0.0) { scale_y(m, beta, y); return 0; }
+  if (!tra) {
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int i = 0; i < nr; i++) {
+      double acc = 0.0;
+      for (int j = irp[i]; j < irp[i + 1]; j++) acc = acc + val[j - 1] * x[ja[j - 1] - 1];
+      y[i] = finish_row(alpha, acc, beta, beta == 0.0 ? 0.0 : y[i]);
+    }
+  } else {
+    scale_y(m, beta, y);
+    for (int i = 0; i < nr; i++)
+      for (int j = irp[i]; j < irp[i + 1]; j++)
+        y[ja[j - 1] - 1] = y[ja[j - 1] - 1] + alpha * val[j - 1] * x[i];
+  }
+  return 0;
+}
+
+int or_hll_csmv(char trans, int nr, int nc, int hksz, const int *irn,
+                const int *hkoffs, const int *hja, const double *hval,
+                double alpha, const double *x, double beta, double *y)
+{
+  int tra = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
+  int nhk = (nr + hksz - 1) / hksz;
+  if (!tra) {
+    if (alpha == 0.0) { scale_y(nr, beta, y); return 0; }
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int h = 0; h < nhk; h++) {
+      int i0 = h * hksz;
+      int ir = (hksz < nr - i0) ? hksz : nr - i0;
+      const int *hj = hja + hkoffs[h];
+      const double *hv = hval + hkoffs[h];
+      for (int ii = 0; ii < ir; ii++) {
+        double acc = 0.0;
+        for (int jj = 0; jj < irn[i0 + ii]; jj++)
+          acc = acc + hv[(int64_t)jj * hksz + ii] * x[hj[(int64_t)jj * hksz + ii] - 1];
+        y[i0 + ii] = finish_row(alpha, acc, beta, beta == 0.0 ? 0.0 : y[i0 + ii]);
+      }
+    }
+  } else {
+    scale_y(nc, beta, y);
+    for (int h = 0; h < nhk; h++) {
+      int i0 = h * hksz;
+      int ir = (hksz < nr - i0) ? hksz : nr - i0;
+      const int *hj = hja + hkoffs[h];
+      const double *hv = hval + hkoffs[h];
+      for (int ii = 0; ii < ir; ii++)
+        for (int jj = 0; jj < irn[i0 + ii]; jj++) {
+          int jc = hj[(int64_t)jj * hksz + ii] - 1;
+          y[jc] = y[jc] + alpha * hv[(int64_t)jj * hksz + ii] * x[i0 + ii];
+        }
+    }
+  }
+  return 0;
+}
+
+int or_ell_csmv(char trans, int nr, int nc, int ldv, int nzm, const int *irn,
+                const int *eja, const double *eval, double alpha,
+                const double *x, double beta, double *y)
+{
+  int tra = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
+  (void)nzm;
+  if (!tra) {
+    if (alpha == 0.0) { scale_y(nr, beta, y); return 0; }
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int i = 0; i < nr; i++) {
+      double acc = 0.0;
+      for (int jj = 0; jj < irn[i]; jj++)
+        acc = acc + eval[(int64_t)jj * ldv + i] * x[eja[(int64_t)jj * ldv + i] - 1];
+      y[i] = finish_row(alpha, acc, beta, beta == 0.0 ? 0.0 : y[i]);
+    }
+  } else {
+    scale_y(nc, beta, y);
+    for (int i = 0; i < nr; i++)
+      for (int jj = 0; jj < irn[i]; jj++) {
+        int jc = eja[(int64_t)jj * ldv + i] - 1;
+        y[jc] = y[jc] + alpha * eval[(int64_t)jj * ldv + i] * x[i];
+      }
+  }
+  return 0;
+}
+
+/* ext/impl/psb_d_hll_get_diag.f90:89-107: d(i) = val(i, idiag(i)) or 0. */
+int or_hll_get_diag(int nr, int hksz, const int *irn, const int *hkoffs,
+                    const double *hval, const int *idiag, double *d)
+{
+  (void)irn;
+  for (int i = 0; i < nr; i++) {
+    int h = i / hksz, ii = i % hksz;
+    d[i] = idiag[i] != 0 ? hval[hkoffs[h] + (int64_t)(idiag[i] - 1) * hksz + ii] : 0.0;
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dense vector kernels.                                                     */
+/* axpby: base/serial/psi_d_serial_impl.F90:593-745 (psi_daxpbyv).  The      */
+/* special cases there (alpha, beta in {0, +1, -1}) equal the generic form   */
+/* bit for bit for finite data; what they change is which operand is read:   */
+/* alpha == 0 never reads x, beta == 0 never reads y.                        */
+/* ------------------------------------------------------------------------ */
+void or_axpby(int n, double alpha, const double *x, double beta, double *y)
+{
+  if (alpha == 0.0) {
+    if (beta == 0.0) { for (int i = 0; i < n; i++) y[i] = 0.0; }
+    else if (beta != 1.0) { for (int i = 0; i < n; i++) y[i] = beta * y[i]; }
+    return;
+  }
+  if (beta == 0.0) { for (int i = 0; i < n; i++) y[i] = alpha * x[i]; return; }
+  for (int i = 0; i < n; i++) y[i] = alpha * x[i] + beta * y[i];
+}
+
+/* psi_daxpbyv2 (psi_d_serial_impl.F90:746-825): z = alpha*x + beta*y. */
+void or_axpbyz(int n, double alpha, const double *x, double beta,
+               const double *y, double *z)
+{
+  for (int i = 0; i < n; i++) {
+    double a = (alpha == 0.0) ? 0.0 : alpha * x[i];
+    z[i] = (beta == 0.0) ? a : (alpha == 0.0 ? beta * y[i] : a + beta * y[i]);
+  }
+}
+
+/* dot and nrm2: base/modules/serial/psb_d_base_vect_mod.F90:974-996 and
+ * :1764-1774 call external BLAS ddot/dnrm2 (third party, unpinned).  The
+ * restatement is a plain left-to-right FP64 sum; nrm2 = sqrt(sum x^2), the
+ * GPU reference's formula (cuda/spgpu/kernels/dnrm2.cu). */
+double or_dot(int n, const double *x, const double *y)
+{
+  if (g_threads <= 1) {
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s = s + x[i] * y[i];
+    return s;
+  }
+  double part[1024];
+  int nt = g_threads > 1024 ? 1024 : g_threads;
+#pragma omp parallel num_threads(nt)
+  {
+    int t = 0, T = 1;
+#ifdef _OPENMP
+    t = omp_get_thread_num(); T = omp_get_num_threads();
+#endif
+    int64_t lo = (int64_t)n * t / T, hi = (int64_t)n * (t + 1) / T;
+    double s = 0.0;
+    for (int64_t i = lo; i < hi; i++) s = s + x[i] * y[i];
+    part[t] = s;
+    if (t == 0) nt = T;
+  }
+  double s = 0.0;
+  for (int t = 0; t < nt; t++) s = s + part[t];
+  return s;
+}
+
+double or_nrm2(int n, const double *x) { return sqrt(or_dot(n, x, x)); }
+
+double or_amax(int n, const double *x)
+{
+  double m = 0.0;
+  for (int i = 0; i < n; i++) { double a = fabs(x[i]); if (a > m) m = a; }
+  return m;
+}
+
+double or_asum(int n, const double *x)
+{
+  double s = 0.0;
+  for (int i = 0; i < n; i++) s = s + fabs(x[i]);
+  return s;
+}
+
+/* mlt: z = alpha*d.*x + beta*z (psb_d_base_vect_mod mlt_a_2; GPU
+ * cuda/spgpu/kernels/axy_base.cuh:110-210).  beta == 0 never reads z;
+ * alpha == 1 gives d*x exactly. */
+void or_mlt(int n, double alpha, const double *d, const double *x,
+            double beta, double *z)
+{
+  for (int i = 0; i < n; i++) {
+    double t = alpha * (d[i] * x[i]);
+    z[i] = (beta == 0.0) ? t : t + beta * z[i];
+  }
+}
+
+/* psi_d_upd_xyz (psi_d_serial_impl.F90:1571-1794): y = alpha*x + beta*y;
+ * z = gamma*y + delta*z. */
+void or_upd_xyz(int n, double alpha, double beta, double gamma, double delta,
+                const double *x, double *y, double *z)
+{
+  or_axpby(n, alpha, x, beta, y);
+  or_axpby(n, gamma, y, delta, z);
+}
+
+/* psi_dxyzw (psi_d_serial_impl.F90:1853-1855): y = a*x+b*y; z = c*y+d*z;
+ * w = e*z+f*w (the CPU semantics; the reference GPU kernel dxyzw.cu:47-49
+ * computes a different expression, which is not followed). */
+void or_xyzw(int n, double a, double b, double c, double d, double e,
+             double f, const double *x, double *y, double *z, double *w)
+{
+  for (int i = 0; i < n; i++) {
+    y[i] = a * x[i] + b * y[i];
+    z[i] = c * y[i] + d * z[i];
+    w[i] = e * z[i] + f * w[i];
+  }
+}
+
+/* prec/impl/psb_d_diagprec_impl.f90:261-267: d = 1/diag, 1 where diag==0. */
+void or_diag_prec_build(int n, const double *diag, double *dinv)
+{
+  for (int i = 0; i < n; i++) dinv[i] = (diag[i] == 0.0) ? 1.0 : 1.0 / diag[i];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Krylov.  Stopping test: krylov/psb_d_krylov_conv_mod.f90:205-356.         */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int istop, itmax;
+  double eps, ani, bni, bn2, r0n2, errnum, errden;
+} conv_t;
+
+static double csr_normi(int n, const int *irp, const double *val)
+{
+  double m = 0.0;
+  for (int i = 0; i < n; i++) {
+    double s = 0.0;
+    for (int j = irp[i]; j < irp[i + 1]; j++) s += fabs(val[j - 1]);
+    if (s > m) m = s;
+  }
+  return m;
+}
+
+static int init_conv(conv_t *c, int istop, int itmax, double eps, int n,
+                     const int *irp, const int *ja, const double *val,
+                     const double *b, const double *x)
+{
+  c->istop = istop; c->itmax = itmax; c->eps = eps;
+  c->errnum = 0.0; c->errden = 1.0;
+  if (istop == 1) {
+    c->ani = csr_normi(n, irp, val);
+    c->bni = or_amax(n, b);
+  } else if (istop == 2) {
+    c->bn2 = or_nrm2(n, b);
+  } else if (istop == 3) {
+    double *r = (double *)malloc(n * sizeof(double));
+    memcpy(r, b, n * sizeof(double));
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    c->r0n2 = or_nrm2(n, r);
+    free(r);
+  } else {
+    return 1;
+  }
+  return 0;
+}
+
+static int check_conv(conv_t *c, int it, int n, const double *x, const double *r)
+{
+  if (c->istop == 1) {
+    c->errnum = or_amax(n, r);
+    c->errden = c->ani * or_amax(n, x) + c->bni;
+  } else if (c->istop == 2) {
+    c->errnum = or_nrm2(n, r);
+    c->errden = c->bn2;
+  } else {
+    c->errnum = or_nrm2(n, r);
+    c->errden = c->r0n2;
+  }
+  int res;
+  if (c->errden == 0.0) res = (c->errnum <= c->eps);
+  else res = (c->errnum <= c->eps * c->errden);
+  return res || (c->itmax <= it);
+}
+
+static double end_err(const conv_t *c)
+{
+  /* krylov/psb_base_krylov_conv_mod.f90:96-136 (log_end) */
+  return c->errden == 0.0 ? c->errnum : c->errnum / c->errden;
+}
+
+static void prec_apply(int n, const double *dinv, const double *x, double *y)
+{
+  if (dinv) or_mlt(n, 1.0, dinv, x, 0.0, y);
+  else memcpy(y, x, n * sizeof(double));
+}
+
+/* krylov/psb_dcg.F90:218-295 (psb_dcg_vect), restart loop included. */
+int or_cg(int n, const int *irp, const int *ja, const double *val,
+          const double *dinv, const double *b, double *x, double eps,
+          int itmax, int istop, int *iter, double *err, double *res_hist)
+{
+  double *p = (double *)calloc(n, sizeof(double));
+  double *q = (double *)calloc(n, sizeof(double));
+  double *r = (double *)calloc(n, sizeof(double));
+  double *z = (double *)calloc(n, sizeof(double));
+  conv_t c;
+  int itx = 0, rc = 0;
+  double alpha = 0.0, rho, rho_old, beta, sigma;
+  for (;;) {
+    if (itx >= itmax) break;
+    int it = 0;
+    or_axpby(n, 1.0, b, 0.0, r);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    rho = 0.0;
+    if (init_conv(&c, istop, itmax, eps, n, irp, ja, val, b, x)) { rc = 1; goto done; }
+    int conv = 0;
+    for (;;) {
+      it++; itx++;
+      prec_apply(n, dinv, r, z);
+      rho_old = rho;
+      rho = or_dot(n, r, z);
+      if (it == 1) {
+        or_axpby(n, 1.0, z, 0.0, p);
+      } else {
+        if (rho_old == 0.0) break;
+        beta = rho / rho_old;
+        or_axpby(n, 1.0, z, beta, p);
+      }
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, p, 0.0, q);
+      sigma = or_dot(n, p, q);
+      if (sigma == 0.0) break;
+      alpha = rho / sigma;
+      or_axpby(n, alpha, p, 1.0, x);
+      or_axpby(n, -alpha, q, 1.0, r);
+      int stop = check_conv(&c, itx, n, x, r);
+      if (res_hist && itx <= itmax) res_hist[itx] = end_err(&c);
+      if (stop) { conv = 1; break; }
+    }
+    if (conv) break;
+  }
+  *iter = itx;
+  *err = end_err(&c);
+done:
+  free(p); free(q); free(r); free(z);
+  return rc;
+}
+
+/* krylov/psb_dcgstab.f90:226-365 (psb_dcgstab_vect), restart loop included. */
+int or_bicgstab(int n, const int *irp, const int *ja, const double *val,
+                const double *dinv, const double *b, double *x, double eps,
+                int itmax, int istop, int *iter, double *err,
+                double *res_hist)
+{
+  double *q = (double *)calloc(n, sizeof(double));
+  double *r = (double *)calloc(n, sizeof(double));
+  double *p = (double *)calloc(n, sizeof(double));
+  double *v = (double *)calloc(n, sizeof(double));
+  double *s = (double *)calloc(n, sizeof(double));
+  double *t = (double *)calloc(n, sizeof(double));
+  double *z = (double *)calloc(n, sizeof(double));
+  double *f = (double *)calloc(n, sizeof(double));
+  conv_t c;
+  int itx = 0, rc = 0;
+  double rho = 0.0, rho_old, alpha = 0.0, omega = 0.0, beta, sigma, tau;
+  if (init_conv(&c, istop, itmax, eps, n, irp, ja, val, b, x)) { rc = 1; goto done; }
+  for (;;) {
+    if (itx >= itmax) break;
+    int it = 0;
+    or_axpby(n, 1.0, b, 0.0, r);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    or_axpby(n, 1.0, r, 0.0, q);
+    if (check_conv(&c, itx, n, x, r)) break;
+    if (res_hist) res_hist[itx] = end_err(&c);
+    rho = 0.0;
+    int conv = 0;
+    for (;;) {
+      it++; itx++;
+      rho_old = rho;
+      rho = or_dot(n, q, r);
+      if (rho == 0.0) break;
+      if (it == 1) {
+        or_axpby(n, 1.0, r, 0.0, p);
+      } else {
+        beta = (rho / rho_old) * (alpha / omega);
+        or_axpby(n, -omega, v, 1.0, p);
+        or_axpby(n, 1.0, r, beta, p);
+      }
+      prec_apply(n, dinv, p, f);
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, f, 0.0, v);
+      sigma = or_dot(n, q, v);
+      if (sigma == 0.0) break;
+      alpha = rho / sigma;
+      or_axpby(n, 1.0, r, 0.0, s);
+      or_axpby(n, -alpha, v, 1.0, s);
+      prec_apply(n, dinv, s, z);
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, z, 0.0, t);
+      sigma = or_dot(n, t, t);
+      if (sigma == 0.0) break;
+      tau = or_dot(n, t, s);
+      omega = tau / sigma;
+      if (omega == 0.0) break;
+      or_axpby(n, alpha, f, 1.0, x);
+      or_axpby(n, omega, z, 1.0, x);
+      or_axpby(n, 1.0, s, 0.0, r);
+      or_axpby(n, -omega, t, 1.0, r);
+      int stop = check_conv(&c, itx, n, x, r);
+      if (res_hist && itx <= itmax) res_hist[itx] = end_err(&c);
+      if (stop) { conv = 1; break; }
+    }
+    if (conv) break;
+  }
+  *iter = itx;
+  *err = end_err(&c);
+done:
+  free(q); free(r); free(p); free(v); free(s); free(t); free(z); free(f);
+  return rc;
+}

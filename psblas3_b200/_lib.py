@@ -1,0 +1,117 @@
+"""ctypes binding of libpsbx.so (the C-ABI declared in include/psbx.h).
+
+The shared library is built in-tree (``python -m psblas3_b200.build`` or
+``__graft_entry__.build()``).  There is no fallback: if the library is
+missing or cannot be loaded, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpsbx.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libpsbx.so not built at {LIB_PATH}; run __graft_entry__.build()")
+
+lib = C.CDLL(LIB_PATH)
+
+I, U, D, F, P, CH = C.c_int, C.c_uint, C.c_double, C.c_float, C.c_void_p, C.c_char_p
+PI = C.POINTER(C.c_int)
+PD = C.POINTER(C.c_double)
+PP = C.POINTER(C.c_void_p)
+
+
+class SolverOptions(C.Structure):
+    """psbx_SolverOptions == psb_c_SolverOptions (cbind/krylov/psb_krylov_cbind.h:17-27)."""
+    _fields_ = [("iter", C.c_int), ("itmax", C.c_int), ("itrace", C.c_int), ("irst", C.c_int),
+                ("istop", C.c_int), ("eps", C.c_double), ("err", C.c_double)]
+
+
+class Cmat(C.Structure):
+    """psbx_d_Cmat == the interoperable d_Cmat of cuda/d_cusparse_mod.F90:36-38."""
+    _fields_ = [("mat", C.c_void_p)]
+
+
+PC = C.POINTER(Cmat)
+
+_SIGS = {
+    # environment
+    "gpuInit": (I, [I]), "gpuClose": (None, []), "setDevice": (I, [I]), "getDevice": (I, []),
+    "getDeviceCount": (I, []), "getDeviceHasUVA": (I, []), "DeviceHasUVA": (I, []),
+    "getGPUMultiProcessors": (I, []), "getGPUMemoryBusWidth": (I, []), "getGPUMemoryClockRate": (I, []),
+    "getGPUWarpSize": (I, []), "getGPUMaxThreadsPerBlock": (I, []), "getGPUMaxThreadsPerMP": (I, []),
+    "getGPUMaxRegistersPerBlock": (I, []), "cpyGPUNameString": (None, [C.c_char_p]),
+    "cudaSync": (None, []), "cudaReset": (None, []), "psb_cudaGetHandle": (P, []),
+    "psb_cudaCreateHandle": (None, []), "psb_cudaDestroyHandle": (None, []),
+    "psb_cudaGetStream": (P, []), "psb_cudaSetStream": (None, [P]),
+    # multivectors
+    "FallocMultiVecDevice": (I, [PP, U, U, U]), "freeMultiVecDevice": (None, [P]),
+    "getMultiVecDeviceSize": (I, [P]), "getMultiVecDeviceCount": (I, [P]), "getMultiVecDevicePitch": (I, [P]),
+    "writeMultiVecDeviceDouble": (I, [P, P]), "writeMultiVecDeviceDoubleR2": (I, [P, P, I]),
+    "readMultiVecDeviceDouble": (I, [P, P]), "readMultiVecDeviceDoubleR2": (I, [P, P, I]),
+    "writeMultiVecDeviceFloat": (I, [P, P]), "readMultiVecDeviceFloat": (I, [P, P]),
+    "setscalMultiVecDeviceDouble": (I, [D, I, I, I, P]), "scalMultiVecDeviceDouble": (I, [D, P]),
+    "nrm2MultiVecDeviceDouble": (I, [PD, I, P]), "amaxMultiVecDeviceDouble": (I, [PD, I, P]),
+    "asumMultiVecDeviceDouble": (I, [PD, I, P]), "dotMultiVecDeviceDouble": (I, [PD, I, P, P]),
+    "axpbyMultiVecDeviceDouble": (I, [I, D, P, D, P]),
+    "upd_xyzMultiVecDeviceDouble": (I, [I, D, D, D, D, P, P, P]),
+    "xyzwMultiVecDeviceDouble": (I, [I, D, D, D, D, D, D, P, P, P, P]),
+    "axyMultiVecDeviceDouble": (I, [I, D, P, P]), "axybzMultiVecDeviceDouble": (I, [I, D, P, P, D, P]),
+    "absMultiVecDeviceDouble2": (I, [I, D, P, P]), "absMultiVecDeviceDouble": (I, [I, D, P]),
+    # HLL
+    "FallocHllDevice": (I, [PP, U, U, U, U, U, U]), "freeHllDevice": (None, [P]),
+    "getHllDeviceParams": (I, [P, PI, PI, PI, PI, PI, PI, PI]),
+    "writeHllDeviceDouble": (I, [P, P, P, P, P, P]), "readHllDeviceDouble": (I, [P, P, P, P, P, P]),
+    "writeHllDeviceFloat": (I, [P, P, P, P, P, P]), "readHllDeviceFloat": (I, [P, P, P, P, P, P]),
+    "psiCopyCooToHlgDouble": (I, [I, I, I, I, I, I, P, P, P, P, P, P]),
+    "spmvHllDeviceDouble": (I, [P, D, P, D, P]), "spmvHllDeviceFloat": (I, [P, F, P, F, P]),
+    # ELL
+    "FallocEllDevice": (I, [PP, U, U, U, U, U, U]), "freeEllDevice": (None, [P]), "zeroEllDevice": (None, [P]),
+    "getEllDevicePitch": (I, [P]), "getEllDeviceMaxRowSize": (I, [P]),
+    "writeEllDeviceDouble": (I, [P, P, P, I, P, P]), "readEllDeviceDouble": (I, [P, P, P, I, P, P]),
+    "psiCopyCooToElgDouble": (I, [I, I, I, I, I, I, P, P, P, P, P]),
+    "spmvEllDeviceDouble": (I, [P, D, P, D, P]),
+    # CSR
+    "d_CSRGDeviceAlloc": (I, [PC, I, I, I]), "d_CSRGDeviceFree": (I, [PC]),
+    "d_CSRGDeviceGetParms": (I, [PC, PI, PI, PI]), "d_CSRGDeviceSetMatType": (I, [PC, I]),
+    "d_CSRGDeviceSetMatFillMode": (I, [PC, I]), "d_CSRGDeviceSetMatDiagType": (I, [PC, I]),
+    "d_CSRGDeviceSetMatIndexBase": (I, [PC, I]),
+    "d_CSRGHost2Device": (I, [PC, I, I, I, P, P, P]), "d_CSRGDevice2Host": (I, [PC, I, I, I, P, P, P]),
+    "d_spmvCSRGDevice": (I, [PC, D, P, D, P]),
+    # additions
+    "psbx_DefaultSolverOptions": (I, [C.POINTER(SolverOptions)]),
+    "psbx_dkrylov": (I, [CH, P, I, P, P, P, C.POINTER(SolverOptions)]),
+    "psbx_diag_prec_build": (I, [P, I, P]),
+    "psbx_hll_from_csr_device": (I, [PP, I, I, I, P, P, P, I, P]),
+    "psbx_hll_make_single": (I, [P]),
+    "psbx_wrapMultiVecDevice": (I, [PP, P, U, U]), "psbx_multivec_data": (P, [P]),
+    "psbx_hll_spmv_raw": (I, [P, D, P, D, P]),
+    "psbx_kernel_launches": (C.c_uint64, []), "psbx_last_error": (C.c_char_p, []),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED = tuple(_SIGS)
+
+SPGPU_SUCCESS, SPGPU_UNSUPPORTED, SPGPU_UNSPECIFIED, SPGPU_OUTOFMEMORY = 0, 1, 2, 3
+PSBX_TIMEOUT, PSBX_BREAKDOWN, PSBX_NOT_CONVERGED = 4, 5, 6
+SPGPU_TYPE_INT, SPGPU_TYPE_FLOAT, SPGPU_TYPE_DOUBLE = 0, 1, 2
+PSBX_FMT_HLL, PSBX_FMT_ELL, PSBX_FMT_CSR = 0, 1, 2
+
+
+class PsbxError(RuntimeError):
+    def __init__(self, where, code):
+        msg = lib.psbx_last_error().decode(errors="replace")
+        super().__init__(f"{where} returned {code} ({msg})")
+        self.code = code
+
+
+def check(rc, where):
+    if rc != 0:
+        raise PsbxError(where, rc)
+    return rc

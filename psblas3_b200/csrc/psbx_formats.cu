@@ -1,0 +1,768 @@
+// psbx_formats.cu -- HLL, ELL and CSR device matrix objects, their
+// host<->device copies, the COO->HLL / COO->ELL device scatter kernels and
+// the device-side CSR->HLL builder.
+//
+// Replaces cuda/hlldev.c:34-540, cuda/elldev.c, the CSRG glue of
+// cuda/fcusparse_fct.h and cuda/CUDA/psi_cuda_CopyCooTo{Hlg,Elg}.cuh.
+#include "psbx_internal.cuh"
+
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+int psbx_csr_partition(int m, const int *irp, int base, int *rowBlocks, int *nBlocks, int *longRows, int *nLong);
+
+static inline size_t vsize(int t) { return t == SPGPU_TYPE_FLOAT ? 4 : 8; }
+
+static int dmalloc(void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return psbx_cuda_status(e, "cudaMalloc");
+  }
+  return SPGPU_SUCCESS;
+}
+
+static int h2d(void *d, const void *h, size_t bytes) {
+  if (!bytes) return SPGPU_SUCCESS;
+  if (!d || !h) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  PSBX_CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c.stream));
+  return SPGPU_SUCCESS;
+}
+
+static int d2h(void *h, const void *d, size_t bytes) {
+  if (!bytes) return SPGPU_SUCCESS;
+  if (!d || !h) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  PSBX_CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c.stream));
+  return SPGPU_SUCCESS;
+}
+
+static int sync_stream() {
+  PSBX_CK(cudaStreamSynchronize(psbx_ctx().stream));
+  return SPGPU_SUCCESS;
+}
+
+// ============================================================== HLL objects
+extern "C" {
+
+int FallocHllDevice(void **deviceMat, unsigned hksize, unsigned rows, unsigned nzeros, unsigned allocsize,
+                    unsigned elementType, unsigned firstIndex) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!deviceMat || hksize == 0) return SPGPU_UNSUPPORTED;
+  if (elementType != SPGPU_TYPE_DOUBLE && elementType != SPGPU_TYPE_FLOAT) return SPGPU_UNSUPPORTED;
+  HllDevice *m = (HllDevice *)calloc(1, sizeof(HllDevice));
+  m->hackSize = (int)hksize;
+  m->rows = (int)rows;
+  m->nzt = (int)nzeros;
+  m->allocsize = (int)allocsize;
+  m->avgNzr = rows ? (int)((nzeros + rows - 1) / rows) : 0;  // hlldev.c:45
+  m->baseIndex = (int)firstIndex;
+  m->hackOffsLength = (int)((rows + hksize - 1) / hksize);
+  m->elemType = (int)elementType;
+  m->cols = (int)rows;
+  m->maxRowLen = -1;
+  rc = dmalloc((void **)&m->rP, sizeof(int) * (size_t)allocsize);
+  if (!rc) rc = dmalloc((void **)&m->rS, sizeof(int) * (size_t)rows);
+  if (!rc) rc = dmalloc((void **)&m->diag, sizeof(int) * (size_t)rows);
+  if (!rc) rc = dmalloc((void **)&m->hackOffs, sizeof(int) * (size_t)(m->hackOffsLength + 1));
+  if (!rc) rc = dmalloc(&m->cM, vsize(m->elemType) * (size_t)allocsize);
+  if (rc) {
+    cudaFree(m->rP); cudaFree(m->rS); cudaFree(m->diag); cudaFree(m->hackOffs); cudaFree(m->cM);
+    free(m);
+    *deviceMat = nullptr;
+    return rc;
+  }
+  *deviceMat = m;
+  return SPGPU_SUCCESS;
+}
+
+void freeHllDevice(void *deviceMat) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m) return;
+  cudaStreamSynchronize(psbx_ctx().stream);
+  cudaFree(m->rP);
+  cudaFree(m->rS);
+  cudaFree(m->diag);
+  cudaFree(m->hackOffs);
+  cudaFree(m->cM);
+  if (m->cM32) cudaFree(m->cM32);
+  if (m->perm) cudaFree(m->perm);
+  free(m);
+}
+
+int getHllDeviceParams(void *deviceMat, int *hksize, int *rows, int *nzeros, int *allocsize, int *hackOffsLength,
+                       int *firstIndex, int *avgnzr) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m) return SPGPU_UNSUPPORTED;
+  *hackOffsLength = m->hackOffsLength;
+  *hksize = m->hackSize;
+  *nzeros = m->nzt;
+  *allocsize = m->allocsize;
+  *rows = m->rows;
+  *avgnzr = m->avgNzr;
+  *firstIndex = m->baseIndex;
+  return SPGPU_SUCCESS;
+}
+
+static int hll_copy(void *deviceMat, void *val, int *ja, int *hkoffs, int *irn, int *idiag, bool write, int type) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m || m->elemType != type) return SPGPU_UNSUPPORTED;
+  size_t as = (size_t)m->allocsize, nr = (size_t)m->rows, nh = (size_t)m->hackOffsLength + 1;
+  int rc;
+  if (write) {
+    rc = h2d(m->cM, val, as * vsize(type));
+    if (!rc) rc = h2d(m->rP, ja, as * sizeof(int));
+    if (!rc) rc = h2d(m->rS, irn, nr * sizeof(int));
+    if (!rc) rc = h2d(m->diag, idiag, nr * sizeof(int));
+    if (!rc) rc = h2d(m->hackOffs, hkoffs, nh * sizeof(int));
+    if (!rc && irn) {
+      int mx = 0;
+      for (size_t i = 0; i < nr; i++) mx = irn[i] > mx ? irn[i] : mx;
+      m->maxRowLen = mx;
+    }
+  } else {
+    rc = d2h(val, m->cM, as * vsize(type));
+    if (!rc) rc = d2h(ja, m->rP, as * sizeof(int));
+    if (!rc) rc = d2h(irn, m->rS, nr * sizeof(int));
+    if (!rc) rc = d2h(idiag, m->diag, nr * sizeof(int));
+    if (!rc) rc = d2h(hkoffs, m->hackOffs, nh * sizeof(int));
+  }
+  if (!rc) rc = sync_stream();
+  return rc;
+}
+
+int writeHllDeviceDouble(void *deviceMat, double *val, int *ja, int *hkoffs, int *irn, int *idiag) {
+  return hll_copy(deviceMat, val, ja, hkoffs, irn, idiag, true, SPGPU_TYPE_DOUBLE);
+}
+int readHllDeviceDouble(void *deviceMat, double *val, int *ja, int *hkoffs, int *irn, int *idiag) {
+  return hll_copy(deviceMat, val, ja, hkoffs, irn, idiag, false, SPGPU_TYPE_DOUBLE);
+}
+int writeHllDeviceFloat(void *deviceMat, float *val, int *ja, int *hkoffs, int *irn, int *idiag) {
+  return hll_copy(deviceMat, val, ja, hkoffs, irn, idiag, true, SPGPU_TYPE_FLOAT);
+}
+int readHllDeviceFloat(void *deviceMat, float *val, int *ja, int *hkoffs, int *irn, int *idiag) {
+  return hll_copy(deviceMat, val, ja, hkoffs, irn, idiag, false, SPGPU_TYPE_FLOAT);
+}
+
+int spmvHllDeviceDouble(void *deviceMat, double alpha, void *deviceX, double beta, void *deviceY) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  MultiVectDevice *x = (MultiVectDevice *)deviceX, *y = (MultiVectDevice *)deviceY;
+  if (!m || !x || !y || y->size_ < m->rows) return SPGPU_UNSUPPORTED;
+  if (x->elemType != SPGPU_TYPE_DOUBLE || y->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  for (int v = 0; v < y->count_ && v < x->count_; v++) {
+    int rc = psbx_launch_hll_spmv(m, alpha, (const double *)x->v_ + (size_t)v * x->pitch_, beta,
+                                  (double *)y->v_ + (size_t)v * y->pitch_, c.stream);
+    if (rc) return rc;
+  }
+  return SPGPU_SUCCESS;
+}
+
+int spmvHllDeviceFloat(void *deviceMat, float alpha, void *deviceX, float beta, void *deviceY) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  MultiVectDevice *x = (MultiVectDevice *)deviceX, *y = (MultiVectDevice *)deviceY;
+  if (!m || !x || !y || y->size_ < m->rows) return SPGPU_UNSUPPORTED;
+  if (x->elemType != SPGPU_TYPE_FLOAT || y->elemType != SPGPU_TYPE_FLOAT) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  for (int v = 0; v < y->count_ && v < x->count_; v++) {
+    int rc = psbx_launch_hll_spmv_f32(m, alpha, (const float *)x->v_ + (size_t)v * x->pitch_, beta,
+                                      (float *)y->v_ + (size_t)v * y->pitch_, c.stream);
+    if (rc) return rc;
+  }
+  return SPGPU_SUCCESS;
+}
+
+int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x, double beta, double *y) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m) return SPGPU_UNSUPPORTED;
+  return psbx_launch_hll_spmv(m, alpha, x, beta, y, psbx_ctx().stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------- COO -> HLL scatter (device)
+// psi_cuda_CopyCooToHlg.cuh:28-68: one thread per row copies the row's COO
+// run into the column-major hack slice; padding takes the column of the
+// first entry of row 2 and value 0; idiag = 1-based diagonal position.
+// Rows past nr in the last hack (not written by the reference) get the same
+// padding so the whole allocation is defined.
+template <class T>
+__global__ void k_coo_to_hll(int nr, int hksz, int base, int nrpad, const int *__restrict__ rS,
+                             const int *__restrict__ hackOffs, const int *__restrict__ idisp,
+                             const int *__restrict__ cja, const T *__restrict__ cval, int jc,
+                             int *__restrict__ idiag, int *__restrict__ rP, T *__restrict__ cM) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nrpad) return;
+  const int h = i / hksz, lane = i - h * hksz;
+  const int nzm = (hackOffs[h + 1] - hackOffs[h]) / hksz;
+  size_t ir = (size_t)hackOffs[h] + lane;
+  int rsz = 0, idval = 0;
+  if (i < nr) {
+    rsz = rS[i];
+    const int p0 = idisp[i];
+    for (int k = 0; k < rsz; k++) {
+      const int c = cja[p0 + k];
+      cM[ir] = cval[p0 + k];
+      if (c == i + base) idval = k + base;
+      rP[ir] = c;
+      ir += hksz;
+    }
+    idiag[i] = idval;
+  }
+  for (int k = rsz; k < nzm; k++) {
+    rP[ir] = jc;
+    cM[ir] = T(0);
+    ir += hksz;
+  }
+}
+
+extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int noffs, int isz, int *irn, int *hoffs,
+                                     int *idisp, int *ja, double *val, void *deviceMat) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m || m->elemType != SPGPU_TYPE_DOUBLE || m->rows != nr || m->hackSize != hacksz) return SPGPU_UNSUPPORTED;
+  if (noffs != m->hackOffsLength || isz > m->allocsize) return SPGPU_UNSUPPORTED;
+  (void)nc;
+  PsbxCtx &c = psbx_ctx();
+  int *dIdisp = nullptr, *dJa = nullptr;
+  double *dVal = nullptr;
+  int rc = dmalloc((void **)&dIdisp, sizeof(int) * (size_t)(nr + 1));
+  if (!rc) rc = dmalloc((void **)&dJa, sizeof(int) * (size_t)nza);
+  if (!rc) rc = dmalloc((void **)&dVal, sizeof(double) * (size_t)nza);
+  if (!rc) rc = h2d(dVal, val, sizeof(double) * (size_t)nza);
+  if (!rc) rc = h2d(dJa, ja, sizeof(int) * (size_t)nza);
+  if (!rc) rc = h2d(m->rS, irn, sizeof(int) * (size_t)nr);
+  if (!rc) rc = h2d(m->hackOffs, hoffs, sizeof(int) * (size_t)(noffs + 1));
+  if (!rc) rc = h2d(dIdisp, idisp, sizeof(int) * (size_t)(nr + 1));
+  if (!rc && nr > 0) {
+    // "pick one valid value" (psi_cuda_CopyCooToHlg.cuh:57-59): column of
+    // entry idisp(2); guarded for one-row matrices.
+    int jc = 1;
+    if (nza > 0) jc = ja[(nr > 1 && idisp[1] < nza) ? idisp[1] : 0];
+    const int nrpad = noffs * hacksz;
+    const int T = 256;
+    k_coo_to_hll<double><<<(nrpad + T - 1) / T, T, 0, c.stream>>>(nr, hacksz, m->baseIndex, nrpad, m->rS,
+                                                                  m->hackOffs, dIdisp, dJa, dVal, jc, m->diag,
+                                                                  m->rP, (double *)m->cM);
+    psbx_count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "k_coo_to_hll");
+    int mx = 0;
+    for (int i = 0; i < nr; i++) mx = irn[i] > mx ? irn[i] : mx;
+    m->maxRowLen = mx;
+  }
+  if (!rc) rc = sync_stream();
+  cudaFree(dIdisp);
+  cudaFree(dJa);
+  cudaFree(dVal);
+  return rc;
+}
+
+// ------------------------------------------------ CSR (device) -> HLL build
+// Restates psi_d_convert_hll_from_coo.f90:31-122 / psi_d_xtr_ell_from_coo
+// on the device: irn from irp, hack widths = max irn in the hack, hkoffs by
+// an exclusive scan, then one block per hack fills the column-major slice.
+// Padding is the CPU converter's: last stored column of the row (the hack's
+// first stored column for an empty row), value 0; rows past nr in the last
+// hack: column nr, value 0 (psi_d_convert_hll_from_coo.f90:94-96).
+// With perm, storage row s of the layout holds matrix row perm[s].
+__global__ void k_hll_widths(int nr, int hksz, const int *__restrict__ irp, const int *__restrict__ perm,
+                             int *__restrict__ irn, int *__restrict__ width, int nhacks) {
+  const int h = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (h >= nhacks) return;
+  int mx = 0;
+  for (int ii = lane; ii < hksz; ii += 32) {
+    const int s = h * hksz + ii;
+    if (s < nr) {
+      const int r = perm ? perm[s] : s;
+      const int len = irp[r + 1] - irp[r];
+      irn[s] = len;
+      mx = max(mx, len);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  if (lane == 0) width[h] = mx;
+}
+
+// Single-block exclusive scan of width[0..n) * hksz into offs[0..n], 64-bit
+// accumulation; flags overflow of the int32 offsets the format uses.
+__global__ void k_scan_offsets(int n, int hksz, const int *__restrict__ width, int *__restrict__ offs,
+                               long long *__restrict__ total) {
+  __shared__ long long warp_tot[32];
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < n; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    long long v = i < n ? (long long)width[i] * hksz : 0;
+    long long incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      long long t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      long long t = lane < nw ? warp_tot[lane] : 0;
+      long long it = t;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        long long u = __shfl_up_sync(0xffffffffu, it, o);
+        if (lane >= o) it += u;
+      }
+      if (lane < nw) warp_tot[lane] = it - t;  // exclusive warp prefix
+    }
+    __syncthreads();
+    const long long excl = carry + warp_tot[wid] + incl - v;
+    if (i < n) offs[i] = (int)excl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    offs[n] = (int)carry;
+    *total = carry;
+  }
+}
+
+__global__ void k_hll_fill(int nr, int hksz, int base, const int *__restrict__ irp, const int *__restrict__ cja,
+                           const double *__restrict__ cval, const int *__restrict__ perm,
+                           const int *__restrict__ irn, const int *__restrict__ hkoffs, int *__restrict__ hja,
+                           double *__restrict__ hval, int *__restrict__ idiag) {
+  const int h = blockIdx.x;
+  const int off = hkoffs[h];
+  const int width = (hkoffs[h + 1] - off) / hksz;
+  if (width == 0) {
+    for (int ii = threadIdx.x; ii < hksz; ii += blockDim.x) {
+      const int s = h * hksz + ii;
+      if (s < nr) idiag[s] = 0;
+    }
+    return;
+  }
+  // first stored column of the hack (jac(1) in psi_d_xtr_ell_from_coo.f90:57)
+  __shared__ int first_col;
+  if (threadIdx.x == 0) {
+    int fc = nr;  // unused when every row of the hack is empty (width 0)
+    for (int ii = 0; ii < hksz; ii++) {
+      const int s = h * hksz + ii;
+      if (s >= nr) break;
+      const int r = perm ? perm[s] : s;
+      if (irp[r + 1] > irp[r]) {
+        fc = cja[irp[r] - base];
+        break;
+      }
+    }
+    first_col = fc;
+  }
+  __syncthreads();
+  const long long total = (long long)width * hksz;
+  for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+    const int j = (int)(e / hksz), ii = (int)(e - (long long)j * hksz);
+    const int s = h * hksz + ii;
+    int col;
+    double v;
+    if (s < nr) {
+      const int r = perm ? perm[s] : s;
+      const int len = irn[s];
+      const int p0 = irp[r] - base;
+      if (j < len) {
+        col = cja[p0 + j];
+        v = cval[p0 + j];
+        if (col == r + base) idiag[s] = j + 1;
+      } else {
+        col = len > 0 ? cja[p0 + len - 1] : first_col;
+        v = 0.0;
+      }
+    } else {
+      col = nr;
+      v = 0.0;
+    }
+    hja[(size_t)off + e] = col;
+    hval[(size_t)off + e] = v;
+  }
+}
+
+__global__ void k_zero_int(int n, int *__restrict__ p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
+}
+
+extern "C" int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, int nnz, const int *d_irp,
+                                        const int *d_ja, const double *d_val, int hksz, const int *d_perm) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!deviceMat || rows < 0 || hksz <= 0 || !d_irp) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  const int nh = (rows + hksz - 1) / hksz;
+  int *width = nullptr, *irn = nullptr, *hk = nullptr;
+  long long *dtot = nullptr;
+  rc = dmalloc((void **)&width, sizeof(int) * (size_t)(nh + 1));
+  if (!rc) rc = dmalloc((void **)&irn, sizeof(int) * (size_t)(rows + 1));
+  if (!rc) rc = dmalloc((void **)&hk, sizeof(int) * (size_t)(nh + 1));
+  if (!rc) rc = dmalloc((void **)&dtot, sizeof(long long));
+  long long total = 0;
+  if (!rc && nh > 0) {
+    k_hll_widths<<<(nh + 7) / 8, 256, 0, c.stream>>>(rows, hksz, d_irp, d_perm, irn, width, nh);
+    k_scan_offsets<<<1, 1024, 0, c.stream>>>(nh, hksz, width, hk, dtot);
+    psbx_count_launch(2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "hll widths/scan");
+    if (!rc) rc = d2h(&total, dtot, sizeof(long long));
+    if (!rc) rc = sync_stream();
+  }
+  if (!rc && total > 0x7fffffffLL) rc = SPGPU_UNSUPPORTED;  // int32 offsets, as psb_ipk_
+  HllDevice *m = nullptr;
+  if (!rc) rc = FallocHllDevice((void **)&m, (unsigned)hksz, (unsigned)rows, (unsigned)nnz, (unsigned)total,
+                                SPGPU_TYPE_DOUBLE, 1);
+  if (!rc) {
+    m->cols = cols;
+    // the builder's own buffers become the object's irn / hkoffs
+    cudaFree(m->rS);
+    cudaFree(m->hackOffs);
+    m->rS = irn;
+    m->hackOffs = hk;
+    irn = nullptr;
+    hk = nullptr;
+    if (d_perm) {
+      rc = dmalloc((void **)&m->perm, sizeof(int) * (size_t)rows);
+      if (!rc) PSBX_CK(cudaMemcpyAsync(m->perm, d_perm, sizeof(int) * (size_t)rows, cudaMemcpyDeviceToDevice, c.stream));
+    }
+  }
+  if (!rc && nh > 0) {
+    k_zero_int<<<psbx_grid_for(rows, 256), 256, 0, c.stream>>>(rows, m->diag);
+    k_hll_fill<<<nh, 256, 0, c.stream>>>(rows, hksz, 1, d_irp, d_ja, d_val, m->perm, m->rS, m->hackOffs, m->rP,
+                                        (double *)m->cM, m->diag);
+    psbx_count_launch(2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "k_hll_fill");
+  }
+  if (!rc) {
+    // longest row, for the solver's choice of kernels
+    std::vector<int> hw(nh > 0 ? nh : 1);
+    if (nh > 0) rc = d2h(hw.data(), width, sizeof(int) * (size_t)nh);
+    if (!rc) rc = sync_stream();
+    int mx = 0;
+    for (int h = 0; h < nh; h++) mx = hw[h] > mx ? hw[h] : mx;
+    if (m) m->maxRowLen = mx;
+  }
+  cudaFree(width);
+  cudaFree(irn);
+  cudaFree(hk);
+  cudaFree(dtot);
+  if (rc) {
+    if (m) freeHllDevice(m);
+    *deviceMat = nullptr;
+    return rc;
+  }
+  *deviceMat = m;
+  return SPGPU_SUCCESS;
+}
+
+__global__ void k_d2f(size_t n, const double *__restrict__ a, float *__restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+extern "C" int psbx_hll_make_single(void *deviceMat) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m || m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  if (m->cM32) return SPGPU_SUCCESS;
+  int rc = dmalloc((void **)&m->cM32, sizeof(float) * (size_t)m->allocsize);
+  if (rc) return rc;
+  PsbxCtx &c = psbx_ctx();
+  k_d2f<<<psbx_grid_for(m->allocsize, 256), 256, 0, c.stream>>>((size_t)m->allocsize, (const double *)m->cM, m->cM32);
+  PSBX_LAUNCH_CK("k_d2f");
+  return sync_stream();
+}
+
+// ============================================================== ELL objects
+static int ell_pitch(int rows) { return ((rows + 31) / 32) * 32; }  // spgpu/ell.c:33-37
+
+extern "C" {
+
+int FallocEllDevice(void **deviceMat, unsigned rows, unsigned maxRowSize, unsigned nnzeros, unsigned columns,
+                    unsigned elementType, unsigned firstIndex) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!deviceMat) return SPGPU_UNSUPPORTED;
+  if (elementType != SPGPU_TYPE_DOUBLE && elementType != SPGPU_TYPE_FLOAT) return SPGPU_UNSUPPORTED;
+  EllDevice *m = (EllDevice *)calloc(1, sizeof(EllDevice));
+  m->rows = (int)rows;
+  m->cMPitch = ell_pitch((int)rows);
+  m->rPPitch = m->cMPitch;
+  m->pitch = m->cMPitch;
+  m->maxRowSize = (int)maxRowSize;
+  m->avgRowSize = rows ? (int)((nnzeros + rows - 1) / rows) : 0;
+  m->allocsize = m->maxRowSize * m->pitch;
+  m->columns = (int)columns;
+  m->baseIndex = (int)firstIndex;
+  m->dataType = (int)elementType;
+  rc = dmalloc((void **)&m->rS, sizeof(int) * (size_t)rows);
+  if (!rc) rc = dmalloc((void **)&m->diag, sizeof(int) * (size_t)rows);
+  if (!rc) rc = dmalloc((void **)&m->rP, sizeof(int) * (size_t)m->allocsize);
+  if (!rc) rc = dmalloc(&m->cM, vsize(m->dataType) * (size_t)m->allocsize);
+  if (rc) {
+    cudaFree(m->rS); cudaFree(m->diag); cudaFree(m->rP); cudaFree(m->cM);
+    free(m);
+    *deviceMat = nullptr;
+    return rc;
+  }
+  *deviceMat = m;
+  return SPGPU_SUCCESS;
+}
+
+void freeEllDevice(void *deviceMat) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  if (!m) return;
+  cudaStreamSynchronize(psbx_ctx().stream);
+  cudaFree(m->rS);
+  cudaFree(m->diag);
+  cudaFree(m->rP);
+  cudaFree(m->cM);
+  free(m);
+}
+
+void zeroEllDevice(void *deviceMat) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  if (!m) return;
+  cudaMemsetAsync(m->cM, 0, vsize(m->dataType) * (size_t)m->allocsize, psbx_ctx().stream);
+  cudaStreamSynchronize(psbx_ctx().stream);
+}
+
+int getEllDevicePitch(void *deviceMat) { return ((EllDevice *)deviceMat)->pitch; }
+int getEllDeviceMaxRowSize(void *deviceMat) { return ((EllDevice *)deviceMat)->maxRowSize; }
+
+static int ell_copy(void *deviceMat, double *val, int *ja, int ldj, int *irn, int *idiag, bool write) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  if (!m || m->dataType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  if (ldj != m->pitch) return SPGPU_UNSUPPORTED;  // host arrays must be pitch x maxRowSize
+  size_t as = (size_t)m->allocsize, nr = (size_t)m->rows;
+  int rc;
+  if (write) {
+    rc = h2d(m->cM, val, as * 8);
+    if (!rc) rc = h2d(m->rP, ja, as * 4);
+    if (!rc) rc = h2d(m->rS, irn, nr * 4);
+    if (!rc) rc = h2d(m->diag, idiag, nr * 4);
+  } else {
+    rc = d2h(val, m->cM, as * 8);
+    if (!rc) rc = d2h(ja, m->rP, as * 4);
+    if (!rc) rc = d2h(irn, m->rS, nr * 4);
+    if (!rc) rc = d2h(idiag, m->diag, nr * 4);
+  }
+  if (!rc) rc = sync_stream();
+  return rc;
+}
+
+int writeEllDeviceDouble(void *deviceMat, double *val, int *ja, int ldj, int *irn, int *idiag) {
+  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, true);
+}
+int readEllDeviceDouble(void *deviceMat, double *val, int *ja, int ldj, int *irn, int *idiag) {
+  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, false);
+}
+
+int spmvEllDeviceDouble(void *deviceMat, double alpha, void *deviceX, double beta, void *deviceY) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  MultiVectDevice *x = (MultiVectDevice *)deviceX, *y = (MultiVectDevice *)deviceY;
+  if (!m || !x || !y || y->size_ < m->rows) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  for (int v = 0; v < y->count_ && v < x->count_; v++) {
+    int rc = psbx_launch_ell_spmv(m, alpha, (const double *)x->v_ + (size_t)v * x->pitch_, beta,
+                                  (double *)y->v_ + (size_t)v * y->pitch_, c.stream);
+    if (rc) return rc;
+  }
+  return SPGPU_SUCCESS;
+}
+
+}  // extern "C"
+
+// COO -> ELL scatter on the device (psi_cuda_CopyCooToElg.cuh): padding as
+// the CPU converter (last column of the row; first COO column if empty).
+__global__ void k_coo_to_ell(int nr, int nzm, int pitch, int base, const int *__restrict__ rS,
+                             const int *__restrict__ idisp, const int *__restrict__ cja,
+                             const double *__restrict__ cval, int *__restrict__ idiag, int *__restrict__ rP,
+                             double *__restrict__ cM) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pitch) return;
+  if (i >= nr) {
+    for (int k = 0; k < nzm; k++) {
+      rP[(size_t)k * pitch + i] = 1;
+      cM[(size_t)k * pitch + i] = 0.0;
+    }
+    return;
+  }
+  const int rsz = rS[i], p0 = idisp[i];
+  int idval = 0, c = cja[0];
+  for (int k = 0; k < rsz; k++) {
+    c = cja[p0 + k];
+    if (c == i + base) idval = k + base;
+    rP[(size_t)k * pitch + i] = c;
+    cM[(size_t)k * pitch + i] = cval[p0 + k];
+  }
+  for (int k = rsz; k < nzm; k++) {
+    rP[(size_t)k * pitch + i] = c;
+    cM[(size_t)k * pitch + i] = 0.0;
+  }
+  idiag[i] = idval;
+}
+
+extern "C" int psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ldv, int nzm, int *irn, int *idisp,
+                                     int *ja, double *val, void *deviceMat) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  (void)nc; (void)hacksz; (void)ldv;
+  if (!m || m->dataType != SPGPU_TYPE_DOUBLE || m->rows != nr || nzm > m->maxRowSize) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  int *dIdisp = nullptr, *dJa = nullptr;
+  double *dVal = nullptr;
+  int rc = dmalloc((void **)&dIdisp, sizeof(int) * (size_t)(nr + 1));
+  if (!rc) rc = dmalloc((void **)&dJa, sizeof(int) * (size_t)(nza > 0 ? nza : 1));
+  if (!rc) rc = dmalloc((void **)&dVal, sizeof(double) * (size_t)(nza > 0 ? nza : 1));
+  if (!rc) rc = h2d(dVal, val, sizeof(double) * (size_t)nza);
+  if (!rc) rc = h2d(dJa, ja, sizeof(int) * (size_t)nza);
+  if (!rc) rc = h2d(m->rS, irn, sizeof(int) * (size_t)nr);
+  if (!rc) rc = h2d(dIdisp, idisp, sizeof(int) * (size_t)(nr + 1));
+  if (!rc && nza == 0) {
+    int one = 1;
+    rc = h2d(dJa, &one, sizeof(int));
+  }
+  if (!rc && m->pitch > 0) {
+    k_coo_to_ell<<<(m->pitch + 255) / 256, 256, 0, c.stream>>>(nr, m->maxRowSize, m->pitch, m->baseIndex, m->rS,
+                                                               dIdisp, dJa, dVal, m->diag, m->rP, (double *)m->cM);
+    psbx_count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "k_coo_to_ell");
+  }
+  if (!rc) rc = sync_stream();
+  cudaFree(dIdisp);
+  cudaFree(dJa);
+  cudaFree(dVal);
+  return rc;
+}
+
+// ============================================================== CSR objects
+static CsrDevice *CM(psbx_d_Cmat *M) { return M ? (CsrDevice *)M->mat : nullptr; }
+
+static void csr_free_arrays(CsrDevice *m) {
+  cudaFree(m->val);
+  cudaFree(m->irp);
+  cudaFree(m->ja);
+  if (m->rowBlocks) cudaFree(m->rowBlocks);
+  if (m->longRows) cudaFree(m->longRows);
+  m->val = nullptr; m->irp = nullptr; m->ja = nullptr; m->rowBlocks = nullptr; m->longRows = nullptr;
+}
+
+extern "C" {
+
+int d_CSRGDeviceAlloc(psbx_d_Cmat *Mat, int nr, int nc, int nz) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!Mat || nr < 0 || nz < 0) return SPGPU_UNSUPPORTED;
+  if (Mat->mat) d_CSRGDeviceFree(Mat);
+  CsrDevice *m = (CsrDevice *)calloc(1, sizeof(CsrDevice));
+  m->m = nr;
+  m->n = nc;
+  m->nz = nz;
+  m->baseIndex = 1;
+  rc = dmalloc((void **)&m->irp, sizeof(int) * (size_t)(nr + 1));
+  if (!rc) rc = dmalloc((void **)&m->ja, sizeof(int) * (size_t)nz);
+  if (!rc) rc = dmalloc((void **)&m->val, sizeof(double) * (size_t)nz);
+  if (rc) {
+    csr_free_arrays(m);
+    free(m);
+    return rc;
+  }
+  Mat->mat = m;
+  return SPGPU_SUCCESS;
+}
+
+int d_CSRGDeviceFree(psbx_d_Cmat *Mat) {
+  CsrDevice *m = CM(Mat);
+  if (!m) return SPGPU_SUCCESS;
+  cudaStreamSynchronize(psbx_ctx().stream);
+  csr_free_arrays(m);
+  free(m);
+  Mat->mat = nullptr;
+  return SPGPU_SUCCESS;
+}
+
+int d_CSRGDeviceGetParms(psbx_d_Cmat *Mat, int *nr, int *nc, int *nz) {
+  CsrDevice *m = CM(Mat);
+  if (!m) return SPGPU_UNSUPPORTED;
+  *nr = m->m;
+  *nc = m->n;
+  *nz = m->nz;
+  return SPGPU_SUCCESS;
+}
+
+// Matrix type / fill mode / diag type only matter for the triangular solve
+// (spsv), which is outside this library; accepted and ignored.
+int d_CSRGDeviceSetMatType(psbx_d_Cmat *Mat, int type) { (void)type; return CM(Mat) ? 0 : SPGPU_UNSUPPORTED; }
+int d_CSRGDeviceSetMatFillMode(psbx_d_Cmat *Mat, int type) { (void)type; return CM(Mat) ? 0 : SPGPU_UNSUPPORTED; }
+int d_CSRGDeviceSetMatDiagType(psbx_d_Cmat *Mat, int type) { (void)type; return CM(Mat) ? 0 : SPGPU_UNSUPPORTED; }
+int d_CSRGDeviceSetMatIndexBase(psbx_d_Cmat *Mat, int type) {
+  CsrDevice *m = CM(Mat);
+  if (!m || (type != 0 && type != 1)) return SPGPU_UNSUPPORTED;
+  m->baseIndex = type;
+  return SPGPU_SUCCESS;
+}
+
+int d_CSRGHost2Device(psbx_d_Cmat *Mat, int m_, int n, int nz, int *irp, int *ja, double *val) {
+  CsrDevice *m = CM(Mat);
+  if (!m || m_ != m->m || nz > m->nz || !irp) return SPGPU_UNSUPPORTED;
+  (void)n;
+  int rc = h2d(m->irp, irp, sizeof(int) * (size_t)(m_ + 1));
+  if (!rc) rc = h2d(m->ja, ja, sizeof(int) * (size_t)nz);
+  if (!rc) rc = h2d(m->val, val, sizeof(double) * (size_t)nz);
+  if (rc) return rc;
+  // row blocks for the streaming kernel
+  std::vector<int> blocks(2 * (size_t)(m_ > 0 ? m_ : 1)), longr(m_ > 0 ? m_ : 1);
+  std::vector<int> irp0(irp, irp + m_ + 1);
+  int nb = 0, nl = 0;
+  psbx_csr_partition(m_, irp0.data(), m->baseIndex, blocks.data(), &nb, longr.data(), &nl);
+  if (m->rowBlocks) cudaFree(m->rowBlocks);
+  if (m->longRows) cudaFree(m->longRows);
+  m->rowBlocks = nullptr;
+  m->longRows = nullptr;
+  rc = dmalloc((void **)&m->rowBlocks, sizeof(int) * (size_t)(2 * nb + 2));
+  if (!rc) rc = dmalloc((void **)&m->longRows, sizeof(int) * (size_t)(nl + 1));
+  if (!rc) rc = h2d(m->rowBlocks, blocks.data(), sizeof(int) * (size_t)(2 * nb));
+  if (!rc) rc = h2d(m->longRows, longr.data(), sizeof(int) * (size_t)nl);
+  m->nBlocks = nb;
+  m->nLong = nl;
+  int mx = 0;
+  for (int i = 0; i < m_; i++) mx = irp[i + 1] - irp[i] > mx ? irp[i + 1] - irp[i] : mx;
+  m->maxRowLen = mx;
+  if (!rc) rc = sync_stream();
+  return rc;
+}
+
+int d_CSRGDevice2Host(psbx_d_Cmat *Mat, int m_, int n, int nz, int *irp, int *ja, double *val) {
+  CsrDevice *m = CM(Mat);
+  if (!m || m_ != m->m || nz > m->nz) return SPGPU_UNSUPPORTED;
+  (void)n;
+  int rc = d2h(irp, m->irp, sizeof(int) * (size_t)(m_ + 1));
+  if (!rc) rc = d2h(ja, m->ja, sizeof(int) * (size_t)nz);
+  if (!rc) rc = d2h(val, m->val, sizeof(double) * (size_t)nz);
+  if (!rc) rc = sync_stream();
+  return rc;
+}
+
+int d_spmvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX, double beta, void *deviceY) {
+  CsrDevice *m = CM(Mat);
+  MultiVectDevice *x = (MultiVectDevice *)deviceX, *y = (MultiVectDevice *)deviceY;
+  if (!m || !x || !y || y->size_ < m->m) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  for (int v = 0; v < y->count_ && v < x->count_; v++) {
+    int rc = psbx_launch_csr_spmv(m, alpha, (const double *)x->v_ + (size_t)v * x->pitch_, beta,
+                                  (double *)y->v_ + (size_t)v * y->pitch_, c.stream);
+    if (rc) return rc;
+  }
+  return SPGPU_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,251 @@
+// psbx_spmv.cu -- sparse matrix-vector kernels y = alpha*A*x + beta*y for
+// the HLL, ELL and CSR device formats (sm_100a).
+//
+// Replaces cuda/spgpu/kernels/hell_spmv_base_template.cuh (spgpuDhellspmv),
+// ell_spmv_base_template.cuh (spgpuDellspmv) and the cuSPARSE call of
+// cuda/fcusparse_fct.h:108-124 (CSRG).
+//
+// HLL / ELL: one thread per row, a warp per 32 consecutive rows of a hack.
+// Entry j of the 32 rows of a warp is one contiguous 256-byte run of values
+// and 128-byte run of indices, so every value/index load instruction of the
+// warp is fully coalesced; they are read with the streaming (evict-first)
+// policy so that the gathered x stays cached.  Each row accumulates its
+// stored entries in order with a rounded multiply and a rounded add, which
+// is the reference's `acc = acc + val*x(ja)` (psb_d_hll_csmv.f90:345-360)
+// bit for bit; padding slots are not read (rows stop at irn).
+//
+// CSR: a block takes a run of whole rows holding at most CSR_TILE entries
+// (the row blocks are built at upload).  Its threads load the run's values
+// and indices coalesced, form the products val*x(ja) and park them in shared
+// memory; then one thread per row adds its products in stored order -- the
+// same bits as the reference's row loop.  Rows longer than CSR_TILE go to a
+// warp-per-row kernel whose shuffle-tree sum differs from the sequential sum
+// only by rounding (checked against a tolerance).
+#include "psbx_internal.cuh"
+
+#define SPMV_T 256
+#define CSR_TILE 2048
+#define CSR_ROWS 256
+
+HllView hll_view(const HllDevice *m) {
+  HllView v;
+  v.val = (const double *)m->cM;
+  v.ja = m->rP;
+  v.irn = m->rS;
+  v.hkoffs = m->hackOffs;
+  v.perm = m->perm;
+  v.rows = m->rows;
+  v.hksz = m->hackSize;
+  v.base = m->baseIndex;
+  return v;
+}
+
+EllView ell_view(const EllDevice *m) {
+  EllView v;
+  v.val = (const double *)m->cM;
+  v.ja = m->rP;
+  v.irn = m->rS;
+  v.rows = m->rows;
+  v.pitch = m->pitch;
+  v.base = m->baseIndex;
+  return v;
+}
+
+CsrView csr_view(const CsrDevice *m) {
+  CsrView v;
+  v.val = m->val;
+  v.ja = m->ja;
+  v.irp = m->irp;
+  v.rows = m->m;
+  v.base = m->baseIndex;
+  return v;
+}
+
+// --------------------------------------------------------------- row kernels
+// MODE 0: y = alpha*acc + beta*y ; MODE 1: beta == 0, y not read.
+template <class View, int MODE>
+__global__ void __launch_bounds__(SPMV_T) k_spmv_rows(View A, double alpha, const double *__restrict__ x,
+                                                      double beta, double *__restrict__ y) {
+  const int s = blockIdx.x * SPMV_T + threadIdx.x;
+  if (s >= A.rows) return;
+  const double acc = row_dot(A, s, x);
+  const int r = out_row(A, s);
+  const double t = rmul(alpha, acc);
+  y[r] = MODE == 1 ? t : radd(t, rmul(beta, y[r]));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(SPMV_T) k_hll_spmv_f32(HllViewF A, float alpha, const float *__restrict__ x,
+                                                         float beta, float *__restrict__ y) {
+  const int s = blockIdx.x * SPMV_T + threadIdx.x;
+  if (s >= A.rows) return;
+  const float acc = (float)row_dot(A, s, x);
+  const int r = out_row(A, s);
+  const float t = rmulf(alpha, acc);
+  y[r] = MODE == 1 ? t : raddf(t, rmulf(beta, y[r]));
+}
+
+template <class View>
+static int launch_rows(const View &A, double alpha, const double *x, double beta, double *y, cudaStream_t st) {
+  if (A.rows <= 0) return SPGPU_SUCCESS;
+  if (alpha == 0.0) return psbx_launch_scale(A.rows, beta, y, st);
+  const int g = (A.rows + SPMV_T - 1) / SPMV_T;
+  if (beta == 0.0)
+    k_spmv_rows<View, 1><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  else
+    k_spmv_rows<View, 0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  PSBX_LAUNCH_CK("k_spmv_rows");
+  return SPGPU_SUCCESS;
+}
+
+int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, double beta, double *y,
+                         cudaStream_t st) {
+  if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  if (alpha == 0.0 && m->perm == nullptr) return psbx_launch_scale(m->rows, beta, y, st);
+  return launch_rows(hll_view(m), alpha, x, beta, y, st);
+}
+
+int psbx_launch_ell_spmv(const EllDevice *m, double alpha, const double *x, double beta, double *y,
+                         cudaStream_t st) {
+  if (m->dataType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  return launch_rows(ell_view(m), alpha, x, beta, y, st);
+}
+
+__global__ void k_f32_scale(int n, float beta, float *__restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = beta == 0.0f ? 0.0f : rmulf(beta, y[i]);
+}
+
+int psbx_launch_hll_spmv_f32(const HllDevice *m, float alpha, const float *x, float beta, float *y,
+                             cudaStream_t st) {
+  HllViewF A;
+  A.val = m->elemType == SPGPU_TYPE_FLOAT ? (const float *)m->cM : m->cM32;
+  if (!A.val) return SPGPU_UNSUPPORTED;
+  A.ja = m->rP;
+  A.irn = m->rS;
+  A.hkoffs = m->hackOffs;
+  A.perm = m->perm;
+  A.rows = m->rows;
+  A.hksz = m->hackSize;
+  A.base = m->baseIndex;
+  if (A.rows <= 0) return SPGPU_SUCCESS;
+  if (alpha == 0.0f) {
+    k_f32_scale<<<psbx_grid_for(A.rows, SPMV_T), SPMV_T, 0, st>>>(A.rows, beta, y);
+    PSBX_LAUNCH_CK("k_f32_scale");
+    return SPGPU_SUCCESS;
+  }
+  const int g = (A.rows + SPMV_T - 1) / SPMV_T;
+  if (beta == 0.0f)
+    k_hll_spmv_f32<1><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  else
+    k_hll_spmv_f32<0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  PSBX_LAUNCH_CK("k_hll_spmv_f32");
+  return SPGPU_SUCCESS;
+}
+
+// --------------------------------------------------------------- CSR stream
+// Block b holds rows rowBlocks[2b] .. rowBlocks[2b+1]-1; their entries (at
+// most CSR_TILE) are contiguous in val/ja.
+template <int MODE>
+__global__ void __launch_bounds__(SPMV_T) k_csr_stream(CsrView A, const int *__restrict__ rowBlocks, double alpha,
+                                                       const double *__restrict__ x, double beta,
+                                                       double *__restrict__ y) {
+  __shared__ double prod[CSR_TILE];
+  const int r0 = rowBlocks[2 * blockIdx.x], r1 = rowBlocks[2 * blockIdx.x + 1];
+  const int e0 = ld_ro(A.irp + r0) - A.base, e1 = ld_ro(A.irp + r1) - A.base;
+  const int ne = e1 - e0;
+  const double *xb = x - A.base;
+  for (int k = threadIdx.x; k < ne; k += SPMV_T) {
+    const int c = ld_stream(A.ja + e0 + k);
+    const double v = ld_stream(A.val + e0 + k);
+    prod[k] = rmul(v, ld_ro(xb + c));
+  }
+  __syncthreads();
+  const int r = r0 + threadIdx.x;
+  if (r < r1) {
+    const int b = ld_ro(A.irp + r) - A.base - e0, e = ld_ro(A.irp + r + 1) - A.base - e0;
+    double acc = 0.0;
+    for (int k = b; k < e; k++) acc = radd(acc, prod[k]);
+    const double t = rmul(alpha, acc);
+    y[r] = MODE == 1 ? t : radd(t, rmul(beta, y[r]));
+  }
+}
+
+// One warp per long row: per-lane partial sums, shuffle tree.
+template <int MODE>
+__global__ void __launch_bounds__(SPMV_T) k_csr_long(CsrView A, const int *__restrict__ rows, int nrows, double alpha,
+                                                     const double *__restrict__ x, double beta,
+                                                     double *__restrict__ y) {
+  const int w = (blockIdx.x * SPMV_T + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nrows) return;
+  const int r = rows[w];
+  const int b = ld_ro(A.irp + r) - A.base, e = ld_ro(A.irp + r + 1) - A.base;
+  const double *xb = x - A.base;
+  double acc = 0.0;
+  for (int k = b + lane; k < e; k += 32) acc = radd(acc, rmul(ld_stream(A.val + k), ld_ro(xb + ld_stream(A.ja + k))));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc = radd(acc, __shfl_down_sync(0xffffffffu, acc, o));
+  if (lane == 0) {
+    const double t = rmul(alpha, acc);
+    y[r] = MODE == 1 ? t : radd(t, rmul(beta, y[r]));
+  }
+}
+
+int psbx_launch_csr_spmv(const CsrDevice *m, double alpha, const double *x, double beta, double *y,
+                         cudaStream_t st) {
+  if (m->m <= 0) return SPGPU_SUCCESS;
+  if (alpha == 0.0) return psbx_launch_scale(m->m, beta, y, st);
+  CsrView A = csr_view(m);
+  if (m->nBlocks > 0) {
+    if (beta == 0.0)
+      k_csr_stream<1><<<m->nBlocks, SPMV_T, 0, st>>>(A, m->rowBlocks, alpha, x, beta, y);
+    else
+      k_csr_stream<0><<<m->nBlocks, SPMV_T, 0, st>>>(A, m->rowBlocks, alpha, x, beta, y);
+    PSBX_LAUNCH_CK("k_csr_stream");
+  }
+  if (m->nLong > 0) {
+    const int g = (m->nLong * 32 + SPMV_T - 1) / SPMV_T;
+    if (beta == 0.0)
+      k_csr_long<1><<<g, SPMV_T, 0, st>>>(A, m->longRows, m->nLong, alpha, x, beta, y);
+    else
+      k_csr_long<0><<<g, SPMV_T, 0, st>>>(A, m->longRows, m->nLong, alpha, x, beta, y);
+    PSBX_LAUNCH_CK("k_csr_long");
+  }
+  return SPGPU_SUCCESS;
+}
+
+// Row-block partition for the CSR stream kernel (host side, from irp).
+// Greedy: extend a block while it holds <= CSR_TILE entries and <= CSR_ROWS
+// rows; a row with more than CSR_TILE entries is a long row.
+int psbx_csr_partition(int m, const int *irp, int base, int *rowBlocks /*2*m max*/, int *nBlocks, int *longRows,
+                       int *nLong) {
+  int nb = 0, nl = 0;
+  int r = 0;
+  while (r < m) {
+    const int len = irp[r + 1] - irp[r];
+    if (len > CSR_TILE) {
+      longRows[nl++] = r;
+      r++;
+      continue;
+    }
+    int start = r, cnt = 0;
+    long long ent = 0;
+    while (r < m && cnt < CSR_ROWS) {
+      const int l = irp[r + 1] - irp[r];
+      if (l > CSR_TILE || ent + l > CSR_TILE) break;
+      ent += l;
+      cnt++;
+      r++;
+    }
+    rowBlocks[2 * nb] = start;
+    rowBlocks[2 * nb + 1] = r;
+    nb++;
+  }
+  (void)base;
+  *nBlocks = nb;
+  *nLong = nl;
+  return 0;
+}
+
+#undef SPMV_T

@@ -1,0 +1,443 @@
+// psbx_vect.cu -- dense multivector objects and the BLAS-1 kernels behind
+// psb_geaxpby / psb_gedot / psb_genrm2 / psb_geamax / psb_geasum / mlt.
+// Replaces cuda/vectordev.c, cuda/dvectordev.c:40-345 and the SPGPU kernels
+// daxpby.cu, ddot.cu, dnrm2.cu, amax/asum, axy_base.cuh, dupd_xyz.cu,
+// dxyzw.cu, scal/setscal/abs.
+//
+// Element-wise kernels use rounded multiplies and adds with no contraction,
+// so their results equal the reference CPU loops (psi_daxpbyv and friends)
+// bit for bit.  Reductions run on the device in a fixed order (per-thread
+// grid-stride partials, a shuffle tree per block, one partial per block, the
+// last block sums the partials), so a result depends only on n and the SM
+// count -- unlike the reference, which copies per-block partials to the host
+// and sums them there (ddot.cu:133-144).
+#include "psbx_internal.cuh"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+static const int VT = 256;  // threads per block for streaming vector kernels
+
+// ------------------------------------------------------------------ objects
+static int vec_pitch(unsigned count, unsigned size, unsigned elem) {
+  // cuda/vectordev.c:40-70: pitch = size for one vector, else rounded to 256 B
+  size_t es = elem == SPGPU_TYPE_DOUBLE ? 8 : 4;
+  if (elem == SPGPU_TYPE_COMPLEX_DOUBLE) es = 16;
+  if (elem == SPGPU_TYPE_COMPLEX_FLOAT) es = 8;
+  if (count <= 1) return (int)size;
+  return (int)((((size_t)size * es + 255) / 256) * 256 / es);
+}
+
+static size_t elem_size(int t) {
+  switch (t) {
+    case SPGPU_TYPE_INT: return 4;
+    case SPGPU_TYPE_FLOAT: return 4;
+    case SPGPU_TYPE_DOUBLE: return 8;
+    case SPGPU_TYPE_COMPLEX_FLOAT: return 8;
+    case SPGPU_TYPE_COMPLEX_DOUBLE: return 16;
+  }
+  return 0;
+}
+
+extern "C" {
+
+int FallocMultiVecDevice(void **deviceMultiVec, unsigned count, unsigned size, unsigned elementType) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!deviceMultiVec || elem_size((int)elementType) == 0) return SPGPU_UNSUPPORTED;
+  MultiVectDevice *v = (MultiVectDevice *)calloc(1, sizeof(MultiVectDevice));
+  v->count_ = (int)count;
+  v->size_ = (int)size;
+  v->pitch_ = vec_pitch(count, size, elementType);
+  v->elemType = (int)elementType;
+  v->owns = 1;
+  size_t bytes = (size_t)v->pitch_ * (count ? count : 1) * elem_size((int)elementType);
+  if (bytes == 0) bytes = 256;
+  cudaError_t e = cudaMalloc(&v->v_, bytes);
+  if (e != cudaSuccess) {
+    free(v);
+    *deviceMultiVec = nullptr;
+    return psbx_cuda_status(e, "FallocMultiVecDevice");
+  }
+  *deviceMultiVec = v;
+  return SPGPU_SUCCESS;
+}
+
+int psbx_wrapMultiVecDevice(void **deviceVec, void *devPtr, unsigned size, unsigned elementType) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!deviceVec || !devPtr || elem_size((int)elementType) == 0) return SPGPU_UNSUPPORTED;
+  MultiVectDevice *v = (MultiVectDevice *)calloc(1, sizeof(MultiVectDevice));
+  v->count_ = 1;
+  v->size_ = (int)size;
+  v->pitch_ = (int)size;
+  v->v_ = devPtr;
+  v->elemType = (int)elementType;
+  v->owns = 0;
+  *deviceVec = v;
+  return SPGPU_SUCCESS;
+}
+
+void *psbx_multivec_data(void *deviceVec) { return deviceVec ? ((MultiVectDevice *)deviceVec)->v_ : nullptr; }
+
+void freeMultiVecDevice(void *deviceVec) {
+  MultiVectDevice *v = (MultiVectDevice *)deviceVec;
+  if (!v) return;
+  if (v->owns && v->v_) {
+    cudaStreamSynchronize(psbx_ctx().stream);
+    cudaFree(v->v_);
+  }
+  free(v);
+}
+
+int getMultiVecDeviceSize(void *deviceVec) { return ((MultiVectDevice *)deviceVec)->size_; }
+int getMultiVecDeviceCount(void *deviceVec) { return ((MultiVectDevice *)deviceVec)->count_; }
+int getMultiVecDevicePitch(void *deviceVec) { return ((MultiVectDevice *)deviceVec)->pitch_; }
+
+static int vec_copy(void *deviceVec, void *host, bool h2d, int expect_type) {
+  MultiVectDevice *v = (MultiVectDevice *)deviceVec;
+  if (!v || !host) return SPGPU_UNSUPPORTED;
+  if (v->elemType != expect_type) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  size_t bytes = (size_t)v->pitch_ * v->count_ * elem_size(v->elemType);
+  if (bytes == 0) return SPGPU_SUCCESS;
+  if (h2d)
+    PSBX_CK(cudaMemcpyAsync(v->v_, host, bytes, cudaMemcpyHostToDevice, c.stream));
+  else
+    PSBX_CK(cudaMemcpyAsync(host, v->v_, bytes, cudaMemcpyDeviceToHost, c.stream));
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  return SPGPU_SUCCESS;
+}
+
+int writeMultiVecDeviceDouble(void *deviceVec, double *hostVec) {
+  return vec_copy(deviceVec, hostVec, true, SPGPU_TYPE_DOUBLE);
+}
+int writeMultiVecDeviceDoubleR2(void *deviceVec, double *hostVec, int ld) {
+  (void)ld;  // dvectordev.c:62-69 ignores ld as well
+  return vec_copy(deviceVec, hostVec, true, SPGPU_TYPE_DOUBLE);
+}
+int readMultiVecDeviceDouble(void *deviceVec, double *hostVec) {
+  return vec_copy(deviceVec, hostVec, false, SPGPU_TYPE_DOUBLE);
+}
+int readMultiVecDeviceDoubleR2(void *deviceVec, double *hostVec, int ld) {
+  (void)ld;
+  return vec_copy(deviceVec, hostVec, false, SPGPU_TYPE_DOUBLE);
+}
+int writeMultiVecDeviceFloat(void *deviceVec, float *hostVec) {
+  return vec_copy(deviceVec, hostVec, true, SPGPU_TYPE_FLOAT);
+}
+int readMultiVecDeviceFloat(void *deviceVec, float *hostVec) {
+  return vec_copy(deviceVec, hostVec, false, SPGPU_TYPE_FLOAT);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_setscal(int first, int last, double val, double *__restrict__ x) {
+  for (long long i = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; i <= last;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = val;
+}
+
+__global__ void k_scal(long long n, double alpha, double *__restrict__ x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = rmul(alpha, x[i]);
+}
+
+__global__ void k_zero(long long n, double *__restrict__ x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = 0.0;
+}
+
+// y = alpha*x + beta*y.  MODE 0: generic; 1: beta == 0 (y not read).
+template <int MODE>
+__global__ void k_axpby(int n, double alpha, const double *__restrict__ x, double beta, double *__restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double ax = rmul(alpha, ld_stream(x + i));
+    y[i] = MODE == 1 ? ax : radd(ax, rmul(beta, y[i]));
+  }
+}
+
+// y = beta*y, for alpha == 0 (x not read); beta == 0 writes zeros.
+__global__ void k_betay(int n, double beta, double *__restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = beta == 0.0 ? 0.0 : rmul(beta, y[i]);
+}
+
+__device__ __forceinline__ double axpby_el(double alpha, double x, double beta, double y) {
+  if (alpha == 0.0) return beta == 0.0 ? 0.0 : rmul(beta, y);
+  double ax = rmul(alpha, x);
+  return beta == 0.0 ? ax : radd(ax, rmul(beta, y));
+}
+
+__global__ void k_upd_xyz(int n, double a, double b, double g, double d, const double *__restrict__ x,
+                          double *__restrict__ y, double *__restrict__ z) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double yy = axpby_el(a, a == 0.0 ? 0.0 : x[i], b, b == 0.0 ? 0.0 : y[i]);
+    y[i] = yy;
+    z[i] = axpby_el(g, yy, d, d == 0.0 ? 0.0 : z[i]);
+  }
+}
+
+__global__ void k_xyzw(int n, double a, double b, double c, double d, double e, double f,
+                       const double *__restrict__ x, double *__restrict__ y, double *__restrict__ z,
+                       double *__restrict__ w) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double yy = radd(rmul(a, x[i]), rmul(b, y[i]));
+    double zz = radd(rmul(c, yy), rmul(d, z[i]));
+    double ww = radd(rmul(e, zz), rmul(f, w[i]));
+    y[i] = yy;
+    z[i] = zz;
+    w[i] = ww;
+  }
+}
+
+// z = alpha*(a.*b) + beta*z   (beta == 0: z not read)
+__global__ void k_axybz(int n, double alpha, const double *__restrict__ a, const double *b, double beta, double *z) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double t = rmul(alpha, rmul(ld_stream(a + i), ld_stream(b + i)));
+    z[i] = beta == 0.0 ? t : radd(t, rmul(beta, z[i]));
+  }
+}
+
+__global__ void k_abs(int n, double alpha, const double *__restrict__ a, double *__restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = rmul(alpha, fabs(a[i]));
+}
+
+enum { R_DOT = 0, R_NRM2 = 1, R_ASUM = 2, R_AMAX = 3 };
+
+// One partial per block per vector (blockIdx.y), finalised by the last block.
+template <int OP>
+__global__ void __launch_bounds__(256) k_reduce(int n, const double *__restrict__ x, int px,
+                                                const double *__restrict__ y, int py,
+                                                double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                double *__restrict__ res) {
+  __shared__ double sm[32];
+  const int v = blockIdx.y;
+  const double *xv = x + (size_t)v * px;
+  const double *yv = OP == R_DOT ? y + (size_t)v * py : nullptr;
+  double acc[1] = {0.0};
+  const int stride = gridDim.x * blockDim.x;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    double a0 = ld_stream(xv + i), a1 = ld_stream(xv + i + stride);
+    double a2 = ld_stream(xv + i + 2 * stride), a3 = ld_stream(xv + i + 3 * stride);
+    if (OP == R_DOT) {
+      double b0 = ld_stream(yv + i), b1 = ld_stream(yv + i + stride);
+      double b2 = ld_stream(yv + i + 2 * stride), b3 = ld_stream(yv + i + 3 * stride);
+      acc[0] = radd(acc[0], rmul(a0, b0));
+      acc[0] = radd(acc[0], rmul(a1, b1));
+      acc[0] = radd(acc[0], rmul(a2, b2));
+      acc[0] = radd(acc[0], rmul(a3, b3));
+    } else if (OP == R_NRM2) {
+      acc[0] = radd(acc[0], rmul(a0, a0));
+      acc[0] = radd(acc[0], rmul(a1, a1));
+      acc[0] = radd(acc[0], rmul(a2, a2));
+      acc[0] = radd(acc[0], rmul(a3, a3));
+    } else if (OP == R_ASUM) {
+      acc[0] = radd(acc[0], fabs(a0));
+      acc[0] = radd(acc[0], fabs(a1));
+      acc[0] = radd(acc[0], fabs(a2));
+      acc[0] = radd(acc[0], fabs(a3));
+    } else {
+      acc[0] = fmax(acc[0], fmax(fmax(fabs(a0), fabs(a1)), fmax(fabs(a2), fabs(a3))));
+    }
+  }
+  for (; i < n; i += stride) {
+    double a = ld_stream(xv + i);
+    if (OP == R_DOT) acc[0] = radd(acc[0], rmul(a, ld_stream(yv + i)));
+    else if (OP == R_NRM2) acc[0] = radd(acc[0], rmul(a, a));
+    else if (OP == R_ASUM) acc[0] = radd(acc[0], fabs(a));
+    else acc[0] = fmax(acc[0], fabs(a));
+  }
+  if (OP == R_AMAX) block_max<1>(acc, sm);
+  else block_sum<1>(acc, sm);
+  if (threadIdx.x == 0) part[(size_t)v * PSBX_MAX_PART + blockIdx.x] = acc[0];
+  if (psbx_last_block(ticket + v, gridDim.x)) {
+    double out[1];
+    if (OP == R_AMAX) final_max<1>(part + (size_t)v * PSBX_MAX_PART, 0, gridDim.x, out, sm);
+    else final_sum<1>(part + (size_t)v * PSBX_MAX_PART, 0, gridDim.x, out, sm);
+    if (threadIdx.x == 0) {
+      res[v] = OP == R_NRM2 ? sqrt(out[0]) : out[0];
+      ticket[v] = 0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ launchers
+int psbx_launch_scale(int n, double beta, double *y, cudaStream_t st) {
+  if (n <= 0) return SPGPU_SUCCESS;
+  int g = psbx_grid_for(n, VT);
+  k_betay<<<g, VT, 0, st>>>(n, beta, y);
+  PSBX_LAUNCH_CK("k_betay");
+  return SPGPU_SUCCESS;
+}
+
+static int launch_axpby(int n, double alpha, const double *x, double beta, double *y, cudaStream_t st) {
+  if (n <= 0) return SPGPU_SUCCESS;
+  int g = psbx_grid_for(n, VT);
+  if (alpha == 0.0) {
+    if (beta == 1.0) return SPGPU_SUCCESS;
+    k_betay<<<g, VT, 0, st>>>(n, beta, y);
+  } else if (beta == 0.0) {
+    k_axpby<1><<<g, VT, 0, st>>>(n, alpha, x, beta, y);
+  } else {
+    k_axpby<0><<<g, VT, 0, st>>>(n, alpha, x, beta, y);
+  }
+  PSBX_LAUNCH_CK("k_axpby");
+  return SPGPU_SUCCESS;
+}
+
+// Runs a reduction over count vectors; results land in c.d_res[0..count).
+static int launch_reduce(int op, int n, const MultiVectDevice *a, const MultiVectDevice *b, int count,
+                         cudaStream_t st, double *host_out) {
+  PsbxCtx &c = psbx_ctx();
+  for (int v0 = 0; v0 < count; v0 += PSBX_NLANES) {
+    int nv = count - v0 < PSBX_NLANES ? count - v0 : PSBX_NLANES;
+    int g = psbx_grid_for(n > 0 ? n : 1, VT * 4, 4);
+    if (g > PSBX_MAX_PART) g = PSBX_MAX_PART;
+    dim3 grid(g, nv);
+    const double *xa = (const double *)a->v_ + (size_t)v0 * a->pitch_;
+    const double *xb = b ? (const double *)b->v_ + (size_t)v0 * b->pitch_ : nullptr;
+    switch (op) {
+      case R_DOT: k_reduce<R_DOT><<<grid, VT, 0, st>>>(n, xa, a->pitch_, xb, b->pitch_, c.d_part, c.d_ticket, c.d_res); break;
+      case R_NRM2: k_reduce<R_NRM2><<<grid, VT, 0, st>>>(n, xa, a->pitch_, nullptr, 0, c.d_part, c.d_ticket, c.d_res); break;
+      case R_ASUM: k_reduce<R_ASUM><<<grid, VT, 0, st>>>(n, xa, a->pitch_, nullptr, 0, c.d_part, c.d_ticket, c.d_res); break;
+      default: k_reduce<R_AMAX><<<grid, VT, 0, st>>>(n, xa, a->pitch_, nullptr, 0, c.d_part, c.d_ticket, c.d_res); break;
+    }
+    PSBX_LAUNCH_CK("k_reduce");
+    PSBX_CK(cudaMemcpyAsync(c.h_res, c.d_res, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < nv; k++) host_out[v0 + k] = c.h_res[k];
+  }
+  return SPGPU_SUCCESS;
+}
+
+static inline MultiVectDevice *MV(void *p) { return (MultiVectDevice *)p; }
+
+extern "C" {
+
+int setscalMultiVecDeviceDouble(double val, int first, int last, int indexBase, void *devVecX) {
+  MultiVectDevice *x = MV(devVecX);
+  if (!x) return SPGPU_UNSUPPORTED;
+  int f = first - indexBase, l = last - indexBase;
+  if (f < 0 || l >= x->pitch_ * x->count_) return SPGPU_UNSUPPORTED;
+  if (l < f) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  int g = psbx_grid_for(l - f + 1, VT);
+  k_setscal<<<g, VT, 0, c.stream>>>(f, l, val, (double *)x->v_);
+  PSBX_LAUNCH_CK("k_setscal");
+  return SPGPU_SUCCESS;
+}
+
+int scalMultiVecDeviceDouble(double alpha, void *devVecA) {
+  MultiVectDevice *x = MV(devVecA);
+  if (!x) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  long long n = (long long)x->pitch_ * x->count_;
+  int g = psbx_grid_for(n, VT);
+  k_scal<<<g, VT, 0, c.stream>>>(n, alpha, (double *)x->v_);
+  PSBX_LAUNCH_CK("k_scal");
+  return SPGPU_SUCCESS;
+}
+
+int nrm2MultiVecDeviceDouble(double *y_res, int n, void *devVecA) {
+  MultiVectDevice *a = MV(devVecA);
+  if (!a || !y_res || n > a->size_) return SPGPU_UNSUPPORTED;
+  return launch_reduce(R_NRM2, n, a, nullptr, a->count_, psbx_ctx().stream, y_res);
+}
+
+int amaxMultiVecDeviceDouble(double *y_res, int n, void *devVecA) {
+  MultiVectDevice *a = MV(devVecA);
+  if (!a || !y_res || n > a->size_) return SPGPU_UNSUPPORTED;
+  return launch_reduce(R_AMAX, n, a, nullptr, a->count_, psbx_ctx().stream, y_res);
+}
+
+int asumMultiVecDeviceDouble(double *y_res, int n, void *devVecA) {
+  MultiVectDevice *a = MV(devVecA);
+  if (!a || !y_res || n > a->size_) return SPGPU_UNSUPPORTED;
+  return launch_reduce(R_ASUM, n, a, nullptr, a->count_, psbx_ctx().stream, y_res);
+}
+
+int dotMultiVecDeviceDouble(double *y_res, int n, void *devVecA, void *devVecB) {
+  MultiVectDevice *a = MV(devVecA), *b = MV(devVecB);
+  if (!a || !b || !y_res || n > a->size_ || n > b->size_ || a->count_ != b->count_) return SPGPU_UNSUPPORTED;
+  return launch_reduce(R_DOT, n, a, b, a->count_, psbx_ctx().stream, y_res);
+}
+
+int axpbyMultiVecDeviceDouble(int n, double alpha, void *devVecX, double beta, void *devVecY) {
+  MultiVectDevice *x = MV(devVecX), *y = MV(devVecY);
+  if (!x || !y || n > y->size_ || n > x->size_) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  for (int j = 0; j < y->count_; j++) {
+    int rc = launch_axpby(n, alpha, (const double *)x->v_ + (size_t)j * x->pitch_, beta,
+                          (double *)y->v_ + (size_t)j * y->pitch_, c.stream);
+    if (rc) return rc;
+  }
+  return SPGPU_SUCCESS;
+}
+
+int upd_xyzMultiVecDeviceDouble(int n, double alpha, double beta, double gamma, double delta, void *devVecX,
+                                void *devVecY, void *devVecZ) {
+  MultiVectDevice *x = MV(devVecX), *y = MV(devVecY), *z = MV(devVecZ);
+  if (!x || !y || !z || n > y->size_ || n > x->size_ || n > z->size_) return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  k_upd_xyz<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, alpha, beta, gamma, delta, (const double *)x->v_,
+                                                       (double *)y->v_, (double *)z->v_);
+  PSBX_LAUNCH_CK("k_upd_xyz");
+  return SPGPU_SUCCESS;
+}
+
+int xyzwMultiVecDeviceDouble(int n, double a, double b, double cc, double d, double e, double f, void *devVecX,
+                             void *devVecY, void *devVecZ, void *devVecW) {
+  MultiVectDevice *x = MV(devVecX), *y = MV(devVecY), *z = MV(devVecZ), *w = MV(devVecW);
+  if (!x || !y || !z || !w || n > y->size_ || n > x->size_ || n > z->size_ || n > w->size_)
+    return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  k_xyzw<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, a, b, cc, d, e, f, (const double *)x->v_,
+                                                    (double *)y->v_, (double *)z->v_, (double *)w->v_);
+  PSBX_LAUNCH_CK("k_xyzw");
+  return SPGPU_SUCCESS;
+}
+
+int axyMultiVecDeviceDouble(int n, double alpha, void *devVecA, void *devVecB) {
+  MultiVectDevice *a = MV(devVecA), *b = MV(devVecB);
+  if (!a || !b || n > a->size_ || n > b->size_) return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  k_axybz<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, alpha, (const double *)a->v_, (const double *)b->v_,
+                                                     0.0, (double *)b->v_);
+  PSBX_LAUNCH_CK("k_axy");
+  return SPGPU_SUCCESS;
+}
+
+int axybzMultiVecDeviceDouble(int n, double alpha, void *devVecA, void *devVecB, double beta, void *devVecZ) {
+  MultiVectDevice *a = MV(devVecA), *b = MV(devVecB), *z = MV(devVecZ);
+  if (!a || !b || !z || n > a->size_ || n > b->size_ || n > z->size_) return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  k_axybz<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, alpha, (const double *)a->v_, (const double *)b->v_,
+                                                     beta, (double *)z->v_);
+  PSBX_LAUNCH_CK("k_axybz");
+  return SPGPU_SUCCESS;
+}
+
+int absMultiVecDeviceDouble2(int n, double alpha, void *devVecA, void *devVecB) {
+  MultiVectDevice *a = MV(devVecA), *b = MV(devVecB);
+  if (!a || !b || n > a->size_ || n > b->size_) return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  k_abs<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, alpha, (const double *)a->v_, (double *)b->v_);
+  PSBX_LAUNCH_CK("k_abs");
+  return SPGPU_SUCCESS;
+}
+
+int absMultiVecDeviceDouble(int n, double alpha, void *devVecA) {
+  return absMultiVecDeviceDouble2(n, alpha, devVecA, devVecA);
+}
+
+}  // extern "C"

@@ -1,0 +1,388 @@
+"""Host-side mirror of the PSBLAS objects on this path, over the C-ABI.
+
+Names and argument meaning follow the reference so tests read like its
+drivers:
+
+* ``DVect``        -- psb_d_vect_cuda (cuda/psb_d_cuda_vect_mod.F90:48-106):
+                      a device multivector handle plus a host copy.
+* ``HllMat``       -- psb_d_cuda_hlg_sparse_mat (HLL on the device), built
+                      from host HLL arrays (to_gpu / writeHllDevice), from
+                      row-sorted COO via psiCopyCooToHlg, or on the device
+                      from CSR (psbx_hll_from_csr_device).
+* ``EllMat``       -- psb_d_cuda_elg_sparse_mat.
+* ``CsrMat``       -- psb_d_cuda_csrg_sparse_mat (d_CSRG* entry points).
+* ``DiagPrec``     -- prec%init('DIAG') / prec%build (psb_d_diagprec).
+* ``psb_spmm``, ``psb_geaxpby``, ``psb_gedot``, ``psb_genrm2``, ``psb_geamax``,
+  ``psb_geasum``, ``psb_gemlt``, ``psb_krylov`` -- base/psblas/* and
+  krylov/psb_dkrylov.f90 entry points (np = 1: no halo, no allreduce).
+
+Every call goes through libpsbx.so; there is no CPU fallback.  Errors raise
+PsbxError carrying the C-ABI status code (the reference's ``info``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def init(dev: int = 0) -> None:
+    """psb_cuda_init -> gpuInit (cuda/psb_cuda_env_mod.F90:43-60)."""
+    check(lib.gpuInit(int(dev)), "gpuInit")
+
+
+# ------------------------------------------------------------------ vectors
+class DVect:
+    """One (count=1) or several (count>1) FP64 device vectors."""
+
+    def __init__(self, n: int, count: int = 1, dtype=np.float64):
+        self.n = int(n)
+        self.count = int(count)
+        self.dtype = np.dtype(dtype)
+        et = L.SPGPU_TYPE_DOUBLE if self.dtype == np.float64 else L.SPGPU_TYPE_FLOAT
+        h = C.c_void_p()
+        check(lib.FallocMultiVecDevice(C.byref(h), self.count, self.n, et), "FallocMultiVecDevice")
+        self.h = h
+        self.pitch = lib.getMultiVecDevicePitch(self.h)
+
+    @classmethod
+    def bld(cls, x):
+        """psb_d_vect_cuda%bld(x): allocate and copy host data to the device."""
+        x = np.asarray(x)
+        v = cls(x.shape[0], 1 if x.ndim == 1 else x.shape[1], np.float32 if x.dtype == np.float32 else np.float64)
+        v.set_vect(x)
+        return v
+
+    def _host(self, x):
+        x = np.asarray(x, dtype=self.dtype)
+        if self.count == 1:
+            return np.ascontiguousarray(x.reshape(self.n))
+        buf = np.zeros((self.count, self.pitch), self.dtype)
+        buf[:, : self.n] = x.reshape(self.n, self.count).T
+        return buf
+
+    def set_vect(self, x):
+        buf = self._host(x)
+        f = lib.writeMultiVecDeviceDouble if self.dtype == np.float64 else lib.writeMultiVecDeviceFloat
+        check(f(self.h, _ptr(buf)), "writeMultiVecDevice")
+
+    def get_vect(self):
+        buf = np.zeros((self.count, self.pitch), self.dtype)
+        f = lib.readMultiVecDeviceDouble if self.dtype == np.float64 else lib.readMultiVecDeviceFloat
+        check(f(self.h, _ptr(buf)), "readMultiVecDevice")
+        out = buf[:, : self.n]
+        return out[0].copy() if self.count == 1 else out.T.copy()
+
+    def set_scal(self, val, first=1, last=None):
+        last = self.n if last is None else last
+        check(lib.setscalMultiVecDeviceDouble(float(val), int(first), int(last), 1, self.h), "setscal")
+
+    def zero(self):
+        self.set_scal(0.0)
+
+    def scal(self, alpha):
+        check(lib.scalMultiVecDeviceDouble(float(alpha), self.h), "scal")
+
+    def free(self):
+        if self.h:
+            lib.freeMultiVecDevice(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ matrices
+class HllMat:
+    fmt = L.PSBX_FMT_HLL
+
+    def __init__(self, h, rows):
+        self.h = h
+        self.rows = rows
+
+    @classmethod
+    def from_host_hll(cls, rows, hksz, irn, hkoffs, ja, val, idiag, nnz=None):
+        """to_gpu: FallocHllDevice + writeHllDeviceDouble with host HLL arrays
+        (psb_d_cuda_hlg_to_gpu.F90:56-58)."""
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        irn = np.ascontiguousarray(irn, np.int32)
+        hkoffs = np.ascontiguousarray(hkoffs, np.int32)
+        idiag = np.ascontiguousarray(idiag, np.int32)
+        nnz = int(irn.sum()) if nnz is None else nnz
+        h = C.c_void_p()
+        check(lib.FallocHllDevice(C.byref(h), hksz, rows, nnz, len(val), L.SPGPU_TYPE_DOUBLE, 1), "FallocHllDevice")
+        check(lib.writeHllDeviceDouble(h, _ptr(val), _ptr(ja), _ptr(hkoffs), _ptr(irn), _ptr(idiag)),
+              "writeHllDeviceDouble")
+        return cls(h, rows)
+
+    @classmethod
+    def from_coo_gpu(cls, rows, ia, ja, val, hksz=32):
+        """psb_d_cuda_cp_hlg_from_coo (GPU scatter path): host hack offsets
+        and idisp (psb_d_cuda_cp_hlg_from_coo.F90:117-188), then
+        psiCopyCooToHlgDouble."""
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        irn = np.bincount(ia - 1, minlength=rows).astype(np.int32)
+        noffs = (rows + hksz - 1) // hksz
+        pad = np.zeros(noffs * hksz, np.int64)
+        pad[:rows] = irn
+        width = pad.reshape(noffs, hksz).max(axis=1) if noffs else np.zeros(0, np.int64)
+        hkoffs = np.zeros(noffs + 1, np.int64)
+        np.cumsum(width * hksz, out=hkoffs[1:])
+        idisp = np.zeros(rows + 1, np.int64)
+        np.cumsum(irn, out=idisp[1:])
+        isz = int(hkoffs[-1])
+        hkoffs32, idisp32 = hkoffs.astype(np.int32), idisp.astype(np.int32)
+        h = C.c_void_p()
+        check(lib.FallocHllDevice(C.byref(h), hksz, rows, len(ia), isz, L.SPGPU_TYPE_DOUBLE, 1), "FallocHllDevice")
+        check(lib.psiCopyCooToHlgDouble(rows, rows, len(ia), hksz, noffs, isz, _ptr(irn), _ptr(hkoffs32),
+                                        _ptr(idisp32), _ptr(ja), _ptr(val), h), "psiCopyCooToHlgDouble")
+        return cls(h, rows)
+
+    @classmethod
+    def from_csr_device(cls, rows, cols, nnz, d_irp, d_ja, d_val, hksz=32, d_perm=None):
+        """Device CSR (raw device pointers, 1-based) -> device HLL."""
+        h = C.c_void_p()
+        check(lib.psbx_hll_from_csr_device(C.byref(h), rows, cols, nnz, C.c_void_p(d_irp), C.c_void_p(d_ja),
+                                           C.c_void_p(d_val), hksz,
+                                           None if d_perm is None else C.c_void_p(d_perm)),
+              "psbx_hll_from_csr_device")
+        return cls(h, rows)
+
+    def params(self):
+        v = [C.c_int() for _ in range(7)]
+        check(lib.getHllDeviceParams(self.h, *[C.byref(t) for t in v]), "getHllDeviceParams")
+        keys = ("hksz", "rows", "nzeros", "allocsize", "hackOffsLength", "firstIndex", "avgnzr")
+        return dict(zip(keys, (t.value for t in v)))
+
+    def read(self):
+        """from_gpu: readHllDeviceDouble into host arrays."""
+        p = self.params()
+        val = np.zeros(max(p["allocsize"], 1))
+        ja = np.zeros(max(p["allocsize"], 1), np.int32)
+        hk = np.zeros(p["hackOffsLength"] + 1, np.int32)
+        irn = np.zeros(max(p["rows"], 1), np.int32)
+        idg = np.zeros(max(p["rows"], 1), np.int32)
+        check(lib.readHllDeviceDouble(self.h, _ptr(val), _ptr(ja), _ptr(hk), _ptr(irn), _ptr(idg)), "readHll")
+        n, a = p["rows"], p["allocsize"]
+        return dict(val=val[:a], ja=ja[:a], hkoffs=hk, irn=irn[:n], idiag=idg[:n], hksz=p["hksz"])
+
+    def make_single(self):
+        check(lib.psbx_hll_make_single(self.h), "psbx_hll_make_single")
+
+    def spmv(self, alpha, x, beta, y):
+        f = lib.spmvHllDeviceDouble if x.dtype == np.float64 else lib.spmvHllDeviceFloat
+        check(f(self.h, alpha, x.h, beta, y.h), "spmvHllDevice")
+
+    def free(self):
+        if self.h:
+            lib.freeHllDevice(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class EllMat:
+    fmt = L.PSBX_FMT_ELL
+
+    def __init__(self, h, rows):
+        self.h = h
+        self.rows = rows
+
+    @classmethod
+    def from_host_ell(cls, rows, nzm, irn, ja, val, idiag, ldv, nnz=None):
+        """psb_d_cuda_elg_to_gpu: reallocate host arrays to (pitch, nzm) and
+        writeEllDeviceDouble (psb_d_cuda_elg_to_gpu.F90:60-90)."""
+        h = C.c_void_p()
+        nnz = int(np.sum(irn)) if nnz is None else nnz
+        check(lib.FallocEllDevice(C.byref(h), rows, nzm, nnz, rows, L.SPGPU_TYPE_DOUBLE, 1), "FallocEllDevice")
+        pitch = lib.getEllDevicePitch(h)
+        ja2 = np.ones((nzm, pitch), np.int32)
+        va2 = np.zeros((nzm, pitch), np.float64)
+        ja2[:, :rows] = np.asarray(ja, np.int32).reshape(nzm, ldv)[:, :rows]
+        va2[:, :rows] = np.asarray(val, np.float64).reshape(nzm, ldv)[:, :rows]
+        irn = np.ascontiguousarray(irn, np.int32)
+        idiag = np.ascontiguousarray(idiag, np.int32)
+        check(lib.writeEllDeviceDouble(h, _ptr(va2), _ptr(ja2), pitch, _ptr(irn), _ptr(idiag)), "writeEll")
+        return cls(h, rows)
+
+    @classmethod
+    def from_coo_gpu(cls, rows, ia, ja, val):
+        ia = np.ascontiguousarray(ia, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        irn = np.bincount(ia - 1, minlength=rows).astype(np.int32)
+        nzm = int(irn.max()) if rows else 0
+        idisp = np.zeros(rows + 1, np.int64)
+        np.cumsum(irn, out=idisp[1:])
+        idisp = idisp.astype(np.int32)
+        h = C.c_void_p()
+        check(lib.FallocEllDevice(C.byref(h), rows, nzm, len(ia), rows, L.SPGPU_TYPE_DOUBLE, 1), "FallocEllDevice")
+        pitch = lib.getEllDevicePitch(h)
+        check(lib.psiCopyCooToElgDouble(rows, rows, len(ia), 1, pitch, nzm, _ptr(irn), _ptr(idisp), _ptr(ja),
+                                        _ptr(val), h), "psiCopyCooToElgDouble")
+        return cls(h, rows)
+
+    def read(self):
+        pitch = lib.getEllDevicePitch(self.h)
+        nzm = lib.getEllDeviceMaxRowSize(self.h)
+        val = np.zeros(max(pitch * nzm, 1))
+        ja = np.zeros(max(pitch * nzm, 1), np.int32)
+        irn = np.zeros(max(self.rows, 1), np.int32)
+        idg = np.zeros(max(self.rows, 1), np.int32)
+        check(lib.readEllDeviceDouble(self.h, _ptr(val), _ptr(ja), pitch, _ptr(irn), _ptr(idg)), "readEll")
+        return dict(val=val[: pitch * nzm], ja=ja[: pitch * nzm], irn=irn[: self.rows], idiag=idg[: self.rows],
+                    ldv=pitch, nzm=nzm)
+
+    def spmv(self, alpha, x, beta, y):
+        check(lib.spmvEllDeviceDouble(self.h, alpha, x.h, beta, y.h), "spmvEllDeviceDouble")
+
+    def free(self):
+        if self.h:
+            lib.freeEllDevice(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class CsrMat:
+    fmt = L.PSBX_FMT_CSR
+
+    def __init__(self, rows, irp, ja, val, cols=None):
+        """to_gpu of psb_d_cuda_csrg_sparse_mat: d_CSRGDeviceAlloc +
+        d_CSRGHost2Device (1-based arrays)."""
+        self.rows = int(rows)
+        self.cm = L.Cmat()
+        irp = np.ascontiguousarray(irp, np.int32)
+        ja = np.ascontiguousarray(ja, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        nz = len(ja)
+        check(lib.d_CSRGDeviceAlloc(C.byref(self.cm), self.rows, cols or self.rows, nz), "d_CSRGDeviceAlloc")
+        check(lib.d_CSRGDeviceSetMatIndexBase(C.byref(self.cm), 1), "SetMatIndexBase")
+        check(lib.d_CSRGHost2Device(C.byref(self.cm), self.rows, cols or self.rows, nz, _ptr(irp), _ptr(ja),
+                                    _ptr(val)), "d_CSRGHost2Device")
+        self.nz = nz
+
+    @property
+    def h(self):
+        return C.addressof(self.cm)
+
+    def spmv(self, alpha, x, beta, y):
+        check(lib.d_spmvCSRGDevice(C.byref(self.cm), alpha, x.h, beta, y.h), "d_spmvCSRGDevice")
+
+    def read(self):
+        irp = np.zeros(self.rows + 1, np.int32)
+        ja = np.zeros(max(self.nz, 1), np.int32)
+        val = np.zeros(max(self.nz, 1))
+        check(lib.d_CSRGDevice2Host(C.byref(self.cm), self.rows, self.rows, self.nz, _ptr(irp), _ptr(ja),
+                                    _ptr(val)), "d_CSRGDevice2Host")
+        return irp, ja[: self.nz], val[: self.nz]
+
+    def free(self):
+        if self.cm.mat:
+            lib.d_CSRGDeviceFree(C.byref(self.cm))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ psblas
+def psb_spmm(alpha, a, x, beta, y):
+    """psb_spmm(alpha, a, x, beta, y, desc_a, info) at np=1 (psb_dspmm.f90:57-310)."""
+    a.spmv(float(alpha), x, float(beta), y)
+
+
+def psb_geaxpby(alpha, x, beta, y, n=None):
+    check(lib.axpbyMultiVecDeviceDouble(int(n or y.n), float(alpha), x.h, float(beta), y.h), "axpby")
+
+
+def _red(f, name, *vs, n=None):
+    out = (C.c_double * vs[0].count)()
+    check(f(out, int(n or vs[0].n), *[v.h for v in vs]), name)
+    return out[0] if vs[0].count == 1 else np.array(out[:])
+
+
+def psb_gedot(x, y, n=None):
+    return _red(lib.dotMultiVecDeviceDouble, "dot", x, y, n=n)
+
+
+def psb_genrm2(x, n=None):
+    return _red(lib.nrm2MultiVecDeviceDouble, "nrm2", x, n=n)
+
+
+def psb_geamax(x, n=None):
+    return _red(lib.amaxMultiVecDeviceDouble, "amax", x, n=n)
+
+
+def psb_geasum(x, n=None):
+    return _red(lib.asumMultiVecDeviceDouble, "asum", x, n=n)
+
+
+def psb_gemlt(alpha, d, x, beta, z, n=None):
+    """z = alpha*d.*x + beta*z (the y%mlt(alpha, dv, x, beta) of the DIAG
+    apply, via axybzMultiVecDevice)."""
+    check(lib.axybzMultiVecDeviceDouble(int(n or z.n), float(alpha), d.h, x.h, float(beta), z.h), "axybz")
+
+
+class DiagPrec:
+    """prec%init('DIAG') + prec%build(a) (psb_d_diagprec_impl.f90:229-292)."""
+
+    def __init__(self, ptype="DIAG"):
+        ptype = ptype.upper()
+        if ptype not in ("DIAG", "NONE", "NOPREC"):
+            raise ValueError(f"preconditioner {ptype} is not provided by this library")
+        self.ptype = ptype
+        self.dv = None
+
+    def build(self, a):
+        if self.ptype == "DIAG":
+            self.dv = DVect(a.rows)
+            check(lib.psbx_diag_prec_build(a.h if a.fmt != L.PSBX_FMT_CSR else C.c_void_p(a.h), a.fmt, self.dv.h),
+                  "psbx_diag_prec_build")
+        return self
+
+    def apply(self, x, y):
+        if self.dv is None:
+            psb_geaxpby(1.0, x, 0.0, y)
+        else:
+            psb_gemlt(1.0, self.dv, x, 0.0, y)
+
+
+def psb_krylov(method, a, prec, b, x, eps=1e-6, itmax=1000, istop=2, itrace=0, irst=10):
+    """psb_krylov(method, a, prec, b, x, eps, desc_a, info, itmax, iter, err,
+    itrace, irst, istop) for 'CG' and 'BICGSTAB', device-resident.
+    Returns (iter, err); raises PsbxError on failure."""
+    opt = L.SolverOptions()
+    lib.psbx_DefaultSolverOptions(C.byref(opt))
+    opt.eps, opt.itmax, opt.istop, opt.itrace, opt.irst = float(eps), int(itmax), int(istop), int(itrace), int(irst)
+    dinv = None if (prec is None or prec.dv is None) else prec.dv.h
+    mh = a.h if a.fmt != L.PSBX_FMT_CSR else C.c_void_p(a.h)
+    check(lib.psbx_dkrylov(method.upper().encode(), mh, a.fmt, dinv, b.h, x.h, C.byref(opt)), "psbx_dkrylov")
+    return opt.iter, opt.err
+
+
+def kernel_launches() -> int:
+    return int(lib.psbx_kernel_launches())

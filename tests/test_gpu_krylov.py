@@ -1,0 +1,111 @@
+"""GPU parity of the device-resident Krylov solvers against the oracle's
+restatement of psb_dcg / psb_dcgstab.
+
+Bar (from the reference's own behaviour): same stop test; iteration count
+within +-2 of the oracle's; final error estimate <= eps; the true residual
+of the returned x within a small factor of eps*||b||."""
+import numpy as np
+import pytest
+
+import oracle as O
+from psblas3_b200 import gen
+
+pytestmark = pytest.mark.gpu
+
+
+def _mats(psb, irp, ja, va, fmt):
+    n = len(irp) - 1
+    ia, _, _ = gen.csr_to_coo(irp, ja, va)
+    if fmt == "HLL":
+        h = O.hll_from_coo(n, ia, ja, va, 32)
+        return psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])
+    if fmt == "ELL":
+        e = O.ell_from_coo(n, ia, ja, va)
+        return psb.EllMat.from_host_ell(n, e["nzm"], e["irn"], e["ja"], e["val"], e["idiag"], e["ldv"])
+    return psb.CsrMat(n, irp, ja, va)
+
+
+def _solve_both(psb, method, irp, ja, va, b, fmt="HLL", eps=1e-9, itmax=1000, istop=2, prec=True):
+    n = len(irp) - 1
+    A = _mats(psb, irp, ja, va, fmt)
+    P = psb.DiagPrec("DIAG" if prec else "NONE").build(A)
+    B, X = psb.DVect.bld(b), psb.DVect.bld(np.zeros(n))
+    it, err = psb.psb_krylov(method, A, P, B, X, eps=eps, itmax=itmax, istop=istop)
+    x = X.get_vect()
+    dinv = None
+    if prec:
+        ia, _, _ = gen.csr_to_coo(irp, ja, va)
+        h = O.hll_from_coo(n, ia, ja, va, 32)
+        dinv = O.diag_prec_build(O.hll_get_diag(h, n))
+        assert np.array_equal(P.dv.get_vect(), dinv)  # prec build is bit-exact
+    xo, ito, erro = O.krylov(method, irp, ja, va, b, dinv=dinv, eps=eps, itmax=itmax, istop=istop)
+    return (x, it, err), (xo, ito, erro)
+
+
+def test_bicgstab_c1(psb):
+    """C1: pde3d 40^3 (a=1, b=(1,1,1)/sqrt3), HLL-32, DIAG, b = A*1, x0 = 0,
+    eps = 1e-9, istop 2."""
+    irp, ja, va = gen.pde3d(40, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    b = O.csr_csmv(irp, ja, va, 1.0, np.ones(n), 0.0, np.zeros(n))
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "BICGSTAB", irp, ja, va, b)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-9 and erro <= 1e-9
+    r = b - gen.csr_matvec(irp, ja, va, x)
+    assert np.linalg.norm(r) <= 2e-9 * np.linalg.norm(b)
+    assert np.max(np.abs(x - xo)) <= 1e-6
+
+
+@pytest.mark.parametrize("fmt", ["HLL", "ELL", "CSR"])
+@pytest.mark.parametrize("method", ["CG", "BICGSTAB"])
+def test_methods_formats_poisson(psb, fmt, method):
+    irp, ja, va = gen.poisson7(24)
+    n = len(irp) - 1
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, b, fmt=fmt, eps=1e-8)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-8
+    r = b - gen.csr_matvec(irp, ja, va, x)
+    assert np.linalg.norm(r) <= 2e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("istop", [1, 2, 3])
+def test_stop_criteria(psb, istop):
+    irp, ja, va = gen.pde3d(14, b=(0.5, 0.25, 0.0))
+    n = len(irp) - 1
+    b = np.random.default_rng(4).uniform(-1, 1, n)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "BICGSTAB", irp, ja, va, b, eps=1e-7, istop=istop)
+    assert abs(it - ito) <= 2, (istop, it, ito)
+    assert err <= 1e-7
+
+
+def test_cg_no_prec_and_itmax(psb):
+    irp, ja, va = gen.poisson7(16)
+    n = len(irp) - 1
+    b = np.random.default_rng(5).uniform(-1, 1, n)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "CG", irp, ja, va, b, prec=False, eps=1e-10)
+    assert abs(it - ito) <= 2
+    # itmax stops the solve with iter == itmax, err above eps (as the reference)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "CG", irp, ja, va, b, eps=1e-14, itmax=7)
+    assert it == 7 and ito == 7 and err > 1e-14
+    assert abs(err - erro) <= 1e-6 * erro
+
+
+def test_zero_rhs_returns_at_once(psb):
+    irp, ja, va = gen.poisson7(8)
+    n = len(irp) - 1
+    for method in ("CG", "BICGSTAB"):
+        (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, np.zeros(n))
+        assert np.all(x == 0)
+        assert it == ito
+
+
+def test_unknown_method_is_an_error(psb):
+    irp, ja, va = gen.poisson7(4)
+    n = len(irp) - 1
+    A = _mats(psb, irp, ja, va, "HLL")
+    from psblas3_b200._lib import PsbxError
+    with pytest.raises(PsbxError):
+        psb.psb_krylov("GMRES", A, None, psb.DVect.bld(np.ones(n)), psb.DVect(n))
+    with pytest.raises(PsbxError):
+        psb.psb_krylov("CG", A, None, psb.DVect.bld(np.ones(n)), psb.DVect(n), istop=7)

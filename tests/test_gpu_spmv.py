@@ -1,0 +1,243 @@
+"""GPU parity of the sparse formats and SpMV kernels against the oracle.
+
+Bar: conversions bit-exact (irn, hkoffs, ja, val including padding; idiag
+on rows that hold a diagonal); HLL / ELL / CSR-stream SpMV bit-exact against
+the oracle's csmv (same per-row order, rounded multiply then add); the CSR
+warp-per-row path for rows longer than 2048 entries within the FP64
+tolerance |dy_i| <= 1e-13 * sum_j |a_ij x_j| (componentwise, so rows whose
+sum cancels are judged on the scale of their terms)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from psblas3_b200 import gen
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL = 1e-13
+
+
+def _host_hll(irp, ja, va, hksz=32):
+    n = len(irp) - 1
+    ia, _, _ = gen.csr_to_coo(irp, ja, va)
+    return O.hll_from_coo(n, ia, ja, va, hksz)
+
+
+def _c1():
+    return gen.pde3d(40, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
+
+
+def test_usmv_kats_on_device(psb):
+    """psb_d_mvsv_tester.f90 non-transposed usmv cases through the GPU
+    HLL / ELL / CSR paths, exact equality."""
+    cases = [c for c in json.load(open(os.path.join(HERE, "golden", "usmv_kats.json")))["cases"]
+             if c["trans"] == "n"]
+    assert len(cases) == 8
+    for c in cases:
+        m = c["m"]
+        ia, ja, va = O.coo_fix(m, c["ia"], c["ja"], c["val"])
+        irp, cja, cv = O.csr_from_coo(m, ia, ja, va)
+        h = O.hll_from_coo(m, ia, ja, va, 32)
+        e = O.ell_from_coo(m, ia, ja, va)
+        mats = [psb.HllMat.from_host_hll(m, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"]),
+                psb.EllMat.from_host_ell(m, e["nzm"], e["irn"], e["ja"], e["val"], e["idiag"], e["ldv"]),
+                psb.CsrMat(m, irp, cja, cv)]
+        for A in mats:
+            x = psb.DVect.bld(np.array(c["x"], float))
+            y = psb.DVect.bld(np.array(c["y_before"], float))
+            psb.psb_spmm(c["alpha"], A, x, c["beta"], y)
+            assert np.array_equal(y.get_vect(), np.array(c["y_after"], float)), (type(A).__name__, c["name"])
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0), (3.0, 1.0), (0.5, -2.0), (0.0, 2.0)])
+def test_hll_spmv_c1_bitexact(psb, alpha, beta):
+    """C1 operator, x ~ U[-1,1] seed 0: GPU HLL SpMV == oracle HLL csmv."""
+    irp, ja, va = _c1()
+    n = len(irp) - 1
+    h = _host_hll(irp, ja, va)
+    A = psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-1, 1, n)
+    y0 = rng.uniform(-1, 1, n)
+    ref = O.hll_csmv(h, n, alpha, x, beta, y0)
+    X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+    psb.psb_spmm(alpha, A, X, beta, Y)
+    assert np.array_equal(Y.get_vect(), ref)
+
+
+def test_hll_beta0_does_not_read_y(psb):
+    irp, ja, va = gen.stencil27(9)
+    n = len(irp) - 1
+    h = _host_hll(irp, ja, va)
+    A = psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])
+    x = np.random.default_rng(1).uniform(-1, 1, n)
+    Y = psb.DVect.bld(np.full(n, np.nan))
+    psb.psb_spmm(2.0, A, psb.DVect.bld(x), 0.0, Y)
+    assert np.array_equal(Y.get_vect(), O.hll_csmv(h, n, 2.0, x, 0.0, np.zeros(n)))
+
+
+def test_device_hll_build_matches_cpu_converter(psb):
+    """psbx_hll_from_csr_device == psi_d_convert_hll_from_coo byte for byte,
+    padding included (C1 operator plus a ragged power-law matrix)."""
+    import torch
+    for irp, ja, va in (_c1(), gen.powerlaw(5000, kmax=300, seed=5)):
+        n = len(irp) - 1
+        h = _host_hll(irp, ja, va)
+        d_irp = torch.from_numpy(irp).cuda()
+        d_ja = torch.from_numpy(ja).cuda()
+        d_va = torch.from_numpy(va).cuda()
+        A = psb.HllMat.from_csr_device(n, n, len(ja), d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+        g = A.read()
+        assert np.array_equal(g["hkoffs"], h["hkoffs"])
+        assert np.array_equal(g["irn"], h["irn"])
+        assert np.array_equal(g["ja"], h["ja"])
+        assert np.array_equal(g["val"].view(np.uint64), h["val"].view(np.uint64))
+        has = h["idiag"] > 0
+        assert np.array_equal(g["idiag"][has], h["idiag"][has])
+        assert np.all(g["idiag"][~has] == 0)
+
+
+def test_psi_copy_coo_to_hlg(psb):
+    """GPU conversion variant (psi_cuda_CopyCooToHlg.cuh): same offsets, row
+    lengths, stored entries and diagonal positions as the CPU converter;
+    padding column = column of the first entry of row 2, value 0."""
+    irp, ja, va = gen.pde3d(13, b=(0.2, 0.1, 0.3))
+    n = len(irp) - 1
+    ia, _, _ = gen.csr_to_coo(irp, ja, va)
+    h = _host_hll(irp, ja, va)
+    A = psb.HllMat.from_coo_gpu(n, ia, ja, va, 32)
+    g = A.read()
+    assert np.array_equal(g["hkoffs"], h["hkoffs"]) and np.array_equal(g["irn"], h["irn"])
+    jc = ja[irp[1] - 1]
+    for k in range(len(h["hkoffs"]) - 1):
+        w = (h["hkoffs"][k + 1] - h["hkoffs"][k]) // 32
+        gj = g["ja"][h["hkoffs"][k]: h["hkoffs"][k + 1]].reshape(w, 32)
+        cj = h["ja"][h["hkoffs"][k]: h["hkoffs"][k + 1]].reshape(w, 32)
+        gv = g["val"][h["hkoffs"][k]: h["hkoffs"][k + 1]].reshape(w, 32)
+        for ii in range(min(32, n - 32 * k)):
+            L = h["irn"][32 * k + ii]
+            assert np.array_equal(gj[:L, ii], cj[:L, ii])
+            assert np.all(gj[L:, ii] == jc) and np.all(gv[L:, ii] == 0)
+    assert np.array_equal(g["idiag"], h["idiag"])
+    x = np.random.default_rng(2).uniform(-1, 1, n)
+    Y = psb.DVect(n)
+    psb.psb_spmm(1.0, A, psb.DVect.bld(x), 0.0, Y)
+    assert np.array_equal(Y.get_vect(), O.hll_csmv(h, n, 1.0, x, 0.0, np.zeros(n)))
+
+
+@pytest.mark.parametrize("maker", ["pde3d", "stencil27", "ragged"])
+def test_ell_spmv_and_conversion(psb, maker):
+    if maker == "pde3d":
+        irp, ja, va = gen.pde3d(11, b=(1 / np.sqrt(3),) * 3)
+    elif maker == "stencil27":
+        irp, ja, va = gen.stencil27(9)
+    else:
+        irp, ja, va = gen.powerlaw(777, kmax=60, seed=7)
+    n = len(irp) - 1
+    ia, _, _ = gen.csr_to_coo(irp, ja, va)
+    e = O.ell_from_coo(n, ia, ja, va)
+    x = np.random.default_rng(3).uniform(-1, 1, n)
+    y0 = np.random.default_rng(4).uniform(-1, 1, n)
+    ref = O.ell_csmv(e, n, -1.5, x, 0.25, y0)
+    for A in (psb.EllMat.from_host_ell(n, e["nzm"], e["irn"], e["ja"], e["val"], e["idiag"], e["ldv"]),
+              psb.EllMat.from_coo_gpu(n, ia, ja, va)):
+        g = A.read()
+        nzm, ldv = g["nzm"], g["ldv"]
+        assert nzm == e["nzm"] and ldv == ((n + 31) // 32) * 32
+        gj = g["ja"].reshape(nzm, ldv)[:, :n]
+        gv = g["val"].reshape(nzm, ldv)[:, :n]
+        assert np.array_equal(gj, e["ja"].reshape(nzm, n))
+        assert np.array_equal(gv, e["val"].reshape(nzm, n))
+        Y = psb.DVect.bld(y0)
+        psb.psb_spmm(-1.5, A, psb.DVect.bld(x), 0.25, Y)
+        assert np.array_equal(Y.get_vect(), ref)
+
+
+@pytest.mark.parametrize("maker", ["pde3d", "stencil27", "powerlaw_long"])
+def test_csr_spmv(psb, maker):
+    if maker == "pde3d":
+        irp, ja, va = gen.pde3d(21, b=(1 / np.sqrt(3),) * 3)
+    elif maker == "stencil27":
+        irp, ja, va = gen.stencil27(17)
+    else:
+        irp, ja, va = gen.powerlaw(60000, kmax=4096, seed=11)
+    n = len(irp) - 1
+    x = np.random.default_rng(5).uniform(-1, 1, n)
+    y0 = np.random.default_rng(6).uniform(-1, 1, n)
+    ref = O.csr_csmv(irp, ja, va, 1.0, x, -1.0, y0)
+    A = psb.CsrMat(n, irp, ja, va)
+    Y = psb.DVect.bld(y0)
+    psb.psb_spmm(1.0, A, psb.DVect.bld(x), -1.0, Y)
+    got = Y.get_vect()
+    lens = np.diff(irp)
+    short = lens <= 2048
+    assert np.array_equal(got[short], ref[short])
+    if (~short).any():
+        ia, _, _ = gen.csr_to_coo(irp, ja, va)
+        scale = np.bincount(ia - 1, weights=np.abs(va * x[ja - 1]), minlength=n) + np.abs(y0)
+        assert np.all(np.abs(got - ref)[~short] <= TOL * scale[~short])
+    irp2, ja2, va2 = A.read()
+    assert np.array_equal(irp2, irp) and np.array_equal(ja2, ja) and np.array_equal(va2, va)
+
+
+def test_edge_shapes(psb):
+    """1-row matrix, an empty row, n not a multiple of 32, hack size 64."""
+    cases = [(1, [1], [1], [2.5]), (5, [1, 2, 2, 5], [1, 1, 2, 5], [1.0, -2.0, 3.0, 4.0]),
+             (45, list(range(1, 46)), list(range(1, 46)), list(np.arange(1.0, 46.0)))]
+    for n, ia, ja, va in cases:
+        ia, ja, va = O.coo_fix(n, ia, ja, va)
+        x = np.random.default_rng(n).uniform(-1, 1, n)
+        for hk in (32, 64):
+            h = O.hll_from_coo(n, ia, ja, va, hk)
+            A = psb.HllMat.from_host_hll(n, hk, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])
+            Y = psb.DVect(n)
+            psb.psb_spmm(1.0, A, psb.DVect.bld(x), 0.0, Y)
+            assert np.array_equal(Y.get_vect(), O.hll_csmv(h, n, 1.0, x, 0.0, np.zeros(n)))
+        irp, cja, cv = O.csr_from_coo(n, ia, ja, va)
+        A = psb.CsrMat(n, irp, cja, cv)
+        Y = psb.DVect(n)
+        psb.psb_spmm(1.0, A, psb.DVect.bld(x), 0.0, Y)
+        assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, cja, cv, 1.0, x, 0.0, np.zeros(n)))
+
+
+def test_size_mismatch_is_an_error(psb):
+    irp, ja, va = gen.poisson7(4)
+    n = len(irp) - 1
+    h = _host_hll(irp, ja, va)
+    A = psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])
+    from psblas3_b200._lib import PsbxError
+    with pytest.raises(PsbxError) as ei:
+        psb.psb_spmm(1.0, A, psb.DVect(n), 0.0, psb.DVect(n - 1))
+    assert ei.value.code == 1  # SPGPU_UNSUPPORTED
+
+
+def test_full_size_27pt_properties(psb):
+    """C2a operator at full size (200^3, 213,847,192 entries), built on the
+    device: A*1 equals the exact row sums (26 - neighbours, integers), and
+    A*(x+y) - (A*x + A*y) stays at rounding level."""
+    import torch
+    irp, ja, va = gen.stencil27(200)
+    n = len(irp) - 1
+    assert len(ja) == 213847192
+    d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (irp, ja, va))
+    A = psb.HllMat.from_csr_device(n, n, len(ja), d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+    del d_irp, d_ja, d_va
+    p = A.params()
+    assert p["allocsize"] == 214591104
+    ones = psb.DVect.bld(np.ones(n))
+    Y = psb.DVect(n)
+    psb.psb_spmm(1.0, A, ones, 0.0, Y)
+    rowsum = 27.0 - np.diff(irp)  # 26 - (len - 1)
+    assert np.array_equal(Y.get_vect(), rowsum)
+    rng = np.random.default_rng(0)
+    x, z = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    Ax, Az, Axz = psb.DVect(n), psb.DVect(n), psb.DVect(n)
+    psb.psb_spmm(1.0, A, psb.DVect.bld(x), 0.0, Ax)
+    psb.psb_spmm(1.0, A, psb.DVect.bld(z), 0.0, Az)
+    psb.psb_spmm(1.0, A, psb.DVect.bld(x + z), 0.0, Axz)
+    d = Axz.get_vect() - (Ax.get_vect() + Az.get_vect())
+    assert np.max(np.abs(d)) <= 1e-12 * 27 * 4
+    A.free()

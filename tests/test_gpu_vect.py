@@ -1,0 +1,123 @@
+"""GPU parity of the vector kernels (psb_geaxpby, mlt, upd_xyz, xyzw, dot,
+nrm2, amax, asum) against the oracle.
+
+Element-wise kernels: bit-exact.  Reductions: the reference sums on the host
+in its own order; here the order is a fixed device tree, so the bar is
+|s_gpu - s_ref| <= 1e-13 * sum|x_i y_i| (1e-13 * sum x_i^2 for nrm2^2)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+SIZES = [1, 31, 1000, 65537, 3_000_001]
+
+
+@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("alpha,beta", [(1.0, 1.0), (-1.0, 1.0), (0.5, 1.0), (2.5, 0.0), (0.0, -0.75),
+                                        (0.0, 0.0), (1.0, -1.0), (-3.25, 0.125)])
+def test_axpby_bitexact(psb, n, alpha, beta):
+    rng = np.random.default_rng(n)
+    x, y = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    X, Y = psb.DVect.bld(x), psb.DVect.bld(y)
+    psb.psb_geaxpby(alpha, X, beta, Y)
+    assert np.array_equal(Y.get_vect(), O.axpby(alpha, x, beta, y))
+
+
+def test_axpby_beta0_ignores_nan_y(psb):
+    x = np.arange(10.0)
+    Y = psb.DVect.bld(np.full(10, np.nan))
+    psb.psb_geaxpby(2.0, psb.DVect.bld(x), 0.0, Y)
+    assert np.array_equal(Y.get_vect(), 2 * x)
+
+
+def test_vecoperation_kats_on_device(psb):
+    n = 1000
+    for c in json.load(open(os.path.join(HERE, "golden", "vecop_kats.json")))["cases"]:
+        X = psb.DVect.bld(np.full(n, c["x"]))
+        if c["op"] == "axpby":
+            Y = psb.DVect.bld(np.full(n, c["y"]))
+            psb.psb_geaxpby(c["alpha"], X, c["beta"], Y)
+            assert np.all(Y.get_vect() == c["expect"])
+        elif c["op"] == "axpbyz":
+            # Z = alpha*X + beta*Y through upd_xyz with a zero Z start
+            Y = psb.DVect.bld(np.full(n, c["y"]))
+            Z = psb.DVect.bld(np.zeros(n))
+            psb.psb_geaxpby(1.0, Y, 0.0, Z)
+            psb.psb_geaxpby(c["alpha"], X, c["beta"], Z)
+            assert np.all(Z.get_vect() == c["expect"])
+        elif c["op"] == "mlt":
+            Z = psb.DVect(n)
+            psb.psb_gemlt(c["alpha"], X, psb.DVect.bld(np.full(n, c["y"])), c["beta"], Z)
+            assert np.all(Z.get_vect() == c["expect"])
+        elif c["op"] == "dot":
+            assert psb.psb_gedot(X, psb.DVect.bld(np.full(n, c["y"]))) == n * c["expect_per_entry"]
+        elif c["op"] == "amax":
+            assert psb.psb_geamax(X) == c["expect"]
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_reductions(psb, n):
+    rng = np.random.default_rng(100 + n)
+    x, y = rng.uniform(-1, 1, n), rng.standard_normal(n)
+    X, Y = psb.DVect.bld(x), psb.DVect.bld(y)
+    d = psb.psb_gedot(X, Y)
+    assert abs(d - O.dot(x, y)) <= 1e-13 * np.sum(np.abs(x * y))
+    nr = psb.psb_genrm2(X)
+    assert abs(nr * nr - O.nrm2(x) ** 2) <= 1e-13 * np.sum(x * x)
+    assert psb.psb_geamax(Y) == O.amax(y)
+    assert abs(psb.psb_geasum(Y) - O.asum(y)) <= 1e-13 * O.asum(y)
+    # deterministic: same bits on a second call
+    assert psb.psb_gedot(X, Y) == d
+
+
+def test_reduction_partial_length_and_multivector(psb):
+    """n < size reduces over the first n entries; count > 1 returns one
+    result per vector (dotMultiVecDevice / nrm2MultiVecDevice)."""
+    rng = np.random.default_rng(7)
+    n, cnt = 5001, 3
+    a, b = rng.uniform(-1, 1, (n, cnt)), rng.uniform(-1, 1, (n, cnt))
+    A, B = psb.DVect.bld(a), psb.DVect.bld(b)
+    assert A.count == 3 and A.pitch % 32 == 0 and A.pitch >= n
+    dots = psb.psb_gedot(A, B)
+    for k in range(cnt):
+        assert abs(dots[k] - O.dot(a[:, k], b[:, k])) <= 1e-13 * np.sum(np.abs(a[:, k] * b[:, k]))
+    nrm = psb.psb_genrm2(A, n=100)
+    for k in range(cnt):
+        assert abs(nrm[k] - O.nrm2(a[:100, k])) <= 1e-13 * O.nrm2(a[:100, k])
+    assert np.array_equal(A.get_vect(), a)
+
+
+@pytest.mark.parametrize("n", [1, 1000, 1_000_003])
+def test_elementwise_family(psb, n):
+    from psblas3_b200._lib import lib, check
+    rng = np.random.default_rng(200 + n)
+    a, b, c, w = (rng.uniform(-1, 1, n) for _ in range(4))
+    # mlt / axybz: z = alpha*a.*b + beta*z
+    Z = psb.DVect.bld(c)
+    psb.psb_gemlt(1.5, psb.DVect.bld(a), psb.DVect.bld(b), -0.5, Z)
+    assert np.array_equal(Z.get_vect(), O.mlt(1.5, a, b, -0.5, c))
+    # upd_xyz
+    X, Y, Z = psb.DVect.bld(a), psb.DVect.bld(b), psb.DVect.bld(c)
+    check(lib.upd_xyzMultiVecDeviceDouble(n, 0.7, -1.0, 2.0, 0.5, X.h, Y.h, Z.h), "upd_xyz")
+    ry, rz = O.upd_xyz(0.7, -1.0, 2.0, 0.5, a, b, c)
+    assert np.array_equal(Y.get_vect(), ry) and np.array_equal(Z.get_vect(), rz)
+    # xyzw (CPU semantics of psi_dxyzw)
+    X, Y, Z, W = psb.DVect.bld(a), psb.DVect.bld(b), psb.DVect.bld(c), psb.DVect.bld(w)
+    check(lib.xyzwMultiVecDeviceDouble(n, 1.0, 2.0, -1.0, 0.5, 3.0, -0.25, X.h, Y.h, Z.h, W.h), "xyzw")
+    ry, rz, rw = O.xyzw(1.0, 2.0, -1.0, 0.5, 3.0, -0.25, a, b, c, w)
+    assert np.array_equal(Y.get_vect(), ry) and np.array_equal(Z.get_vect(), rz)
+    assert np.array_equal(W.get_vect(), rw)
+    # abs, scal, setscal
+    A = psb.DVect.bld(a)
+    check(lib.absMultiVecDeviceDouble(n, 2.0, A.h), "abs")
+    assert np.array_equal(A.get_vect(), 2.0 * np.abs(a))
+    A.scal(-0.5)
+    assert np.array_equal(A.get_vect(), -0.5 * (2.0 * np.abs(a)))
+    A.set_scal(3.0, first=1, last=max(1, n // 2))
+    got = A.get_vect()
+    assert np.all(got[: max(1, n // 2)] == 3.0)
