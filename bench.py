@@ -26,7 +26,6 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -62,53 +61,60 @@ def profile_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every ~5 ms in a
+    background thread during the timed region (the same counters nvidia-smi
+    prints: clocks.sm, clocks.max.sm, clocks_event_reasons.*)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    def __init__(self, index, period=0.005):
+        self.index, self.period = index, period
+        self.samples, self.reasons, self.smax = [], set(), None
+        self._stop = None
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
+    def _run(self):
+        import pynvml as N
+        names = {"hw_slowdown": getattr(N, "nvmlClocksEventReasonHwSlowdown", 0x8),
+                 "hw_thermal_slowdown": getattr(N, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+                 "sw_thermal_slowdown": getattr(N, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+                 "sw_power_cap": getattr(N, "nvmlClocksEventReasonSwPowerCap", 0x4)}
+        h = N.nvmlDeviceGetHandleByIndex(self.index)
+        self.smax = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            self.samples.append(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+            try:
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                r = N.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            for k, bit in names.items():
+                if r & bit:
+                    self.reasons.add(k)
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            import pynvml as N
+            N.nvmlInit()
+            # NVML indexes physical GPUs; map through CUDA_VISIBLE_DEVICES
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            if vis:
+                ids = [v.strip() for v in vis.split(",")]
+                if self.index < len(ids) and ids[self.index].isdigit():
+                    self.index = int(ids[self.index])
+            self._stop = threading.Event()
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._stop = None
         return self
 
     def __exit__(self, *a):
-        self.lines = []
-        if self.proc:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+        if self._stop is not None:
+            self._stop.set()
+            self._t.join(timeout=2)
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for l in getattr(self, "lines", []):
-            f = [t.strip() for t in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 def dist_setup():
@@ -170,7 +176,7 @@ def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     from psblas3_b200 import gen
-    irp, ja, va = gen.stencil27(GRID)
+    irp, ja, va = gen.stencil27(args.grid)
     n = len(irp) - 1
     x = np.random.default_rng(0).uniform(-1, 1, n)
     vals = []
@@ -184,7 +190,7 @@ def run_reference(args):
     line = base_line(args, 1)
     line.update({
         "impl": "reference", "value": v, "ms_per_step": algorithmic_bytes(n, len(ja)) / v / 1e6,
-        "config": {"workload": "C2a: FP64 SpMV, 27-point Poisson 200^3, CSR rows (reference CPU csmv order)",
+        "config": {"workload": f"C2a: FP64 SpMV, 27-point Poisson {args.grid}^3, CSR rows (reference CPU csmv order)",
                    "rows": n, "nnz": len(ja)},
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} steps x up to 10 full-matrix SpMVs (<= 4 s each)"},
@@ -202,7 +208,7 @@ def run_ours(args):
     psb.init(local)
 
     # ---- matrix: generated on the host, built into HLL on the device
-    irp, ja, va = gen.stencil27(GRID)
+    irp, ja, va = gen.stencil27(args.grid)
     n, nnz = len(irp) - 1, len(ja)
     d_irp, d_ja, d_va = (torch.from_numpy(a).to(f"cuda:{local}") for a in (irp, ja, va))
     A = psb.HllMat.from_csr_device(n, n, nnz, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
@@ -261,7 +267,7 @@ def run_ours(args):
         line = base_line(args, world)
         line.update({
             "value": value, "ms_per_step": ms_max,
-            "config": {"workload": "C2a: FP64 SpMV, 27-point Poisson 200^3, HLL hack 32, int32 indices",
+            "config": {"workload": f"C2a: FP64 SpMV, 27-point Poisson {args.grid}^3, HLL hack 32, int32 indices",
                        "rows": n, "nnz": nnz, "bytes_per_step": bytes_alg, "parallelism": f"replicas x{world}",
                        "l2": "inputs 2.74 GB per step > 126 MB L2, no flush"},
             "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8,
@@ -289,6 +295,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=GRID, help="grid side (profiling runs use a smaller case)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -354,17 +354,53 @@ void or_axpbyz(int n, double alpha, const double *x, double beta,
 }
 
 /* dot and nrm2: base/modules/serial/psb_d_base_vect_mod.F90:974-996 and
- * :1764-1774 call external BLAS ddot/dnrm2 (third party, unpinned).  The
- * restatement is a plain left-to-right FP64 sum; nrm2 = sqrt(sum x^2), the
- * GPU reference's formula (cuda/spgpu/kernels/dnrm2.cu). */
+ * :1764-1774 call external BLAS ddot/dnrm2 (third party, version not pinned,
+ * so the reference fixes no summation order).  The restatement computes the
+ * dot product with the compensated algorithm Dot2 (Ogita, Rump, Oishi,
+ * "Accurate sum and dot product", SIAM J. Sci. Comput. 26(6), 2005): every
+ * product is split exactly into p + e with an FMA, the running sum is kept
+ * as s + c with TwoSum, and the result is s + c, which is as accurate as a
+ * sum in twice the working precision and then rounded.  It is at least as
+ * accurate as any ordering a BLAS ddot could use, and it makes the result
+ * (nearly always) independent of the summation order, which is what lets a
+ * parallel device reduction agree with it bit for bit.  nrm2 = sqrt(dot(x,x))
+ * as the reference's GPU kernel (cuda/spgpu/kernels/dnrm2.cu) computes it.
+ * The FMA here is explicit (fma()), not a contraction. */
+typedef struct { double s, c; } dd_t;
+
+static inline dd_t dd_two_sum(double a, double b)
+{
+  dd_t r;
+  r.s = a + b;
+  double bb = r.s - a;
+  r.c = (a - (r.s - bb)) + (b - bb);
+  return r;
+}
+
+static inline void dd_add_prod(dd_t *acc, double a, double b)
+{
+  double p = a * b;
+  double e = fma(a, b, -p);
+  dd_t t = dd_two_sum(acc->s, p);
+  acc->s = t.s;
+  acc->c = acc->c + (t.c + e);
+}
+
+static inline dd_t dd_merge(dd_t x, dd_t y)
+{
+  dd_t t = dd_two_sum(x.s, y.s);
+  t.c = t.c + (x.c + y.c);
+  return t;
+}
+
 double or_dot(int n, const double *x, const double *y)
 {
   if (g_threads <= 1) {
-    double s = 0.0;
-    for (int i = 0; i < n; i++) s = s + x[i] * y[i];
-    return s;
+    dd_t acc = {0.0, 0.0};
+    for (int i = 0; i < n; i++) dd_add_prod(&acc, x[i], y[i]);
+    return acc.s + acc.c;
   }
-  double part[1024];
+  dd_t part[1024];
   int nt = g_threads > 1024 ? 1024 : g_threads;
 #pragma omp parallel num_threads(nt)
   {
@@ -373,14 +409,14 @@ double or_dot(int n, const double *x, const double *y)
     t = omp_get_thread_num(); T = omp_get_num_threads();
 #endif
     int64_t lo = (int64_t)n * t / T, hi = (int64_t)n * (t + 1) / T;
-    double s = 0.0;
-    for (int64_t i = lo; i < hi; i++) s = s + x[i] * y[i];
-    part[t] = s;
+    dd_t acc = {0.0, 0.0};
+    for (int64_t i = lo; i < hi; i++) dd_add_prod(&acc, x[i], y[i]);
+    part[t] = acc;
     if (t == 0) nt = T;
   }
-  double s = 0.0;
-  for (int t = 0; t < nt; t++) s = s + part[t];
-  return s;
+  dd_t acc = {0.0, 0.0};
+  for (int t = 0; t < nt; t++) acc = dd_merge(acc, part[t]);
+  return acc.s + acc.c;
 }
 
 double or_nrm2(int n, const double *x) { return sqrt(or_dot(n, x, x)); }

@@ -32,7 +32,7 @@ static int ctx_create(int dev) {
   c.maxThreadsPerMP = c.prop.maxThreadsPerMultiProcessor;
   PSBX_CK(cudaStreamCreateWithFlags(&c.defaultStream, cudaStreamNonBlocking));
   c.stream = c.defaultStream;
-  PSBX_CK(cudaMalloc(&c.d_part, sizeof(double) * PSBX_NLANES * PSBX_MAX_PART));
+  PSBX_CK(cudaMalloc(&c.d_part, sizeof(double) * 2 * PSBX_NLANES * PSBX_MAX_PART));
   PSBX_CK(cudaMalloc(&c.d_ticket, sizeof(unsigned) * 64));
   PSBX_CK(cudaMemset(c.d_ticket, 0, sizeof(unsigned) * 64));
   PSBX_CK(cudaMalloc(&c.d_res, sizeof(double) * 64));

@@ -78,7 +78,7 @@ struct CsrDevice {
 // ---------------------------------------------------------------------------
 // Context: one per process (the reference keeps one global SPGPU handle).
 // ---------------------------------------------------------------------------
-#define PSBX_MAX_PART 4096     // partial-sum slots per reduction lane
+#define PSBX_MAX_PART 4096     // partial-sum slots (pairs) per reduction lane
 #define PSBX_NLANES   8        // simultaneous reductions (vectors / dots)
 
 struct PsbxCtx {
@@ -190,6 +190,104 @@ __device__ __forceinline__ void block_max(double (&v)[NV], double *smem) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Compensated dot products (Dot2 of Ogita, Rump and Oishi, SIAM J. Sci.
+// Comput. 26(6), 2005): each product is split exactly into p + e with an
+// FMA, running sums are kept as an unevaluated pair s + c (TwoSum), partial
+// pairs merge with TwoSum.  The rounded result s + c is as accurate as a sum
+// in twice the precision, so it almost never depends on the summation order:
+// the device tree and the oracle's left-to-right loop give the same bits.
+// ---------------------------------------------------------------------------
+struct dd_t {
+  double s, c;
+};
+
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+
+__device__ __forceinline__ void dd_add_prod(dd_t &acc, double x, double y) {
+  const double p = __dmul_rn(x, y);
+  const double e = __fma_rn(x, y, -p);
+  double s, t;
+  two_sum(acc.s, p, s, t);
+  acc.s = s;
+  acc.c = __dadd_rn(acc.c, __dadd_rn(t, e));
+}
+
+__device__ __forceinline__ dd_t dd_merge(dd_t x, dd_t y) {
+  dd_t r;
+  double t;
+  two_sum(x.s, y.s, r.s, t);
+  r.c = __dadd_rn(t, __dadd_rn(x.c, y.c));
+  return r;
+}
+
+__device__ __forceinline__ double dd_value(dd_t a) { return __dadd_rn(a.s, a.c); }
+
+template <int NV>
+__device__ __forceinline__ void block_sum_dd(dd_t (&v)[NV], double *smem /*[64*NV]*/) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      dd_t u;
+      u.s = __shfl_down_sync(0xffffffffu, v[k].s, o);
+      u.c = __shfl_down_sync(0xffffffffu, v[k].c, o);
+      v[k] = dd_merge(v[k], u);
+    }
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      smem[(k * 32 + warp) * 2] = v[k].s;
+      smem[(k * 32 + warp) * 2 + 1] = v[k].c;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      dd_t t = {0.0, 0.0};
+      if (lane < nw) {
+        t.s = smem[(k * 32 + lane) * 2];
+        t.c = smem[(k * 32 + lane) * 2 + 1];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        dd_t u;
+        u.s = __shfl_down_sync(0xffffffffu, t.s, o);
+        u.c = __shfl_down_sync(0xffffffffu, t.c, o);
+        t = dd_merge(t, u);
+      }
+      v[k] = t;  // valid in thread 0
+    }
+  }
+}
+
+// Partial pairs of lane k, block b live at part[2*(k*stride + b)] (+1).
+template <int NV>
+__device__ __forceinline__ void final_sum_dd(const double *part, int stride, int n, dd_t (&out)[NV],
+                                             double *smem) {
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    dd_t a = {0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      dd_t u;
+      u.s = __ldcg(part + 2 * ((size_t)k * stride + i));
+      u.c = __ldcg(part + 2 * ((size_t)k * stride + i) + 1);
+      a = dd_merge(a, u);
+    }
+    out[k] = a;
+  }
+  block_sum_dd<NV>(out, smem);
+}
+
 // Last-block-done: every block publishes its partials, then takes a ticket;
 // the block that draws gridSize-1 sees all partials and finalises.  The
 // finaliser resets the ticket for the next launch.
@@ -267,12 +365,20 @@ struct CsrView {
   int rows, base;
 };
 
+// HLL with the reference's GPU hack size (32 = warp size,
+// psb_d_cuda_cp_hlg_from_coo.F90:60): hack and lane come from shifts and the
+// entry stride is a compile-time constant.
+struct Hll32View : HllView {};
+
 // Unrolled in-order accumulation over one row whose j-th entry sits at
-// off + j*stride.  Loads of a group are issued before its adds.
-template <class VT, class XT, int U>
-__device__ __forceinline__ double row_acc_strided(const VT *__restrict__ val, const int *__restrict__ ja,
-                                                  size_t off, size_t stride, int n,
-                                                  const XT *__restrict__ xb) {
+// vp[j*stride] / jp[j*stride] (32-bit offsets: every format keeps its
+// allocation below 2^31 entries, as psb_ipk_ does).  The U index and value
+// loads of a group are issued before its U gathers, the gathers before the
+// adds, so each thread keeps 2U streaming loads in flight.
+template <class VT, class XT, int U, int STRIDE>
+__device__ __forceinline__ double row_acc(const VT *__restrict__ vp, const int *__restrict__ jp, int stride, int n,
+                                          const XT *__restrict__ xb) {
+  const int st = STRIDE > 0 ? STRIDE : stride;
   double acc = 0.0;
   int j = 0;
   for (; j + U <= n; j += U) {
@@ -280,8 +386,8 @@ __device__ __forceinline__ double row_acc_strided(const VT *__restrict__ val, co
     VT v[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      c[u] = ld_stream(ja + off + (size_t)(j + u) * stride);
-      v[u] = ld_stream(val + off + (size_t)(j + u) * stride);
+      c[u] = ld_stream(jp + (j + u) * st);
+      v[u] = ld_stream(vp + (j + u) * st);
     }
     XT xv[U];
 #pragma unroll
@@ -290,40 +396,46 @@ __device__ __forceinline__ double row_acc_strided(const VT *__restrict__ val, co
     for (int u = 0; u < U; u++) acc = radd(acc, rmul((double)v[u], (double)xv[u]));
   }
   for (; j < n; j++) {
-    int c = ld_stream(ja + off + (size_t)j * stride);
-    VT v = ld_stream(val + off + (size_t)j * stride);
+    const int c = ld_stream(jp + j * st);
+    const VT v = ld_stream(vp + j * st);
     acc = radd(acc, rmul((double)v, (double)ld_ro(xb + c)));
   }
   return acc;
 }
 
+__device__ __forceinline__ double row_dot(const Hll32View &A, int s, const double *__restrict__ x) {
+  const int off = ld_ro(A.hkoffs + (s >> 5)) + (s & 31);
+  return row_acc<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base);
+}
+
 __device__ __forceinline__ double row_dot(const HllView &A, int s, const double *__restrict__ x) {
   const int h = s / A.hksz;
-  const int ii = s - h * A.hksz;
-  const size_t off = (size_t)ld_ro(A.hkoffs + h) + ii;
-  const int n = ld_ro(A.irn + s);
-  return row_acc_strided<double, double, 4>(A.val, A.ja, off, (size_t)A.hksz, n, x - A.base);
+  const int off = ld_ro(A.hkoffs + h) + (s - h * A.hksz);
+  return row_acc<double, double, 8, 0>(A.val + off, A.ja + off, A.hksz, ld_ro(A.irn + s), x - A.base);
 }
 
 __device__ __forceinline__ double row_dot(const HllViewF &A, int s, const float *__restrict__ x) {
   const int h = s / A.hksz;
-  const int ii = s - h * A.hksz;
-  const size_t off = (size_t)ld_ro(A.hkoffs + h) + ii;
-  const int n = ld_ro(A.irn + s);
-  return row_acc_strided<float, float, 4>(A.val, A.ja, off, (size_t)A.hksz, n, x - A.base);
+  const int off = ld_ro(A.hkoffs + h) + (s - h * A.hksz);
+  if (A.hksz == 32)
+    return row_acc<float, float, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base);
+  return row_acc<float, float, 8, 0>(A.val + off, A.ja + off, A.hksz, ld_ro(A.irn + s), x - A.base);
 }
 
 __device__ __forceinline__ double row_dot(const EllView &A, int r, const double *__restrict__ x) {
-  const int n = ld_ro(A.irn + r);
-  return row_acc_strided<double, double, 4>(A.val, A.ja, (size_t)r, (size_t)A.pitch, n, x - A.base);
+  return row_acc<double, double, 8, 0>(A.val + r, A.ja + r, A.pitch, ld_ro(A.irn + r), x - A.base);
 }
 
 __device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *__restrict__ x) {
   const int b = ld_ro(A.irp + r) - A.base, e = ld_ro(A.irp + r + 1) - A.base;
-  return row_acc_strided<double, double, 4>(A.val, A.ja, (size_t)b, 1, e - b, x - A.base);
+  return row_acc<double, double, 4, 1>(A.val + b, A.ja + b, 1, e - b, x - A.base);
 }
 
 // sum_j |val(r,j)| over the stored entries (psb_spnrmi, for istop = 1)
+__device__ __forceinline__ double row_abs_sum(const HllView &A, int s);
+__device__ __forceinline__ double row_abs_sum(const Hll32View &A, int s) {
+  return row_abs_sum(static_cast<const HllView &>(A), s);
+}
 __device__ __forceinline__ double row_abs_sum(const HllView &A, int s) {
   const int h = s / A.hksz, ii = s - h * A.hksz;
   const size_t off = (size_t)A.hkoffs[h] + ii;
@@ -343,11 +455,17 @@ __device__ __forceinline__ double row_abs_sum(const CsrView &A, int r) {
 }
 
 __device__ __forceinline__ int out_row(const HllView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
+__device__ __forceinline__ int out_row(const Hll32View &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const HllViewF &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const EllView &, int r) { return r; }
 __device__ __forceinline__ int out_row(const CsrView &, int r) { return r; }
 
 HllView hll_view(const HllDevice *m);
+static inline Hll32View hll32_view(const HllView &v) {
+  Hll32View w;
+  static_cast<HllView &>(w) = v;
+  return w;
+}
 EllView ell_view(const EllDevice *m);
 CsrView csr_view(const CsrDevice *m);
 

@@ -79,48 +79,78 @@ __device__ __forceinline__ int check_conv(KState *S, double sum_rr, double amax_
   return res || (S->itmax <= S->itx);
 }
 
+// Partials: lane k of block b at part[2*(k*grid + b)] (pairs for the
+// compensated sums, first slot only for maxima).  Lanes 0-1: sums; 2-3: max.
+template <int NS>
+__device__ __forceinline__ void publish_sums(double *part, int grid, const dd_t (&v)[NS]) {
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      part[2 * ((size_t)k * grid + blockIdx.x)] = v[k].s;
+      part[2 * ((size_t)k * grid + blockIdx.x) + 1] = v[k].c;
+    }
+  }
+}
+
+__device__ __forceinline__ void publish_max2(double *part, int grid, const double (&m)[2]) {
+  if (threadIdx.x == 0) {
+    part[2 * ((size_t)2 * grid + blockIdx.x)] = m[0];
+    part[2 * ((size_t)3 * grid + blockIdx.x)] = m[1];
+  }
+}
+
+__device__ __forceinline__ void final_max2(const double *part, int grid, int n, double (&m)[2], double *smem) {
+  m[0] = 0.0;
+  m[1] = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    m[0] = fmax(m[0], __ldcg(part + 2 * ((size_t)2 * grid + i)));
+    m[1] = fmax(m[1], __ldcg(part + 2 * ((size_t)3 * grid + i)));
+  }
+  block_max<2>(m, smem);
+}
+
 // ---------------------------------------------------------------- setup
-// bn2 = ||b||_2, bni = ||b||_inf; with istop 1 also ani = ||A||_inf (row abs
-// sums of the stored entries).
+// bn2 = ||b||_2, bni = ||b||_inf.
 __global__ void __launch_bounds__(KT) k_kry_setup(int n, const double *__restrict__ b, KState *S,
                                                   double *__restrict__ part, unsigned *__restrict__ ticket,
                                                   int grid) {
-  __shared__ double sm[64];
-  double s[1] = {0.0}, m[1] = {0.0};
+  __shared__ double sm[128];
+  dd_t s[1] = {{0.0, 0.0}};
+  double m[2] = {0.0, 0.0};
   for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
     const double v = b[i];
-    s[0] = radd(s[0], rmul(v, v));
+    dd_add_prod(s[0], v, v);
     m[0] = fmax(m[0], fabs(v));
   }
-  block_sum<1>(s, sm);
-  block_max<1>(m, sm + 32);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = s[0];
-    part[grid + blockIdx.x] = m[0];
-  }
+  block_sum_dd<1>(s, sm);
+  block_max<2>(m, sm + 64);
+  publish_sums<1>(part, grid, s);
+  publish_max2(part, grid, m);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[1], mm[1];
-    final_sum<1>(part, 0, gridDim.x, o, sm);
-    final_max<1>(part + grid, 0, gridDim.x, mm, sm + 32);
+    dd_t o[1];
+    double mm[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, mm, sm + 64);
     if (threadIdx.x == 0) {
-      S->bn2 = sqrt(o[0]);
+      S->bn2 = sqrt(dd_value(o[0]));
       S->bni = mm[0];
       *ticket = 0;
     }
   }
 }
 
+// ani = ||A||_inf from the stored entries (psb_spnrmi, for istop 1).
 template <class View>
 __global__ void __launch_bounds__(KT) k_kry_normi(View A, KState *S, double *__restrict__ part,
-                                                  unsigned *__restrict__ ticket) {
-  __shared__ double sm[32];
-  double m[1] = {0.0};
+                                                  unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[64];
+  double m[2] = {0.0, 0.0};
   for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) m[0] = fmax(m[0], row_abs_sum(A, s));
-  block_max<1>(m, sm);
-  if (threadIdx.x == 0) part[blockIdx.x] = m[0];
+  block_max<2>(m, sm);
+  publish_max2(part, grid, m);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[1];
-    final_max<1>(part, 0, gridDim.x, o, sm);
+    double o[2];
+    final_max2(part, grid, gridDim.x, o, sm);
     if (threadIdx.x == 0) {
       S->ani = o[0];
       *ticket = 0;
@@ -129,15 +159,15 @@ __global__ void __launch_bounds__(KT) k_kry_normi(View A, KState *S, double *__r
 }
 
 // ---------------------------------------------------------------- CG
-// restart: r = b - A*x; z = M^-1 r; rho = (r,z); rr = (r,r) for istop 3.
+// restart: r = b - A*x; z = M^-1 r; rho = (r,z); (r,r) for istop 3.
 template <class View>
 __global__ void __launch_bounds__(KT) k_cg_init(View A, KState *S, const double *__restrict__ b,
                                                 const double *__restrict__ x, const double *__restrict__ dinv,
                                                 double *__restrict__ r, double *__restrict__ z,
                                                 double *__restrict__ part, unsigned *__restrict__ ticket,
                                                 int grid) {
-  __shared__ double sm[64];
-  double acc[2] = {0.0, 0.0};
+  __shared__ double sm[128];
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
   for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
     const double ax = row_dot(A, s, x);
     const int i = out_row(A, s);
@@ -146,21 +176,18 @@ __global__ void __launch_bounds__(KT) k_cg_init(View A, KState *S, const double 
     const double zi = prec(dinv, i, ri);
     r[i] = ri;
     z[i] = zi;
-    acc[0] = radd(acc[0], rmul(ri, zi));
-    acc[1] = radd(acc[1], rmul(ri, ri));
+    dd_add_prod(acc[0], ri, zi);
+    dd_add_prod(acc[1], ri, ri);
   }
-  block_sum<2>(acc, sm);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc[0];
-    part[grid + blockIdx.x] = acc[1];
-  }
+  block_sum_dd<2>(acc, sm);
+  publish_sums<2>(part, grid, acc);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[2];
-    final_sum<2>(part, grid, gridDim.x, o, sm);
+    dd_t o[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
     if (threadIdx.x == 0) {
-      if (S->istop == 3) S->r0n2 = sqrt(o[1]);  // init_conv inside CG's restart loop
+      if (S->istop == 3) S->r0n2 = sqrt(dd_value(o[1]));  // init_conv inside CG's restart loop
       S->rho_old = 0.0;
-      S->rho = o[0];
+      S->rho = dd_value(o[0]);
       S->it = 1;
       S->itx = S->itx + 1;
       S->status = ST_RUN;
@@ -182,25 +209,26 @@ __global__ void __launch_bounds__(KT) k_cg_p(KState *S, int n, const double *__r
 template <class View>
 __global__ void __launch_bounds__(KT) k_cg_spmv(View A, KState *S, const double *__restrict__ p,
                                                 double *__restrict__ q, double *__restrict__ part,
-                                                unsigned *__restrict__ ticket) {
-  __shared__ double sm[32];
+                                                unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[64];
   if (stopped(S)) return;
-  double acc[1] = {0.0};
+  dd_t acc[1] = {{0.0, 0.0}};
   for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
     const double t = row_dot(A, s, p);
     const int i = out_row(A, s);
     q[i] = t;
-    acc[0] = radd(acc[0], rmul(ld_ro(p + i), t));
+    dd_add_prod(acc[0], ld_ro(p + i), t);
   }
-  block_sum<1>(acc, sm);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[1];
-    final_sum<1>(part, 0, gridDim.x, o, sm);
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
     if (threadIdx.x == 0) {
-      S->sigma = o[0];
-      if (o[0] == 0.0) S->status = ST_BREAK;  // psb_dcg.F90:265-270
-      else S->alpha = S->rho / o[0];
+      const double sigma = dd_value(o[0]);
+      S->sigma = sigma;
+      if (sigma == 0.0) S->status = ST_BREAK;  // psb_dcg.F90:265-270
+      else S->alpha = S->rho / sigma;
       *ticket = 0;
     }
   }
@@ -212,10 +240,11 @@ __global__ void __launch_bounds__(KT) k_cg_update(KState *S, int n, const double
                                                   double *__restrict__ x, double *__restrict__ r,
                                                   double *__restrict__ z, double *__restrict__ part,
                                                   unsigned *__restrict__ ticket, int grid) {
-  __shared__ double sm[128];
+  __shared__ double sm[192];
   if (stopped(S)) return;
   const double alpha = S->alpha, malpha = -S->alpha;
-  double acc[2] = {0.0, 0.0}, mx[2] = {0.0, 0.0};
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
   for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
     const double xi = radd(rmul(alpha, p[i]), x[i]);
     const double ri = radd(rmul(malpha, q[i]), r[i]);
@@ -223,32 +252,29 @@ __global__ void __launch_bounds__(KT) k_cg_update(KState *S, int n, const double
     x[i] = xi;
     r[i] = ri;
     z[i] = zi;
-    acc[0] = radd(acc[0], rmul(ri, zi));
-    acc[1] = radd(acc[1], rmul(ri, ri));
+    dd_add_prod(acc[0], ri, zi);
+    dd_add_prod(acc[1], ri, ri);
     mx[0] = fmax(mx[0], fabs(ri));
     mx[1] = fmax(mx[1], fabs(xi));
   }
-  block_sum<2>(acc, sm);
-  block_max<2>(mx, sm + 64);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc[0];
-    part[grid + blockIdx.x] = acc[1];
-    part[2 * grid + blockIdx.x] = mx[0];
-    part[3 * grid + blockIdx.x] = mx[1];
-  }
+  block_sum_dd<2>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<2>(part, grid, acc);
+  publish_max2(part, grid, mx);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[2], m[2];
-    final_sum<2>(part, grid, gridDim.x, o, sm);
-    final_max<2>(part + 2 * grid, grid, gridDim.x, m, sm + 64);
+    dd_t o[2];
+    double m[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
     if (threadIdx.x == 0) {
-      if (check_conv(S, o[1], m[0], m[1])) {
+      if (check_conv(S, dd_value(o[1]), m[0], m[1])) {
         S->status = ST_DONE;
       } else {
         // next iteration: rho_old = rho; rho = (r,z); breakdown on rho_old
         S->it += 1;
         S->itx += 1;
         S->rho_old = S->rho;
-        S->rho = o[0];
+        S->rho = dd_value(o[0]);
         if (S->rho_old == 0.0) S->status = ST_BREAK;  // psb_dcg.F90:253-258
         else S->beta = S->rho / S->rho_old;
       }
@@ -264,42 +290,42 @@ __global__ void __launch_bounds__(KT) k_bcg_init(View A, KState *S, const double
                                                  const double *__restrict__ x, double *__restrict__ r,
                                                  double *__restrict__ q, double *__restrict__ part,
                                                  unsigned *__restrict__ ticket, int grid) {
-  __shared__ double sm[128];
-  double acc[1] = {0.0}, mx[2] = {0.0, 0.0};
+  __shared__ double sm[192];
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
   for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
     const double ax = row_dot(A, s, x);
     const int i = out_row(A, s);
     const double ri = radd(rmul(-1.0, ax), b[i]);
     r[i] = ri;
     q[i] = ri;
-    acc[0] = radd(acc[0], rmul(ri, ri));
+    dd_add_prod(acc[0], ri, ri);
     mx[0] = fmax(mx[0], fabs(ri));
     mx[1] = fmax(mx[1], fabs(ld_ro(x + i)));
   }
-  block_sum<1>(acc, sm);
-  block_max<2>(mx, sm + 64);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc[0];
-    part[2 * grid + blockIdx.x] = mx[0];
-    part[3 * grid + blockIdx.x] = mx[1];
-  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[1], m[2];
-    final_sum<1>(part, 0, gridDim.x, o, sm);
-    final_max<2>(part + 2 * grid, grid, gridDim.x, m, sm + 64);
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
     if (threadIdx.x == 0) {
+      const double rr = dd_value(o[0]);
       if (S->istop == 3 && !S->r0set) {  // init_conv outside the restart loop
-        S->r0n2 = sqrt(o[0]);
+        S->r0n2 = sqrt(rr);
         S->r0set = 1;
       }
-      if (check_conv(S, o[0], m[0], m[1])) {
+      if (check_conv(S, rr, m[0], m[1])) {
         S->status = ST_DONE;
       } else {
         S->it = 1;
         S->itx += 1;
         S->rho_old = 0.0;
-        S->rho = o[0];  // (q,r) with q == r
-        S->status = (o[0] == 0.0) ? ST_BREAK : ST_RUN;  // psb_dcgstab.f90:267
+        S->rho = rr;  // (q,r) with q == r
+        S->status = (rr == 0.0) ? ST_BREAK : ST_RUN;  // psb_dcgstab.f90:267
       }
       *ticket = 0;
     }
@@ -330,25 +356,27 @@ __global__ void __launch_bounds__(KT) k_bcg_p(KState *S, int n, const double *__
 template <class View>
 __global__ void __launch_bounds__(KT) k_bcg_spmv1(View A, KState *S, const double *__restrict__ f,
                                                   const double *__restrict__ q, double *__restrict__ v,
-                                                  double *__restrict__ part, unsigned *__restrict__ ticket) {
-  __shared__ double sm[32];
+                                                  double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                  int grid) {
+  __shared__ double sm[64];
   if (stopped(S)) return;
-  double acc[1] = {0.0};
+  dd_t acc[1] = {{0.0, 0.0}};
   for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
     const double t = row_dot(A, s, f);
     const int i = out_row(A, s);
     v[i] = t;
-    acc[0] = radd(acc[0], rmul(ld_ro(q + i), t));
+    dd_add_prod(acc[0], ld_ro(q + i), t);
   }
-  block_sum<1>(acc, sm);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[1];
-    final_sum<1>(part, 0, gridDim.x, o, sm);
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
     if (threadIdx.x == 0) {
-      S->sigma = o[0];
-      if (o[0] == 0.0) S->status = ST_BREAK;  // psb_dcgstab.f90:298
-      else S->alpha = S->rho / o[0];
+      const double sigma = dd_value(o[0]);
+      S->sigma = sigma;
+      if (sigma == 0.0) S->status = ST_BREAK;  // psb_dcgstab.f90:298
+      else S->alpha = S->rho / sigma;
       *ticket = 0;
     }
   }
@@ -373,31 +401,29 @@ __global__ void __launch_bounds__(KT) k_bcg_spmv2(View A, KState *S, const doubl
                                                   const double *__restrict__ sv, double *__restrict__ t,
                                                   double *__restrict__ part, unsigned *__restrict__ ticket,
                                                   int grid) {
-  __shared__ double sm[64];
+  __shared__ double sm[128];
   if (stopped(S)) return;
-  double acc[2] = {0.0, 0.0};
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
   for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
     const double ti = row_dot(A, s, z);
     const int i = out_row(A, s);
     t[i] = ti;
-    acc[0] = radd(acc[0], rmul(ti, ti));
-    acc[1] = radd(acc[1], rmul(ti, ld_ro(sv + i)));
+    dd_add_prod(acc[0], ti, ti);
+    dd_add_prod(acc[1], ti, ld_ro(sv + i));
   }
-  block_sum<2>(acc, sm);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc[0];
-    part[grid + blockIdx.x] = acc[1];
-  }
+  block_sum_dd<2>(acc, sm);
+  publish_sums<2>(part, grid, acc);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[2];
-    final_sum<2>(part, grid, gridDim.x, o, sm);
+    dd_t o[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
     if (threadIdx.x == 0) {
-      S->sigma = o[0];
-      if (o[0] == 0.0) {
+      const double sigma = dd_value(o[0]);
+      S->sigma = sigma;
+      if (sigma == 0.0) {
         S->status = ST_BREAK;  // psb_dcgstab.f90:328
       } else {
-        S->tau = o[1];
-        S->omega = o[1] / o[0];
+        S->tau = dd_value(o[1]);
+        S->omega = S->tau / sigma;
         if (S->omega == 0.0) S->status = ST_BREAK;  // psb_dcgstab.f90:346
       }
       *ticket = 0;
@@ -413,42 +439,40 @@ __global__ void __launch_bounds__(KT) k_bcg_update(KState *S, int n, const doubl
                                                    double *__restrict__ x, double *__restrict__ r,
                                                    double *__restrict__ part, unsigned *__restrict__ ticket,
                                                    int grid) {
-  __shared__ double sm[128];
+  __shared__ double sm[192];
   if (stopped(S)) return;
   const double alpha = S->alpha, omega = S->omega, momega = -S->omega;
-  double acc[2] = {0.0, 0.0}, mx[2] = {0.0, 0.0};
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
   for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
     double xi = radd(rmul(alpha, f[i]), x[i]);
     xi = radd(rmul(omega, z[i]), xi);
     const double ri = radd(rmul(momega, t[i]), s[i]);
     x[i] = xi;
     r[i] = ri;
-    acc[0] = radd(acc[0], rmul(ld_ro(q + i), ri));
-    acc[1] = radd(acc[1], rmul(ri, ri));
+    dd_add_prod(acc[0], ld_ro(q + i), ri);
+    dd_add_prod(acc[1], ri, ri);
     mx[0] = fmax(mx[0], fabs(ri));
     mx[1] = fmax(mx[1], fabs(xi));
   }
-  block_sum<2>(acc, sm);
-  block_max<2>(mx, sm + 64);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc[0];
-    part[grid + blockIdx.x] = acc[1];
-    part[2 * grid + blockIdx.x] = mx[0];
-    part[3 * grid + blockIdx.x] = mx[1];
-  }
+  block_sum_dd<2>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<2>(part, grid, acc);
+  publish_max2(part, grid, mx);
   if (psbx_last_block(ticket, gridDim.x)) {
-    double o[2], m[2];
-    final_sum<2>(part, grid, gridDim.x, o, sm);
-    final_max<2>(part + 2 * grid, grid, gridDim.x, m, sm + 64);
+    dd_t o[2];
+    double m[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
     if (threadIdx.x == 0) {
-      if (check_conv(S, o[1], m[0], m[1])) {
+      if (check_conv(S, dd_value(o[1]), m[0], m[1])) {
         S->status = ST_DONE;
       } else {
         S->it += 1;
         S->itx += 1;
         S->rho_old = S->rho;
-        S->rho = o[0];
-        if (o[0] == 0.0) S->status = ST_BREAK;  // psb_dcgstab.f90:267
+        S->rho = dd_value(o[0]);
+        if (S->rho == 0.0) S->status = ST_BREAK;  // psb_dcgstab.f90:267
         else S->beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
       }
       *ticket = 0;
@@ -537,7 +561,7 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
   KState *S = nullptr;
   unsigned *ticket = nullptr;
   PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * (size_t)nvec * (size_t)(n > 0 ? n : 1), st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * KLANES * (size_t)grid, st));
+  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
   PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
   PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
@@ -561,7 +585,7 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
   k_kry_setup<<<grid, KT, 0, st>>>(n, b, S, part, ticket, grid);
   psbx_count_launch();
   if (opt->istop == 1) {
-    k_kry_normi<View><<<grid, KT, 0, st>>>(A, S, part, ticket);
+    k_kry_normi<View><<<grid, KT, 0, st>>>(A, S, part, ticket, grid);
     psbx_count_launch();
   }
 
@@ -574,11 +598,11 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     for (int k = 0; k < KGRAPH_ITERS; k++) {
       if (!bicg) {
         k_cg_p<<<grid, KT, 0, st>>>(S, n, v3, v0);
-        k_cg_spmv<View><<<grid, KT, 0, st>>>(A, S, v0, v1, part, ticket);
+        k_cg_spmv<View><<<grid, KT, 0, st>>>(A, S, v0, v1, part, ticket, grid);
         k_cg_update<<<grid, KT, 0, st>>>(S, n, v0, v1, dinv, x, v2, v3, part, ticket, grid);
       } else {
         k_bcg_p<<<grid, KT, 0, st>>>(S, n, v1, v3, dinv, v2, v7);
-        k_bcg_spmv1<View><<<grid, KT, 0, st>>>(A, S, v7, v0, v3, part, ticket);
+        k_bcg_spmv1<View><<<grid, KT, 0, st>>>(A, S, v7, v0, v3, part, ticket, grid);
         k_bcg_s<<<grid, KT, 0, st>>>(S, n, v1, v3, dinv, v4, v6);
         k_bcg_spmv2<View><<<grid, KT, 0, st>>>(A, S, v6, v4, v5, part, ticket, grid);
         k_bcg_update<<<grid, KT, 0, st>>>(S, n, v7, v6, v4, v5, v0, x, v1, part, ticket, grid);
@@ -663,6 +687,8 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
   if (fmt == PSBX_FMT_HLL) {
     HllDevice *m = (HllDevice *)mat;
     if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+    if (m->hackSize == 32)
+      return solve(hll32_view(hll_view(m)), bicg, dv, (const double *)B->v_, (double *)X->v_, n, opt);
     return solve(hll_view(m), bicg, dv, (const double *)B->v_, (double *)X->v_, n, opt);
   }
   if (fmt == PSBX_FMT_ELL)

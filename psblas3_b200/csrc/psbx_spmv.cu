@@ -102,6 +102,7 @@ int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, doub
                          cudaStream_t st) {
   if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
   if (alpha == 0.0 && m->perm == nullptr) return psbx_launch_scale(m->rows, beta, y, st);
+  if (m->hackSize == 32) return launch_rows(hll32_view(hll_view(m)), alpha, x, beta, y, st);
   return launch_rows(hll_view(m), alpha, x, beta, y, st);
 }
 

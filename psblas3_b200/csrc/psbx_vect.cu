@@ -209,58 +209,78 @@ __global__ void k_abs(int n, double alpha, const double *__restrict__ a, double 
 enum { R_DOT = 0, R_NRM2 = 1, R_ASUM = 2, R_AMAX = 3 };
 
 // One partial per block per vector (blockIdx.y), finalised by the last block.
+// DOT and NRM2 accumulate compensated pairs (Dot2); ASUM is a plain sum;
+// AMAX a max.  Partials of vector v, block b: part[2*(v*PSBX_MAX_PART + b)].
 template <int OP>
 __global__ void __launch_bounds__(256) k_reduce(int n, const double *__restrict__ x, int px,
                                                 const double *__restrict__ y, int py,
                                                 double *__restrict__ part, unsigned *__restrict__ ticket,
                                                 double *__restrict__ res) {
-  __shared__ double sm[32];
+  __shared__ double sm[64];
   const int v = blockIdx.y;
   const double *xv = x + (size_t)v * px;
-  const double *yv = OP == R_DOT ? y + (size_t)v * py : nullptr;
-  double acc[1] = {0.0};
+  const double *yv = OP == R_DOT ? y + (size_t)v * py : xv;
   const int stride = gridDim.x * blockDim.x;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  for (; i + 3 * stride < n; i += 4 * stride) {
-    double a0 = ld_stream(xv + i), a1 = ld_stream(xv + i + stride);
-    double a2 = ld_stream(xv + i + 2 * stride), a3 = ld_stream(xv + i + 3 * stride);
-    if (OP == R_DOT) {
-      double b0 = ld_stream(yv + i), b1 = ld_stream(yv + i + stride);
-      double b2 = ld_stream(yv + i + 2 * stride), b3 = ld_stream(yv + i + 3 * stride);
-      acc[0] = radd(acc[0], rmul(a0, b0));
-      acc[0] = radd(acc[0], rmul(a1, b1));
-      acc[0] = radd(acc[0], rmul(a2, b2));
-      acc[0] = radd(acc[0], rmul(a3, b3));
-    } else if (OP == R_NRM2) {
-      acc[0] = radd(acc[0], rmul(a0, a0));
-      acc[0] = radd(acc[0], rmul(a1, a1));
-      acc[0] = radd(acc[0], rmul(a2, a2));
-      acc[0] = radd(acc[0], rmul(a3, a3));
-    } else if (OP == R_ASUM) {
-      acc[0] = radd(acc[0], fabs(a0));
-      acc[0] = radd(acc[0], fabs(a1));
-      acc[0] = radd(acc[0], fabs(a2));
-      acc[0] = radd(acc[0], fabs(a3));
-    } else {
-      acc[0] = fmax(acc[0], fmax(fmax(fabs(a0), fabs(a1)), fmax(fabs(a2), fabs(a3))));
+  double *pv = part + 2 * (size_t)v * PSBX_MAX_PART;
+  if (OP == R_DOT || OP == R_NRM2) {
+    dd_t acc[1] = {{0.0, 0.0}};
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+      const double a0 = ld_stream(xv + i), a1 = ld_stream(xv + i + stride);
+      const double a2 = ld_stream(xv + i + 2 * stride), a3 = ld_stream(xv + i + 3 * stride);
+      double b0 = a0, b1 = a1, b2 = a2, b3 = a3;
+      if (OP == R_DOT) {
+        b0 = ld_stream(yv + i);
+        b1 = ld_stream(yv + i + stride);
+        b2 = ld_stream(yv + i + 2 * stride);
+        b3 = ld_stream(yv + i + 3 * stride);
+      }
+      dd_add_prod(acc[0], a0, b0);
+      dd_add_prod(acc[0], a1, b1);
+      dd_add_prod(acc[0], a2, b2);
+      dd_add_prod(acc[0], a3, b3);
     }
+    for (; i < n; i += stride) {
+      const double a = ld_stream(xv + i);
+      dd_add_prod(acc[0], a, OP == R_DOT ? ld_stream(yv + i) : a);
+    }
+    block_sum_dd<1>(acc, sm);
+    if (threadIdx.x == 0) {
+      pv[2 * blockIdx.x] = acc[0].s;
+      pv[2 * blockIdx.x + 1] = acc[0].c;
+    }
+    if (psbx_last_block(ticket + v, gridDim.x)) {
+      dd_t out[1];
+      final_sum_dd<1>(pv, 0, gridDim.x, out, sm);
+      if (threadIdx.x == 0) {
+        const double t = dd_value(out[0]);
+        res[v] = OP == R_NRM2 ? sqrt(t) : t;
+        ticket[v] = 0;
+      }
+    }
+    return;
   }
-  for (; i < n; i += stride) {
-    double a = ld_stream(xv + i);
-    if (OP == R_DOT) acc[0] = radd(acc[0], rmul(a, ld_stream(yv + i)));
-    else if (OP == R_NRM2) acc[0] = radd(acc[0], rmul(a, a));
-    else if (OP == R_ASUM) acc[0] = radd(acc[0], fabs(a));
-    else acc[0] = fmax(acc[0], fabs(a));
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double a = ld_stream(xv + i);
+    acc[0] = OP == R_ASUM ? radd(acc[0], fabs(a)) : fmax(acc[0], fabs(a));
   }
   if (OP == R_AMAX) block_max<1>(acc, sm);
   else block_sum<1>(acc, sm);
-  if (threadIdx.x == 0) part[(size_t)v * PSBX_MAX_PART + blockIdx.x] = acc[0];
+  if (threadIdx.x == 0) pv[2 * blockIdx.x] = acc[0];
   if (psbx_last_block(ticket + v, gridDim.x)) {
     double out[1];
-    if (OP == R_AMAX) final_max<1>(part + (size_t)v * PSBX_MAX_PART, 0, gridDim.x, out, sm);
-    else final_sum<1>(part + (size_t)v * PSBX_MAX_PART, 0, gridDim.x, out, sm);
+    double s = 0.0, m = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+      const double t = __ldcg(pv + 2 * k);
+      s = radd(s, t);
+      m = fmax(m, t);
+    }
+    out[0] = OP == R_AMAX ? m : s;
+    if (OP == R_AMAX) block_max<1>(out, sm);
+    else block_sum<1>(out, sm);
     if (threadIdx.x == 0) {
-      res[v] = OP == R_NRM2 ? sqrt(out[0]) : out[0];
+      res[v] = out[0];
       ticket[v] = 0;
     }
   }
