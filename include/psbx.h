@@ -273,6 +273,27 @@ void *psbx_multivec_data(void *deviceVec);
  * (x, y: double, y may not alias x) on the library stream, asynchronously. */
 int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x,
                       double beta, double *y);
+/* Allocation-free dot products.  No counterpart in the reference: it is a
+ * variant of dotMultiVecDeviceDouble for callers that cannot let a library
+ * call cudaMalloc -- code that owns all device memory through its own pool or
+ * a fixed budget, and latency-critical loops where an allocation would
+ * synchronise the device.  It allocates nothing: its scratch is a fixed
+ * file-scope device array (512 KiB of partial sums plus 8 counters, held on
+ * every GPU that loads the library until the process exits).
+ *   d_res   device pointer to count doubles: d_res[k] = sum_i x_k[i]*y_k[i]
+ *   n       entries per vector; count 1..8 vectors (more is rejected with
+ *           SPGPU_UNSUPPORTED and a message), pitch = entries between the
+ *           vectors of x and of y (ignored when count == 1)
+ *   x, y    device pointers; stream: cudaStream_t (NULL: default stream)
+ * The call is asynchronous on the stream and allocates nothing.  The first
+ * call on each device looks up the scratch's device address, so make that
+ * first call before any stream capture.  All calls share the one scratch
+ * array: calls whose kernels overlap on the GPU (different streams, or
+ * different host threads) race and give wrong results; order them.  Results
+ * equal dotMultiVecDeviceDouble's (same kernel, same compensated sum). */
+int psbx_dot_noalloc(double *d_res, int n, int count, const double *x, const double *y, int pitch,
+                     void *stream);
+
 /* Number of kernels launched by the library since load (for accounting). */
 uint64_t psbx_kernel_launches(void);
 /* Last CUDA error string seen by the library (static storage). */

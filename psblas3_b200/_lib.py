@@ -88,6 +88,7 @@ _SIGS = {
     "psbx_hll_make_single": (I, [P]),
     "psbx_wrapMultiVecDevice": (I, [PP, P, U, U]), "psbx_multivec_data": (P, [P]),
     "psbx_hll_spmv_raw": (I, [P, D, P, D, P]),
+    "psbx_dot_noalloc": (I, [P, I, I, P, P, I, P]),
     "psbx_kernel_launches": (C.c_uint64, []), "psbx_last_error": (C.c_char_p, []),
 }
 

@@ -23,6 +23,11 @@ int psbx_cuda_status(cudaError_t e, const char *where) {
   return SPGPU_UNSPECIFIED;
 }
 
+void psbx_set_error(const char *msg) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+  fprintf(stderr, "libpsbx: %s\n", g_last_error);
+}
+
 static int ctx_create(int dev) {
   PsbxCtx &c = g_ctx;
   PSBX_CK(cudaSetDevice(dev));

@@ -461,3 +461,78 @@ int absMultiVecDeviceDouble(int n, double alpha, void *devVecA) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free dot products.
+//
+// dotMultiVecDeviceDouble keeps its per-block partial sums in scratch that
+// the library allocates with cudaMalloc the first time it is used.  Some
+// callers cannot let a library call cudaMalloc: code that owns every byte
+// of device memory through its own pool or a fixed budget, and latency-
+// critical loops where an allocation would synchronise the device.  For
+// them psbx_dot_noalloc runs the same reduction kernel with its scratch in
+// the file-scope device arrays below (512 KiB of partial pairs plus 8
+// tickets, present on every GPU that loads the library until the process
+// exits) and allocates nothing.
+// ---------------------------------------------------------------------------
+#define PSBX_NOALLOC_MAX_VECS PSBX_NLANES
+#define PSBX_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) double psbx_noalloc_part[2 * PSBX_NLANES * PSBX_MAX_PART];
+static __device__ __align__(256) unsigned psbx_noalloc_ticket[PSBX_NLANES];
+
+static double *g_na_part[PSBX_NOALLOC_MAX_DEVICES];
+static unsigned *g_na_ticket[PSBX_NOALLOC_MAX_DEVICES];
+static int g_na_sms[PSBX_NOALLOC_MAX_DEVICES];
+static bool g_na_ready[PSBX_NOALLOC_MAX_DEVICES];
+
+void psbx_set_error(const char *msg);
+
+// Once per device, with that device current: the device addresses of the
+// scratch arrays (in host code their names are host-side stand-ins, not
+// device addresses) and the SM count for the grid size.
+static int noalloc_setup(int dev) {
+  if (g_na_ready[dev]) return SPGPU_SUCCESS;
+  cudaError_t e = cudaGetSymbolAddress((void **)&g_na_part[dev], psbx_noalloc_part);
+  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaGetSymbolAddress(psbx_noalloc_part)");
+  e = cudaGetSymbolAddress((void **)&g_na_ticket[dev], psbx_noalloc_ticket);
+  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaGetSymbolAddress(psbx_noalloc_ticket)");
+  e = cudaDeviceGetAttribute(&g_na_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaDeviceGetAttribute");
+  g_na_ready[dev] = true;
+  return SPGPU_SUCCESS;
+}
+
+extern "C" int psbx_dot_noalloc(double *d_res, int n, int count, const double *x, const double *y, int pitch,
+                                void *stream) {
+  if (count < 1 || count > PSBX_NOALLOC_MAX_VECS) {
+    psbx_set_error("psbx_dot_noalloc: count must be between 1 and 8 (the size of its fixed scratch)");
+    return SPGPU_UNSUPPORTED;
+  }
+  if (n < 0 || !d_res || !x || !y || (count > 1 && pitch < n)) {
+    psbx_set_error("psbx_dot_noalloc: invalid arguments");
+    return SPGPU_UNSUPPORTED;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaGetDevice");
+  if (dev < 0 || dev >= PSBX_NOALLOC_MAX_DEVICES) {
+    psbx_set_error("psbx_dot_noalloc: device ordinal beyond 63");
+    return SPGPU_UNSUPPORTED;
+  }
+  int rc = noalloc_setup(dev);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the tickets must start at zero; the array keeps the previous call's state
+  e = cudaMemsetAsync(g_na_ticket[dev], 0, sizeof(unsigned) * PSBX_NOALLOC_MAX_VECS, st);
+  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaMemsetAsync(ticket)");
+  long long blocks = ((long long)(n > 0 ? n : 1) + VT * 4 - 1) / (VT * 4);
+  long long cap = (long long)g_na_sms[dev] * 4;
+  int g = (int)(blocks < cap ? blocks : cap);
+  if (g > PSBX_MAX_PART) g = PSBX_MAX_PART;
+  if (g < 1) g = 1;
+  const int px = count > 1 ? pitch : n;
+  k_reduce<R_DOT><<<dim3(g, count), VT, 0, st>>>(n, x, px, y, px, g_na_part[dev], g_na_ticket[dev], d_res);
+  PSBX_LAUNCH_CK("k_reduce (noalloc)");
+  return SPGPU_SUCCESS;
+}
