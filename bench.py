@@ -67,8 +67,16 @@ class ClockSampler:
 
     def __init__(self, index, period=0.005):
         self.index, self.period = index, period
-        self.samples, self.reasons, self.smax = [], set(), None
+        self.samples, self.stamps, self.reasons, self.smax = [], [], set(), None
         self._stop = None
+        self.t_start = self.t_stop = None
+
+    def start(self):
+        """Marks the start of the timed region (sampling runs before it)."""
+        self.t_start = time.perf_counter()
+
+    def stop(self):
+        self.t_stop = time.perf_counter()
 
     def _run(self):
         import pynvml as N
@@ -79,6 +87,7 @@ class ClockSampler:
         h = N.nvmlDeviceGetHandleByIndex(self.index)
         self.smax = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
         while not self._stop.is_set():
+            self.stamps.append(time.perf_counter())
             self.samples.append(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
             try:
                 r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
@@ -113,8 +122,10 @@ class ClockSampler:
             self._t.join(timeout=2)
 
     def summary(self):
-        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
-                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+        inside = [c for c, t in zip(self.samples, self.stamps)
+                  if self.t_start is None or (self.t_start <= t <= (self.t_stop or t))]
+        return {"sm_mhz": statistics.median(inside) if inside else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(inside)}
 
 
 def dist_setup():
@@ -199,6 +210,334 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _time_spmv(mat, X, Y, steps, stream):
+    import torch
+    for _ in range(3):
+        mat.spmv(1.0, X, 0.0, Y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        mat.spmv(1.0, X, 0.0, Y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _host_ell(irp, ja, va):
+    """ELL arrays (nzm x n, column-major by row, padding = last column of the
+    row, value 0) from 1-based CSR, as psi_d_convert_ell_from_coo lays them."""
+    n = len(irp) - 1
+    irn = np.diff(irp).astype(np.int32)
+    nzm = int(irn.max())
+    ia = np.repeat(np.arange(n), irn)
+    pos = np.arange(len(ja)) - (irp[ia].astype(np.int64) - 1)
+    last = ja[np.maximum(irp[1:].astype(np.int64) - 2, 0)]
+    eja = np.repeat(last[None, :], nzm, axis=0).astype(np.int32)
+    eva = np.zeros((nzm, n))
+    eja[pos, ia] = ja
+    eva[pos, ia] = va
+    idiag = np.zeros(n, np.int32)
+    d = ja == ia + 1
+    idiag[ia[d]] = pos[d] + 1
+    return nzm, irn, eja.ravel(), eva.ravel(), idiag
+
+
+def _part(out, name, fn):
+    """Runs one sub-benchmark; a failure is recorded, not fatal."""
+    import torch
+    t0 = time.perf_counter()
+    try:
+        out[name] = fn()
+    except Exception as e:  # keep the other measurements
+        out[name] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    print(f"[bench] {name}: {time.perf_counter() - t0:.1f} s {json.dumps(out[name])[:300]}", file=sys.stderr,
+          flush=True)
+
+
+def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
+    """Other configurations of the workload set, timed the same way (CUDA
+    events on the library stream): C2a in ELL and CSR, the C2b power-law
+    matrix, the C1 BiCGSTAB solve (with the oracle's CPU time), the C3 CG
+    solve in FP64 and in mixed precision, C4 batched and C5 serving."""
+    import torch
+    import oracle as O
+    out = {}
+    n, nnz = len(irp) - 1, len(ja)
+    B = algorithmic_bytes(n, nnz)
+    steps = max(10, min(args.steps, 50))
+
+    def c2a_formats():
+        X, Y = psb.DVect.bld(x_host), psb.DVect(n)
+        res = {}
+        nzm, irn, eja, eva, idiag = _host_ell(irp, ja, va)
+        E = psb.EllMat.from_host_ell(n, nzm, irn, eja, eva, idiag, n, nnz=nnz)
+        del eja, eva
+        ms = _time_spmv(E, X, Y, steps, stream)
+        res["ell"] = {"gb_s": B / ms / 1e6, "ms": ms, "bitexact_vs_hll": bool(np.array_equal(Y.get_vect(), y_ref))}
+        E.free()
+        Cm = psb.CsrMat(n, irp, ja, va)
+        ms = _time_spmv(Cm, X, Y, steps, stream)
+        res["csr"] = {"gb_s": B / ms / 1e6, "ms": ms, "bitexact_vs_hll": bool(np.array_equal(Y.get_vect(), y_ref))}
+        Cm.free()
+        return res
+
+    def c2b_powerlaw():
+        pi, pj, pv = gen.powerlaw(4_000_000, seed=0)
+        n2, nnz2 = len(pi) - 1, len(pj)
+        B2 = algorithmic_bytes(n2, nnz2)
+        x2 = np.random.default_rng(0).uniform(-1, 1, n2)
+        X2, Y2 = psb.DVect.bld(x2), psb.DVect(n2)
+        Cm = psb.CsrMat(n2, pi, pj, pv)
+        ms = _time_spmv(Cm, X2, Y2, steps, stream)
+        lens = np.diff(pi)
+        res = {"rows": n2, "nnz": nnz2, "max_row": int(lens.max()), "rows_over_2048": int((lens > 2048).sum()),
+               "csr": {"gb_s": B2 / ms / 1e6, "ms": ms}}
+        y_csr = Y2.get_vect()
+        Cm.free()
+        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
+        H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+        del d_irp, d_ja, d_va
+        ms = _time_spmv(H, X2, Y2, max(3, steps // 5), stream)
+        res["hll_unsorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2}
+        yh = Y2.get_vect()
+        short = lens <= 2048
+        res["csr_equals_hll_on_short_rows"] = bool(np.array_equal(yh[short], y_csr[short]))
+        H.free()
+        return res
+
+    def c1_bicgstab():
+        ci, cj, cv = gen.pde3d(40, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
+        n1 = len(ci) - 1
+        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (ci, cj, cv))
+        A1 = psb.HllMat.from_csr_device(n1, n1, len(cj), d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+        P1 = psb.DiagPrec("DIAG").build(A1)
+        ones, B1 = psb.DVect.bld(np.ones(n1)), psb.DVect(n1)
+        A1.spmv(1.0, ones, 0.0, B1)
+        X1 = psb.DVect(n1)
+        times = []
+        for _ in range(6):
+            X1.zero()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            its, err = psb.psb_krylov("BICGSTAB", A1, P1, B1, X1, eps=1e-9, itmax=1000)
+            times.append(time.perf_counter() - t0)
+        b_host = B1.get_vect()
+        O.set_threads(os.cpu_count() or 1)
+        rows1 = np.repeat(np.arange(n1), np.diff(ci))
+        diag1 = np.zeros(n1)
+        on_diag = cj == rows1 + 1
+        diag1[rows1[on_diag]] = cv[on_diag]
+        dinv = O.diag_prec_build(diag1)
+        t0 = time.perf_counter()
+        _, ito, erro = O.krylov("BICGSTAB", ci, cj, cv, b_host, dinv=dinv, eps=1e-9)
+        tcpu = time.perf_counter() - t0
+        A1.free()
+        return {"gpu_ms": 1e3 * statistics.median(times[1:]), "iters": its, "err": err, "cpu_ms": 1e3 * tcpu,
+                "cpu_iters": ito, "cpu_err": erro, "cpu_threads": os.cpu_count()}
+
+    def c3_cg():
+        qi, qj, qv = gen.poisson7(256)
+        n3 = len(qi) - 1
+        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (qi, qj, qv))
+        A3 = psb.HllMat.from_csr_device(n3, n3, len(qj), d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+        del d_irp, d_ja, d_va
+        P3 = psb.DiagPrec("DIAG").build(A3)
+        ustar = np.random.default_rng(0).uniform(0, 1, n3)
+        U, B3, X3 = psb.DVect.bld(ustar), psb.DVect(n3), psb.DVect(n3)
+        A3.spmv(1.0, U, 0.0, B3)
+        times = []
+        for _ in range(2):
+            X3.zero()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            it3, err3 = psb.psb_krylov("CG", A3, P3, B3, X3, eps=1e-10, itmax=20000)
+            times.append(time.perf_counter() - t0)
+        x64 = X3.get_vect()
+        res = {"rows": n3, "nnz": len(qj),
+               "fp64": {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "iters": it3, "err": err3,
+                        "max_abs_err_vs_ustar": float(np.max(np.abs(x64 - ustar)))}}
+        # mixed precision: FP32 inner CG, FP64-accumulated dots, FP64 refinement
+        A3.make_single()
+        eng = psb.BatchSolver(1, n3, 1)
+        dx = torch.zeros(n3, dtype=torch.float64, device="cuda")
+        db = torch.from_numpy(B3.get_vect()).cuda()
+        times = []
+        for _ in range(2):
+            dx.zero_()
+            s = eng.add(A3, db, dx, P3.dv.data_ptr, eps=1e-10)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.run(replays_per_step=8)
+            times.append(time.perf_counter() - t0)
+            st, outer, its, err = eng.poll(s)
+            eng.remove(s)
+        xm = dx.cpu().numpy()
+        res["mixed"] = {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "inner_iters": its[0],
+                        "outer": outer, "converged": st == 1, "err": err[0],
+                        "max_abs_err_vs_ustar": float(np.max(np.abs(xm - ustar))),
+                        "max_abs_diff_vs_fp64_solve": float(np.max(np.abs(xm - x64)))}
+        res["mixed_speedup_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+        eng.free()
+        A3.free()
+        return res
+
+    _part(out, "c2a_formats", c2a_formats)
+    _part(out, "c2b_powerlaw", c2b_powerlaw)
+    _part(out, "c1_bicgstab", c1_bicgstab)
+    if not args.skip_c3:
+        _part(out, "c3_cg", c3_cg)
+    if not args.skip_c4:
+        _part(out, "c4_batched", lambda: c4_batched(psb, gen))
+    if not args.skip_c5:
+        _part(out, "c5_serving", lambda: c5_serving(psb, gen))
+    return out
+
+
+def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
+    """C4: 512 SPD 2-D anisotropic systems -eps u_xx - u_yy on n x n grids
+    (n uniform in [32, 256], eps log-uniform in [1e-2, 1]), 8 right-hand
+    sides each (uniform [-1, 1]), solved to ||r|| <= 1e-10 ||b|| by the
+    batched mixed-precision engine; beside it the plain FP64 device CG one
+    solve at a time on a random sample of the same (system, rhs) pairs."""
+    import torch
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    mats, keep, total = [], [], 0
+    for _ in range(n_sys):
+        m = int(rng.integers(32, 257))
+        eps = float(np.exp(rng.uniform(np.log(1e-2), 0.0)))
+        irp, ja, va = gen.aniso2d(m, eps)
+        n = len(irp) - 1
+        rhs = rng.uniform(-1, 1, (n, k))
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
+        A.make_single()
+        P = psb.DiagPrec("DIAG").build(A)
+        db = torch.from_numpy(np.ascontiguousarray(rhs.reshape(-1))).cuda()
+        dx = torch.zeros_like(db)
+        mats.append((irp, ja, va, rhs, A, P, db, dx))
+        total += n
+    eng = psb.BatchSolver(n_sys, total, k)
+    slots = [eng.add(A, db, dx, P.dv.data_ptr, eps=1e-10)
+             for (_, _, _, _, A, P, db, dx) in mats]
+    torch.cuda.synchronize()
+    l0 = psb.kernel_launches()
+    t0 = time.perf_counter()
+    eng.run(replays_per_step=4)
+    tb = time.perf_counter() - t0
+    launches = psb.kernel_launches() - l0
+    states, iters, worst = [], [], 0.0
+    for s in slots:
+        st, outer, its, err = eng.poll(s)
+        states.append(st)
+        iters.extend(its)
+        worst = max(worst, max(err))
+    # FP64 check of a few solutions on the host (oracle CSR product)
+    checked = 0.0
+    for i in rng.choice(n_sys, 4, replace=False):
+        irp, ja, va, rhs, A, P, db, dx = mats[i]
+        x = dx.cpu().numpy().reshape(-1, k)
+        for j in range(k):
+            r = O.csr_csmv(irp, ja, va, -1.0, x[:, j], 1.0, rhs[:, j])
+            checked = max(checked, np.linalg.norm(r) / np.linalg.norm(rhs[:, j]))
+    eng.free()
+    # plain FP64 GPU path, one solve at a time, on a sample
+    t64, it64 = 0.0, []
+    pairs = [(int(i), int(j)) for i, j in zip(rng.integers(0, n_sys, fp64_sample), rng.integers(0, k, fp64_sample))]
+    for i, j in pairs:
+        irp, ja, va, rhs, A, P, db, dx = mats[i]
+        B, X = psb.DVect.bld(rhs[:, j]), psb.DVect(len(irp) - 1)
+        X.zero()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        it, err = psb.psb_krylov("CG", A, P, B, X, eps=1e-10, itmax=100000)
+        t64 += time.perf_counter() - t1
+        it64.append(it)
+    solves = n_sys * k
+    return {"systems": n_sys, "rhs_per_system": k, "rows_total": total, "batched_s": tb,
+            "batched_solves_per_s": solves / tb, "converged": int(sum(1 for s in states if s == 1)),
+            "max_err": worst, "host_checked_max_relres": checked, "inner_iters_max": int(max(iters)),
+            "inner_iters_median": float(np.median(iters)), "kernel_launches": int(launches),
+            "fp64_one_at_a_time_solves_per_s": len(pairs) / t64, "fp64_sample": len(pairs),
+            "fp64_iters_median": float(np.median(it64)),
+            "speedup_vs_fp64_one_at_a_time": (solves / tb) / (len(pairs) / t64)}
+
+
+def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0, fp64_sample=16):
+    """C5: Poisson arrivals (rate per second, for `window` seconds) of solve
+    requests drawn 50/50 from 3-D 7-point Poisson grids (side uniform in
+    [10, 128]) and power-law unstructured SPD matrices (rows log-uniform in
+    [1e3, 2e6], alpha 2.1, diagonally dominant), one seeded right-hand side
+    each, FP64 tolerance 1e-10, admitted by a 150 GB HBM budget into the
+    continuous-batching server; the matrices stay resident in a device pool.
+    Beside it: the plain FP64 device CG one request at a time on a sample."""
+    import torch
+    import oracle as O
+    from psblas3_b200 import serve
+    rng = np.random.default_rng(seed)
+    pool = serve.Pool()
+    host = []
+    kinds = []
+    for _ in range(pool_each):
+        side = int(rng.integers(10, 129))
+        irp, ja, va = gen.poisson7(side)
+        pool.add_csr(irp, ja, va)
+        host.append((irp, ja, va))
+        kinds.append("poisson")
+    for _ in range(pool_each):
+        rows = int(np.exp(rng.uniform(np.log(1e3), np.log(2e6))))
+        irp, ja, va = gen.powerlaw_spd(rows, kmax=min(4096, rows - 1), seed=int(rng.integers(1 << 30)))
+        irp, ja, va, _ = gen.sort_rows_by_length(irp, ja, va)
+        pool.add_csr(irp, ja, va)
+        host.append((irp, ja, va))
+        kinds.append("powerlaw")
+    # arrival stream
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window:
+            break
+        k = int(rng.integers(0, pool_each)) + (pool_each if rng.random() < 0.5 else 0)
+        reqs.append(serve.Request(len(reqs), k, int(rng.integers(1 << 31)), 1e-10, t))
+    srv = serve.Server(pool, hbm_budget=150e9)
+    l0 = psb.kernel_launches()
+    wall = serve.run_stream(srv, reqs)
+    launches = psb.kernel_launches() - l0
+    done = srv.done
+    stats = serve.latency_stats(done)
+    ok = sum(1 for r in done if r.state == 1)
+    # FP64 check of a few results on the host
+    worst = 0.0
+    for r in done[:: max(1, len(done) // 6)][:6]:
+        irp, ja, va = host[r.mat]
+        b = serve.request_rhs(r, pool.mats[r.mat]["n"]).cpu().numpy()
+        res = O.csr_csmv(irp, ja, va, -1.0, r.x, 1.0, b)
+        worst = max(worst, np.linalg.norm(res) / np.linalg.norm(b))
+    srv.close()
+    # plain FP64 GPU path, one request at a time
+    t64, sample = 0.0, done[:: max(1, len(done) // fp64_sample)][:fp64_sample]
+    for r in sample:
+        m = pool.mats[r.mat]
+        b = serve.request_rhs(r, m["n"]).cpu().numpy()
+        B, X = psb.DVect.bld(b), psb.DVect(m["n"])
+        X.zero()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        psb.psb_krylov("CG", m["A"], m["P"], B, X, eps=1e-10, itmax=100000)
+        t64 += time.perf_counter() - t1
+    out = {"arrival_rate_per_s": rate, "window_s": window, "requests": len(reqs), "completed": len(done),
+           "converged": ok, "wall_s": wall, "solves_per_s": len(done) / wall, "latency": stats,
+           "host_checked_max_relres": worst, "pool_matrices": len(pool.mats),
+           "pool_rows": [m["n"] for m in pool.mats], "kernel_launches": int(launches),
+           "fp64_one_at_a_time_solves_per_s": len(sample) / t64 if t64 else None, "fp64_sample": len(sample)}
+    for m in pool.mats:
+        m["A"].free()
+    return out
+
+
 def run_ours(args):
     world, rank, local = dist_setup()
     import torch
@@ -228,11 +567,14 @@ def run_ours(args):
     l0 = psb.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        time.sleep(0.05)  # let the sampler take its first readings
+        clk.start()
         e0.record(stream)
         for _ in range(args.steps):
             A.spmv(1.0, X, 0.0, Y)
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.stop()
     dist_barrier(world)
     torch.cuda.synchronize()
     launches = psb.kernel_launches() - l0
@@ -281,6 +623,8 @@ def run_ours(args):
             gbs, reps, threads = cpu_spmv_gbs(irp, ja, va, x_host)
             line["cpu_baseline"] = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
                                     "sample": f"{reps} full-matrix SpMVs of the same operator (CSR, oracle csmv)"}
+        if world == 1 and not args.no_secondary:
+            line["secondary"] = secondary(args, psb, gen, irp, ja, va, x_host, Y.get_vect(), stream)
         print(json.dumps(line), flush=True)
     A.free()
     if world > 1:
@@ -296,6 +640,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=GRID, help="grid side (profiling runs use a smaller case)")
+    ap.add_argument("--no-secondary", action="store_true", help="headline workload only")
+    ap.add_argument("--skip-c3", action="store_true", help="skip the 256^3 CG solves among the secondaries")
+    ap.add_argument("--skip-c4", action="store_true", help="skip the batched 512-system solve")
+    ap.add_argument("--skip-c5", action="store_true", help="skip the serving stream")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -273,6 +273,34 @@ void *psbx_multivec_data(void *deviceVec);
  * (x, y: double, y may not alias x) on the library stream, asynchronously. */
 int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x,
                       double beta, double *y);
+/* Batched mixed-precision CG engine (stands in for many psb_krylov('CG')
+ * calls of krylov/psb_dcg.F90 with the DIAG preconditioner; no single
+ * reference entry).  Each system is an FP64 HLL handle with hack size 32 and
+ * 1-based indices (an FP32 copy of its values is made if absent) and nrhs
+ * (1 or 8) right-hand sides interleaved as v[row*nrhs + k].  Per rhs: outer
+ * FP64 refinement r = b - A x, stop at ||r|| <= eps ||b||, inner Jacobi-CG
+ * in FP32 (FP64-accumulated dots) to a relative reduction inner_tol, then
+ * x += ||r|| d.  All systems advance together in one persistent grid whose
+ * iterations are captured in a CUDA graph; each system has its own
+ * convergence state and leaves the work when done; systems can be added
+ * and removed between steps.  A system's results do not depend on which
+ * other systems share the engine.
+ *   create : max_systems slots, max_rows_total rows over all slots
+ *   add    : d_b, d_x device arrays (rows*nrhs doubles, x = x0 on entry and
+ *            the solution on exit, owned by the caller), d_dinv the FP64
+ *            inverse diagonal or NULL; *slot receives the slot id
+ *   step   : replays the captured iterations `replays` times (8 iterations
+ *            each), then reports how many slots are still running
+ *   poll   : state 0 running / 1 converged / 2 stopped (itmax, breakdown);
+ *            outer steps, inner iterations and ||b-Ax||/||b|| per rhs */
+int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs);
+int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, const double *d_dinv, double eps,
+                   double inner_tol, int itmax, int *slot);
+int psbx_batch_step(void *eng, int replays, int *n_running);
+int psbx_batch_poll(void *eng, int slot, int *state, int *outer, int *iters, double *err);
+int psbx_batch_remove(void *eng, int slot);
+int psbx_batch_destroy(void *eng);
+
 /* Allocation-free dot products.  No counterpart in the reference: it is a
  * variant of dotMultiVecDeviceDouble for callers that cannot let a library
  * call cudaMalloc -- code that owns all device memory through its own pool or

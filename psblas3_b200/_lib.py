@@ -89,6 +89,12 @@ _SIGS = {
     "psbx_wrapMultiVecDevice": (I, [PP, P, U, U]), "psbx_multivec_data": (P, [P]),
     "psbx_hll_spmv_raw": (I, [P, D, P, D, P]),
     "psbx_dot_noalloc": (I, [P, I, I, P, P, I, P]),
+    "psbx_batch_create": (I, [PP, I, I, I]),
+    "psbx_batch_add": (I, [P, P, P, P, P, D, D, I, PI]),
+    "psbx_batch_step": (I, [P, I, PI]),
+    "psbx_batch_poll": (I, [P, I, PI, PI, PI, PD]),
+    "psbx_batch_remove": (I, [P, I]),
+    "psbx_batch_destroy": (I, [P]),
     "psbx_kernel_launches": (C.c_uint64, []), "psbx_last_error": (C.c_char_p, []),
 }
 

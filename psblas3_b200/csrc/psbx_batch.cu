@@ -1,0 +1,838 @@
+// psbx_batch.cu -- batched, mixed-precision CG engine: many independent SPD
+// systems (each with K right-hand sides) solved together by one persistent
+// grid, FP32 inner CG iterations with FP64-accumulated dot products inside
+// an FP64 iterative-refinement loop, per-system convergence masks, CUDA-graph
+// replays, and systems that join and leave between replays (the serving
+// loop's continuous batching).
+//
+// Method per right-hand side (CG of krylov/psb_dcg.F90:218-295 with the
+// diagonal preconditioner of prec/impl/psb_d_diagprec_impl.f90, used as the
+// inner solver of iterative refinement):
+//   r = b - A x                               (FP64 values, FP64 SpMV)
+//   stop when ||r||_2 <= eps ||b||_2          (istop 2, FP64)
+//   solve A d = r/||r|| by Jacobi-CG in FP32 until ||r_in||_2 <= tau,
+//     tau = max(inner_tol, eps ||b|| / (2 ||r||)); values FP32, vectors
+//     FP32, every dot product accumulated in FP64 (products of two FP32
+//     numbers are exact in FP64)
+//   x = x + ||r|| d                           (FP64)
+//
+// Layout: each system is an HLL-32 matrix (FP64 values, FP32 copy, shared
+// indices) with 1-based local columns, and K interleaved vectors
+// v[row*K + j].  Work is cut in tiles of up to TILE_ROWS rows of one system;
+// a block takes a contiguous range of tiles.  A tile's partial sums go to
+// part[tile]; the block that completes the last tile of a system (per-system
+// ticket) adds that system's partials in tile order -- fixed order, so the
+// result does not depend on scheduling -- and advances the system's phase.
+// Every kernel only touches systems in its own phase; a graph of ITERS x 6
+// kernels is replayed and the host looks at the phases once per replay.
+#include "psbx_internal.cuh"
+
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+namespace {
+
+enum Phase { PH_IDLE = 0, PH_RESID = 1, PH_INIT = 2, PH_INNER = 3, PH_XUPD = 4, PH_DONE = 5 };
+enum { BT = 256, TILE_ROWS = 2048, ITERS = 8, MAXK = 8, LONG_ROW = 128 };
+
+struct BSys {                 // read-only for the kernels
+  const double *val64;
+  const float *val32;
+  const int *ja, *irn, *hkoffs;
+  const double *b;
+  double *x, *r64;
+  float *r32, *z, *p, *q, *d;
+  const float *dinv;
+  int rows, sol0, tile0, ntiles;
+  int nlong;                  // leading rows handled warp-per-row (host use)
+};
+
+struct BState {               // written by the kernels
+  int phase;
+  unsigned ticket;
+  int outer;
+  int done_flag;
+};
+
+struct BSol {                 // one right-hand side
+  double rho, sigma, alpha, beta;
+  double bn2, rn, scale, tau, eps, inner_tol;
+  int it, it_total, itmax, outer_max;
+  int active;                 // inner CG running for this rhs
+  int done;                   // 0 running, 1 converged, 2 stopped (itmax / breakdown)
+  int first;                  // bn2 not yet computed
+  int pad;
+};
+
+struct BTile {
+  int sys, row0, nrows, kind;  // kind 1: one warp per row (long rows)
+};
+
+struct BCtl {                 // read by every kernel at launch; lets the tile
+  int ntiles, cap;            // table grow without re-capturing the graph
+  const BTile *tiles;
+  double *part;               // cap * 2*MAXK partial sums
+};
+
+struct Eng {
+  int K = 1, max_sys = 0, max_tiles = 0, grid = 0;
+  BSys *d_sys = nullptr;
+  BState *d_state = nullptr;
+  BSol *d_sol = nullptr;
+  BTile *d_tiles = nullptr;
+  BCtl *d_ctl = nullptr;
+  double *d_part = nullptr;   // max_tiles * K * 2
+  std::vector<BSys> h_sys;
+  std::vector<BState> h_state;
+  std::vector<int> used;      // slot in use
+  std::vector<void *> owned;  // per slot: one allocation holding its vectors
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  BState *h_state_pinned = nullptr;
+  BSol *h_sol_pinned = nullptr;
+};
+
+// --------------------------------------------------------------- helpers
+__device__ __forceinline__ void tile_range(int ntiles, int &t0, int &t1) {
+  // contiguous ranges of tiles per block (consecutive tiles of a system stay
+  // together); depends only on ntiles and the grid size
+  const long long per = ((long long)ntiles + gridDim.x - 1) / gridDim.x;
+  t0 = (int)min((long long)ntiles, per * blockIdx.x);
+  t1 = (int)min((long long)ntiles, per * (blockIdx.x + 1));
+}
+
+// Row sums of one HLL-32 row for K interleaved vectors.
+template <class VT, class XT, int K>
+__device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int *__restrict__ ja,
+                                          const int *__restrict__ hkoffs, const int *__restrict__ irn, int r,
+                                          const XT *__restrict__ x, double (&acc)[K]) {
+  const int off = __ldg(hkoffs + (r >> 5)) + (r & 31);
+  const int n = __ldg(irn + r);
+  const VT *vp = val + off;
+  const int *jp = ja + off;
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k] = 0.0;
+  constexpr int U = K == 1 ? 8 : 2;
+  int j = 0;
+  for (; j + U <= n; j += U) {
+    int c[U];
+    VT v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      c[u] = ld_stream(jp + (j + u) * 32) - 1;
+      v[u] = ld_stream(vp + (j + u) * 32);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      XT xv[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) xv[k] = __ldg(x + (size_t)c[u] * K + k);
+#pragma unroll
+      for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul((double)v[u], (double)xv[k]));
+    }
+  }
+  for (; j < n; j++) {
+    const int c = ld_stream(jp + j * 32) - 1;
+    const double v = (double)ld_stream(vp + j * 32);
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)__ldg(x + (size_t)c * K + k)));
+  }
+}
+
+// One HLL-32 row summed by a whole warp (rows longer than LONG_ROW): lane l
+// takes entries l, l+32, ...; a fixed shuffle tree combines them; the
+// result is valid in every lane.
+template <class VT, class XT, int K>
+__device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const int *__restrict__ ja,
+                                               const int *__restrict__ hkoffs, const int *__restrict__ irn, int r,
+                                               const XT *__restrict__ x, double (&acc)[K]) {
+  const int lane = threadIdx.x & 31;
+  const int off = __ldg(hkoffs + (r >> 5)) + (r & 31);
+  const int n = __ldg(irn + r);
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k] = 0.0;
+  for (int j = lane; j < n; j += 32) {
+    const int c = ld_stream(ja + off + j * 32) - 1;
+    const double v = (double)ld_stream(val + off + j * 32);
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)__ldg(x + (size_t)c * K + k)));
+  }
+#pragma unroll
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] = radd(acc[k], __shfl_xor_sync(0xffffffffu, acc[k], o));
+}
+
+// Block-reduce NS sums per rhs (K of each), publish the tile's partials,
+// take the system's ticket; returns true in the block that finalises.
+template <int K, int NS>
+__device__ __forceinline__ bool tile_publish(double (&v)[NS][K], double *part, int tile, BState *st, int ntiles,
+                                             double *smem /* >= 32*NS*K */) {
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double t = v[m][k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t = radd(t, __shfl_down_sync(0xffffffffu, t, o));
+      v[m][k] = t;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < NS; m++)
+#pragma unroll
+      for (int k = 0; k < K; k++) smem[(m * K + k) * 32 + warp] = v[m][k];
+  }
+  __syncthreads();
+  if (threadIdx.x < NS * K) {
+    double s = 0.0;
+    for (int w = 0; w < BT / 32; w++) s = radd(s, smem[threadIdx.x * 32 + w]);
+    part[(size_t)tile * (2 * MAXK) + threadIdx.x] = s;
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == (unsigned)(ntiles - 1);
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Sum of the system's tile partials, in tile order (thread j < NS*K).
+__device__ __forceinline__ double sys_total(const double *part, int tile0, int ntiles, int idx) {
+  double s = 0.0;
+  for (int t = 0; t < ntiles; t++) s = radd(s, __ldcg(part + (size_t)(tile0 + t) * (2 * MAXK) + idx));
+  return s;
+}
+
+// --------------------------------------------------------------- kernels
+// PH_RESID: r = b - A x (FP64), ||r||^2 and (first time) ||b||^2 per rhs;
+// stop test; next phase PH_INIT or PH_DONE.
+template <int K>
+__global__ void __launch_bounds__(BT) kb_resid(const BSys *__restrict__ sys, BState *state, BSol *sol,
+                                               const BCtl *ctl) {
+  __shared__ double sm[32 * 2 * MAXK];
+  int t0, t1;
+  tile_range(ctl->ntiles, t0, t1);
+  const BTile *__restrict__ tiles = ctl->tiles;
+  double *part = ctl->part;
+  (void)part;
+  for (int t = t0; t < t1; t++) {
+    const BTile T = tiles[t];
+    BState *st = state + T.sys;
+    if (st->phase != PH_RESID) continue;
+    const BSys S = sys[T.sys];
+    double v[2][K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[0][k] = v[1][k] = 0.0;
+    const bool wide = T.kind == 1;
+    const int step = wide ? BT / 32 : BT;
+    for (int i = wide ? (threadIdx.x >> 5) : threadIdx.x; i < T.nrows; i += step) {
+      const int r = T.row0 + i;
+      double ax[K];
+      if (wide)
+        row_multi_warp<double, double, K>(S.val64, S.ja, S.hkoffs, S.irn, r, S.x, ax);
+      else
+        row_multi<double, double, K>(S.val64, S.ja, S.hkoffs, S.irn, r, S.x, ax);
+      if (wide && (threadIdx.x & 31)) continue;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const double bb = S.b[(size_t)r * K + k];
+        const double rr = radd(bb, -ax[k]);
+        S.r64[(size_t)r * K + k] = rr;
+        v[0][k] = radd(v[0][k], rmul(rr, rr));
+        v[1][k] = radd(v[1][k], rmul(bb, bb));
+      }
+    }
+    if (tile_publish<K, 2>(v, part, t, st, S.ntiles, sm)) {
+      if (threadIdx.x < K) {
+        const int k = threadIdx.x;
+        BSol *so = sol + S.sol0 + k;
+        const double rr = sys_total(part, S.tile0, S.ntiles, k);
+        if (so->first) {
+          so->bn2 = sqrt(sys_total(part, S.tile0, S.ntiles, K + k));
+          so->first = 0;
+        }
+        if (so->done == 0) {
+          so->rn = sqrt(rr);
+          const double err = so->bn2 == 0.0 ? so->rn : so->rn / so->bn2;
+          if (err <= so->eps) {
+            so->done = 1;
+          } else if (so->it_total >= so->itmax || st->outer >= so->outer_max) {
+            so->done = 2;
+          } else {
+            so->scale = so->rn;
+            so->tau = fmax(so->inner_tol, 0.5 * so->eps * (so->bn2 == 0.0 ? 1.0 : so->bn2) / so->rn);
+          }
+        }
+        so->active = 0;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int all = 1;
+        for (int k = 0; k < K; k++) all &= sol[S.sol0 + k].done != 0;
+        st->phase = all ? PH_DONE : PH_INIT;
+        st->done_flag = all;
+        st->ticket = 0;
+      }
+    }
+  }
+}
+
+// PH_INIT: r32 = r/scale, z = D r32, d = 0; rho = (r32, z).
+template <int K>
+__global__ void __launch_bounds__(BT) kb_init(const BSys *__restrict__ sys, BState *state, BSol *sol,
+                                              const BCtl *ctl) {
+  __shared__ double sm[32 * 2 * MAXK];
+  int t0, t1;
+  tile_range(ctl->ntiles, t0, t1);
+  const BTile *__restrict__ tiles = ctl->tiles;
+  double *part = ctl->part;
+  (void)part;
+  for (int t = t0; t < t1; t++) {
+    const BTile T = tiles[t];
+    BState *st = state + T.sys;
+    if (st->phase != PH_INIT) continue;
+    const BSys S = sys[T.sys];
+    double inv[K];
+    bool live[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const BSol *so = sol + S.sol0 + k;
+      live[k] = so->done == 0;
+      inv[k] = live[k] ? 1.0 / so->scale : 0.0;
+    }
+    double v[1][K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[0][k] = 0.0;
+    for (int i = threadIdx.x; i < T.nrows; i += BT) {
+      const int r = T.row0 + i;
+      const float dg = S.dinv ? S.dinv[r] : 1.0f;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const size_t o = (size_t)r * K + k;
+        const float rv = live[k] ? (float)rmul(S.r64[o], inv[k]) : 0.0f;
+        const float zv = rmulf(dg, rv);
+        S.r32[o] = rv;
+        S.z[o] = zv;
+        S.d[o] = 0.0f;
+        v[0][k] = radd(v[0][k], rmul((double)rv, (double)zv));
+      }
+    }
+    if (tile_publish<K, 1>(v, part, t, st, S.ntiles, sm)) {
+      if (threadIdx.x < K) {
+        BSol *so = sol + S.sol0 + threadIdx.x;
+        if (so->done == 0) {
+          so->rho = sys_total(part, S.tile0, S.ntiles, threadIdx.x);
+          so->it = 1;
+          so->active = so->rho > 0.0 ? 1 : 0;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        st->phase = PH_INNER;
+        st->outer += 1;
+        st->ticket = 0;
+      }
+    }
+  }
+}
+
+// PH_INNER: p = z (it == 1) or p = z + beta p, for active rhs.
+template <int K>
+__global__ void __launch_bounds__(BT) kb_p(const BSys *__restrict__ sys, const BState *state, const BSol *sol,
+                                           const BCtl *ctl) {
+  int t0, t1;
+  tile_range(ctl->ntiles, t0, t1);
+  const BTile *__restrict__ tiles = ctl->tiles;
+  double *part = ctl->part;
+  (void)part;
+  for (int t = t0; t < t1; t++) {
+    const BTile T = tiles[t];
+    if (state[T.sys].phase != PH_INNER) continue;
+    const BSys S = sys[T.sys];
+    float beta[K];
+    bool act[K], first[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const BSol *so = sol + S.sol0 + k;
+      act[k] = so->active;
+      first[k] = so->it == 1;
+      beta[k] = (float)so->beta;
+    }
+    for (int i = threadIdx.x; i < T.nrows; i += BT) {
+      const size_t o = (size_t)(T.row0 + i) * K;
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        if (act[k]) S.p[o + k] = first[k] ? S.z[o + k] : raddf(S.z[o + k], rmulf(beta[k], S.p[o + k]));
+    }
+  }
+}
+
+// PH_INNER: q = A32 p ; sigma = (p, q) ; alpha = rho / sigma.
+template <int K>
+__global__ void __launch_bounds__(BT) kb_spmv(const BSys *__restrict__ sys, BState *state, BSol *sol,
+                                              const BCtl *ctl) {
+  __shared__ double sm[32 * 2 * MAXK];
+  int t0, t1;
+  tile_range(ctl->ntiles, t0, t1);
+  const BTile *__restrict__ tiles = ctl->tiles;
+  double *part = ctl->part;
+  (void)part;
+  for (int t = t0; t < t1; t++) {
+    const BTile T = tiles[t];
+    BState *st = state + T.sys;
+    if (st->phase != PH_INNER) continue;
+    const BSys S = sys[T.sys];
+    double v[1][K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[0][k] = 0.0;
+    const bool wide = T.kind == 1;
+    const int step = wide ? BT / 32 : BT;
+    for (int i = wide ? (threadIdx.x >> 5) : threadIdx.x; i < T.nrows; i += step) {
+      const int r = T.row0 + i;
+      double aq[K];
+      if (wide)
+        row_multi_warp<float, float, K>(S.val32, S.ja, S.hkoffs, S.irn, r, S.p, aq);
+      else
+        row_multi<float, float, K>(S.val32, S.ja, S.hkoffs, S.irn, r, S.p, aq);
+      if (wide && (threadIdx.x & 31)) continue;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const size_t o = (size_t)r * K + k;
+        const float qv = (float)aq[k];
+        S.q[o] = qv;
+        v[0][k] = radd(v[0][k], rmul((double)S.p[o], (double)qv));
+      }
+    }
+    if (tile_publish<K, 1>(v, part, t, st, S.ntiles, sm)) {
+      if (threadIdx.x < K) {
+        BSol *so = sol + S.sol0 + threadIdx.x;
+        if (so->active) {
+          so->sigma = sys_total(part, S.tile0, S.ntiles, threadIdx.x);
+          if (so->sigma > 0.0) {
+            so->alpha = so->rho / so->sigma;
+          } else {
+            so->active = 0;  // breakdown of the inner solve: refine with what we have
+            so->alpha = 0.0;
+          }
+        } else {
+          so->alpha = 0.0;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) st->ticket = 0;
+    }
+  }
+}
+
+// PH_INNER: d += alpha p ; r -= alpha q ; z = D r ; (r,z), (r,r) ; inner stop
+// test per rhs ; all rhs stopped -> PH_XUPD.
+template <int K>
+__global__ void __launch_bounds__(BT) kb_update(const BSys *__restrict__ sys, BState *state, BSol *sol,
+                                                const BCtl *ctl) {
+  __shared__ double sm[32 * 2 * MAXK];
+  int t0, t1;
+  tile_range(ctl->ntiles, t0, t1);
+  const BTile *__restrict__ tiles = ctl->tiles;
+  double *part = ctl->part;
+  (void)part;
+  for (int t = t0; t < t1; t++) {
+    const BTile T = tiles[t];
+    BState *st = state + T.sys;
+    if (st->phase != PH_INNER) continue;
+    const BSys S = sys[T.sys];
+    float alpha[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const BSol *so = sol + S.sol0 + k;
+      act[k] = so->active;
+      alpha[k] = (float)so->alpha;
+    }
+    double v[2][K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[0][k] = v[1][k] = 0.0;
+    for (int i = threadIdx.x; i < T.nrows; i += BT) {
+      const int r = T.row0 + i;
+      const float dg = S.dinv ? S.dinv[r] : 1.0f;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        if (!act[k]) continue;
+        const size_t o = (size_t)r * K + k;
+        S.d[o] = raddf(S.d[o], rmulf(alpha[k], S.p[o]));
+        const float rv = raddf(S.r32[o], -rmulf(alpha[k], S.q[o]));
+        const float zv = rmulf(dg, rv);
+        S.r32[o] = rv;
+        S.z[o] = zv;
+        v[0][k] = radd(v[0][k], rmul((double)rv, (double)zv));
+        v[1][k] = radd(v[1][k], rmul((double)rv, (double)rv));
+      }
+    }
+    if (tile_publish<K, 2>(v, part, t, st, S.ntiles, sm)) {
+      if (threadIdx.x < K) {
+        const int k = threadIdx.x;
+        BSol *so = sol + S.sol0 + k;
+        if (so->active) {
+          const double rz = sys_total(part, S.tile0, S.ntiles, k);
+          const double rr = sys_total(part, S.tile0, S.ntiles, K + k);
+          so->it_total += 1;
+          if (sqrt(rr) <= so->tau || so->it_total >= so->itmax || rz <= 0.0) {
+            so->active = 0;
+          } else {
+            so->beta = rz / so->rho;
+            so->rho = rz;
+            so->it += 1;
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int any = 0;
+        for (int k = 0; k < K; k++) any |= sol[S.sol0 + k].active;
+        if (!any) st->phase = PH_XUPD;
+        st->ticket = 0;
+      }
+    }
+  }
+}
+
+// PH_XUPD: x += scale * d (FP64) for rhs still running ; -> PH_RESID.
+template <int K>
+__global__ void __launch_bounds__(BT) kb_xupd(const BSys *__restrict__ sys, BState *state, const BSol *sol,
+                                              const BCtl *ctl) {
+  int t0, t1;
+  tile_range(ctl->ntiles, t0, t1);
+  const BTile *__restrict__ tiles = ctl->tiles;
+  double *part = ctl->part;
+  (void)part;
+  for (int t = t0; t < t1; t++) {
+    const BTile T = tiles[t];
+    BState *st = state + T.sys;
+    if (st->phase != PH_XUPD) continue;
+    const BSys S = sys[T.sys];
+    double sc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const BSol *so = sol + S.sol0 + k;
+      sc[k] = so->done == 0 ? so->scale : 0.0;
+    }
+    for (int i = threadIdx.x; i < T.nrows; i += BT) {
+      const size_t o = (size_t)(T.row0 + i) * K;
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        if (sc[k] != 0.0) S.x[o + k] = radd(S.x[o + k], rmul(sc[k], (double)S.d[o + k]));
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == (unsigned)(S.ntiles - 1);
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      st->phase = PH_RESID;
+      st->ticket = 0;
+    }
+  }
+}
+
+__global__ void kb_d2f_inv(int n, const double *__restrict__ dinv, float *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = dinv ? (float)dinv[i] : 1.0f;
+}
+
+// --------------------------------------------------------------- host side
+template <int K>
+static void capture_iters(Eng *e, cudaStream_t st) {
+  for (int it = 0; it < ITERS; it++) {
+    kb_xupd<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_resid<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_init<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_p<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_spmv<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_update<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+  }
+}
+
+static int upload_tables(Eng *e, cudaStream_t st) {
+  // rebuild the tile table from the slots in use
+  std::vector<BTile> tiles;
+  for (int s = 0; s < e->max_sys; s++) {
+    if (!e->used[s]) continue;
+    BSys &S = e->h_sys[s];
+    S.tile0 = (int)tiles.size();
+    const int wide_rows = BT / 32;  // one warp per long row
+    for (int r = 0; r < S.nlong; r += wide_rows) {
+      BTile T;
+      T.sys = s;
+      T.row0 = r;
+      T.nrows = S.nlong - r < wide_rows ? S.nlong - r : wide_rows;
+      T.kind = 1;
+      tiles.push_back(T);
+    }
+    for (int r = S.nlong; r < S.rows; r += TILE_ROWS) {
+      BTile T;
+      T.sys = s;
+      T.row0 = r;
+      T.nrows = S.rows - r < TILE_ROWS ? S.rows - r : TILE_ROWS;
+      T.kind = 0;
+      tiles.push_back(T);
+    }
+    S.ntiles = (int)tiles.size() - S.tile0;
+  }
+  if ((int)tiles.size() > e->max_tiles) {
+    // grow the tile table and the partial sums (kernels read them via d_ctl)
+    PSBX_CK(cudaStreamSynchronize(st));
+    const int cap = (int)tiles.size() * 2;
+    BTile *nt = nullptr;
+    double *np_ = nullptr;
+    PSBX_CK(cudaMalloc(&nt, sizeof(BTile) * cap));
+    cudaError_t err = cudaMalloc(&np_, sizeof(double) * 2 * MAXK * (size_t)cap);
+    if (err != cudaSuccess) {
+      cudaFree(nt);
+      return psbx_cuda_status(err, "psbx_batch tiles");
+    }
+    cudaFree(e->d_tiles);
+    cudaFree(e->d_part);
+    e->d_tiles = nt;
+    e->d_part = np_;
+    e->max_tiles = cap;
+  }
+  BCtl c;
+  memset(&c, 0, sizeof(c));
+  c.ntiles = (int)tiles.size();
+  c.cap = e->max_tiles;
+  c.tiles = e->d_tiles;
+  c.part = e->d_part;
+  if (!tiles.empty())
+    PSBX_CK(cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(BTile) * tiles.size(), cudaMemcpyHostToDevice, st));
+  PSBX_CK(cudaMemcpyAsync(e->d_sys, e->h_sys.data(), sizeof(BSys) * e->max_sys, cudaMemcpyHostToDevice, st));
+  PSBX_CK(cudaMemcpyAsync(e->d_ctl, &c, sizeof(BCtl), cudaMemcpyHostToDevice, st));
+  PSBX_CK(cudaStreamSynchronize(st));  // the host vectors above are reused
+  return SPGPU_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!eng || max_systems <= 0 || max_rows_total <= 0 || (nrhs != 1 && nrhs != 8)) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  Eng *e = new Eng();
+  e->K = nrhs;
+  e->max_sys = max_systems;
+  e->max_tiles = max_rows_total / TILE_ROWS + max_systems + 1;
+  e->grid = c.sms * 4;
+  e->h_sys.assign(max_systems, BSys());
+  e->h_state.assign(max_systems, BState());
+  e->used.assign(max_systems, 0);
+  e->owned.assign(max_systems, nullptr);
+  memset(e->h_sys.data(), 0, sizeof(BSys) * max_systems);
+  memset(e->h_state.data(), 0, sizeof(BState) * max_systems);
+  cudaError_t err = cudaSuccess;
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_sys, sizeof(BSys) * max_systems);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_state, sizeof(BState) * max_systems);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_sol, sizeof(BSol) * max_systems * nrhs);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_tiles, sizeof(BTile) * e->max_tiles);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_ctl, sizeof(BCtl));
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_part, sizeof(double) * 2 * MAXK * (size_t)e->max_tiles);
+  if (err == cudaSuccess) err = cudaHostAlloc(&e->h_state_pinned, sizeof(BState) * max_systems, 0);
+  if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sol_pinned, sizeof(BSol) * max_systems * nrhs, 0);
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->d_state, 0, sizeof(BState) * max_systems, c.stream);
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->d_sol, 0, sizeof(BSol) * max_systems * nrhs, c.stream);
+  if (err != cudaSuccess) {
+    rc = psbx_cuda_status(err, "psbx_batch_create");
+    psbx_batch_destroy(e);
+    *eng = nullptr;
+    return rc;
+  }
+  rc = upload_tables(e, c.stream);
+  if (!rc) {
+    err = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      if (nrhs == 1) capture_iters<1>(e, c.stream);
+      else capture_iters<8>(e, c.stream);
+      err = cudaStreamEndCapture(c.stream, &e->graph);
+    }
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&e->gexec, e->graph, 0);
+    if (err != cudaSuccess) rc = psbx_cuda_status(err, "psbx_batch_create graph");
+  }
+  if (rc) {
+    psbx_batch_destroy(e);
+    *eng = nullptr;
+    return rc;
+  }
+  *eng = e;
+  return SPGPU_SUCCESS;
+}
+
+int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, const double *d_dinv, double eps,
+                   double inner_tol, int itmax, int *slot) {
+  Eng *e = (Eng *)eng;
+  HllDevice *m = (HllDevice *)hllMat;
+  if (!e || !m || !d_b || !d_x || !slot) return SPGPU_UNSUPPORTED;
+  if (m->elemType != SPGPU_TYPE_DOUBLE || m->hackSize != 32 || m->perm || m->baseIndex != 1) return SPGPU_UNSUPPORTED;
+  if (!m->cM32) {
+    int rc = psbx_hll_make_single(m);
+    if (rc) return rc;
+  }
+  int s = -1;
+  for (int i = 0; i < e->max_sys; i++)
+    if (!e->used[i]) {
+      s = i;
+      break;
+    }
+  if (s < 0) return SPGPU_OUTOFMEMORY;  // no free slot
+  PsbxCtx &c = psbx_ctx();
+  const int K = e->K;
+  const size_t n = (size_t)m->rows;
+  // one allocation per slot: r64 (K n doubles), r32 z p q d (5 K n floats), dinv (n floats)
+  const size_t bytes = sizeof(double) * K * n + sizeof(float) * (5 * K + 1) * n + 256;
+  char *buf = nullptr;
+  cudaError_t err = cudaMallocAsync((void **)&buf, bytes, c.stream);
+  if (err != cudaSuccess) return psbx_cuda_status(err, "psbx_batch_add");
+  BSys S;
+  memset(&S, 0, sizeof(S));
+  S.val64 = (const double *)m->cM;
+  S.val32 = m->cM32;
+  S.ja = m->rP;
+  S.irn = m->rS;
+  S.hkoffs = m->hackOffs;
+  S.b = d_b;
+  S.x = d_x;
+  S.r64 = (double *)buf;
+  float *f = (float *)(buf + sizeof(double) * K * n);
+  S.r32 = f;
+  S.z = f + K * n;
+  S.p = f + 2 * K * n;
+  S.q = f + 3 * K * n;
+  S.d = f + 4 * K * n;
+  float *dv = f + 5 * K * n;
+  S.dinv = dv;
+  S.rows = (int)n;
+  S.sol0 = s * K;
+  {
+    // leading run of rows longer than LONG_ROW (matrices whose rows are sorted
+    // by length put all their long rows there)
+    const int probe = n < 65536 ? (int)n : 65536;
+    std::vector<int> irn(probe > 0 ? probe : 1);
+    if (probe > 0) PSBX_CK(cudaMemcpy(irn.data(), m->rS, sizeof(int) * probe, cudaMemcpyDeviceToHost));
+    int nl = 0;
+    while (nl < probe && irn[nl] > LONG_ROW) nl++;
+    S.nlong = nl;
+  }
+  kb_d2f_inv<<<psbx_grid_for(n, 256), 256, 0, c.stream>>>((int)n, d_dinv, dv);
+  psbx_count_launch();
+  std::vector<BSol> so(K);
+  memset(so.data(), 0, sizeof(BSol) * K);
+  for (int k = 0; k < K; k++) {
+    so[k].eps = eps;
+    so[k].inner_tol = inner_tol;
+    so[k].itmax = itmax;
+    so[k].outer_max = 64;
+    so[k].first = 1;
+  }
+  BState bs;
+  memset(&bs, 0, sizeof(bs));
+  bs.phase = PH_RESID;
+  e->h_sys[s] = S;
+  e->used[s] = 1;
+  e->owned[s] = buf;
+  PSBX_CK(cudaMemcpyAsync(e->d_sol + (size_t)s * K, so.data(), sizeof(BSol) * K, cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaMemcpyAsync(e->d_state + s, &bs, sizeof(BState), cudaMemcpyHostToDevice, c.stream));
+  int rc = upload_tables(e, c.stream);
+  if (rc) return rc;
+  *slot = s;
+  return SPGPU_SUCCESS;
+}
+
+// Runs `replays` replays of the captured batch (ITERS iterations each) and
+// returns how many slots are still running in *n_running.
+int psbx_batch_step(void *eng, int replays, int *n_running) {
+  Eng *e = (Eng *)eng;
+  if (!e) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  const int K = e->K;
+  for (int r = 0; r < replays; r++) {
+    cudaError_t err = cudaGraphLaunch(e->gexec, c.stream);
+    if (err != cudaSuccess) return psbx_cuda_status(err, "psbx_batch_step");
+    psbx_count_launch(6 * ITERS);
+  }
+  PSBX_CK(cudaMemcpyAsync(e->h_state_pinned, e->d_state, sizeof(BState) * e->max_sys, cudaMemcpyDeviceToHost,
+                          c.stream));
+  PSBX_CK(cudaMemcpyAsync(e->h_sol_pinned, e->d_sol, sizeof(BSol) * e->max_sys * K, cudaMemcpyDeviceToHost,
+                          c.stream));
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  int running = 0;
+  for (int s = 0; s < e->max_sys; s++)
+    if (e->used[s] && e->h_state_pinned[s].phase != PH_DONE) running++;
+  if (n_running) *n_running = running;
+  return SPGPU_SUCCESS;
+}
+
+// Status of a slot as of the last step: *state 0 running, 1 all rhs
+// converged, 2 finished with some rhs stopped (itmax / breakdown);
+// iters[k] inner iterations, err[k] = ||b - A x||/||b|| at the last check.
+int psbx_batch_poll(void *eng, int slot, int *state, int *outer, int *iters, double *err) {
+  Eng *e = (Eng *)eng;
+  if (!e || slot < 0 || slot >= e->max_sys || !e->used[slot]) return SPGPU_UNSUPPORTED;
+  const BState &bs = e->h_state_pinned[slot];
+  int st = 0;
+  if (bs.phase == PH_DONE) {
+    st = 1;
+    for (int k = 0; k < e->K; k++)
+      if (e->h_sol_pinned[slot * e->K + k].done != 1) st = 2;
+  }
+  if (state) *state = st;
+  if (outer) *outer = bs.outer;
+  for (int k = 0; k < e->K; k++) {
+    const BSol &so = e->h_sol_pinned[slot * e->K + k];
+    if (iters) iters[k] = so.it_total;
+    if (err) err[k] = so.bn2 == 0.0 ? so.rn : so.rn / so.bn2;
+  }
+  return SPGPU_SUCCESS;
+}
+
+int psbx_batch_remove(void *eng, int slot) {
+  Eng *e = (Eng *)eng;
+  if (!e || slot < 0 || slot >= e->max_sys || !e->used[slot]) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  BState bs;
+  memset(&bs, 0, sizeof(bs));
+  PSBX_CK(cudaMemcpyAsync(e->d_state + slot, &bs, sizeof(BState), cudaMemcpyHostToDevice, c.stream));
+  cudaFreeAsync(e->owned[slot], c.stream);
+  e->owned[slot] = nullptr;
+  e->used[slot] = 0;
+  memset(&e->h_sys[slot], 0, sizeof(BSys));
+  return upload_tables(e, c.stream);
+}
+
+int psbx_batch_destroy(void *eng) {
+  Eng *e = (Eng *)eng;
+  if (!e) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  cudaStreamSynchronize(c.stream);
+  for (int s = 0; s < e->max_sys; s++)
+    if (e->owned[s]) cudaFreeAsync(e->owned[s], c.stream);
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  cudaFree(e->d_sys);
+  cudaFree(e->d_state);
+  cudaFree(e->d_sol);
+  cudaFree(e->d_tiles);
+  cudaFree(e->d_ctl);
+  cudaFree(e->d_part);
+  cudaFreeHost(e->h_state_pinned);
+  cudaFreeHost(e->h_sol_pinned);
+  cudaStreamSynchronize(c.stream);
+  delete e;
+  return SPGPU_SUCCESS;
+}
+
+}  // extern "C"

@@ -10,7 +10,7 @@
 #include <string.h>
 #include <vector>
 
-int psbx_csr_partition(int m, const int *irp, int base, int *rowBlocks, int *nBlocks, int *longRows, int *nLong);
+void psbx_csr_partition(int m, const int *irp, std::vector<int> &rowBlocks, std::vector<int> &chunks, int *nLong);
 
 static inline size_t vsize(int t) { return t == SPGPU_TYPE_FLOAT ? 4 : 8; }
 
@@ -652,8 +652,11 @@ static void csr_free_arrays(CsrDevice *m) {
   cudaFree(m->irp);
   cudaFree(m->ja);
   if (m->rowBlocks) cudaFree(m->rowBlocks);
-  if (m->longRows) cudaFree(m->longRows);
-  m->val = nullptr; m->irp = nullptr; m->ja = nullptr; m->rowBlocks = nullptr; m->longRows = nullptr;
+  if (m->chunks) cudaFree(m->chunks);
+  if (m->chunkPart) cudaFree(m->chunkPart);
+  if (m->chunkTicket) cudaFree(m->chunkTicket);
+  m->val = nullptr; m->irp = nullptr; m->ja = nullptr; m->rowBlocks = nullptr;
+  m->chunks = nullptr; m->chunkPart = nullptr; m->chunkTicket = nullptr;
 }
 
 extern "C" {
@@ -719,20 +722,28 @@ int d_CSRGHost2Device(psbx_d_Cmat *Mat, int m_, int n, int nz, int *irp, int *ja
   if (!rc) rc = h2d(m->ja, ja, sizeof(int) * (size_t)nz);
   if (!rc) rc = h2d(m->val, val, sizeof(double) * (size_t)nz);
   if (rc) return rc;
-  // row blocks for the streaming kernel
-  std::vector<int> blocks(2 * (size_t)(m_ > 0 ? m_ : 1)), longr(m_ > 0 ? m_ : 1);
-  std::vector<int> irp0(irp, irp + m_ + 1);
-  int nb = 0, nl = 0;
-  psbx_csr_partition(m_, irp0.data(), m->baseIndex, blocks.data(), &nb, longr.data(), &nl);
+  // work partition of the adaptive kernel
+  std::vector<int> blocks, chunks;
+  int nl = 0;
+  psbx_csr_partition(m_, irp, blocks, chunks, &nl);
   if (m->rowBlocks) cudaFree(m->rowBlocks);
-  if (m->longRows) cudaFree(m->longRows);
+  if (m->chunks) cudaFree(m->chunks);
+  if (m->chunkPart) cudaFree(m->chunkPart);
+  if (m->chunkTicket) cudaFree(m->chunkTicket);
   m->rowBlocks = nullptr;
-  m->longRows = nullptr;
-  rc = dmalloc((void **)&m->rowBlocks, sizeof(int) * (size_t)(2 * nb + 2));
-  if (!rc) rc = dmalloc((void **)&m->longRows, sizeof(int) * (size_t)(nl + 1));
-  if (!rc) rc = h2d(m->rowBlocks, blocks.data(), sizeof(int) * (size_t)(2 * nb));
-  if (!rc) rc = h2d(m->longRows, longr.data(), sizeof(int) * (size_t)nl);
+  m->chunks = nullptr;
+  m->chunkPart = nullptr;
+  m->chunkTicket = nullptr;
+  const int nb = (int)blocks.size() / 2, nc = (int)chunks.size() / 6;
+  rc = dmalloc((void **)&m->rowBlocks, sizeof(int) * (blocks.size() + 2));
+  if (!rc) rc = dmalloc((void **)&m->chunks, sizeof(int) * (chunks.size() + 6));
+  if (!rc) rc = dmalloc((void **)&m->chunkPart, sizeof(double) * (size_t)(nc + 1));
+  if (!rc) rc = dmalloc((void **)&m->chunkTicket, sizeof(unsigned) * (size_t)(nl + 1));
+  if (!rc) rc = h2d(m->rowBlocks, blocks.data(), sizeof(int) * blocks.size());
+  if (!rc) rc = h2d(m->chunks, chunks.data(), sizeof(int) * chunks.size());
+  if (!rc) PSBX_CK(cudaMemsetAsync(m->chunkTicket, 0, sizeof(unsigned) * (size_t)(nl + 1), psbx_ctx().stream));
   m->nBlocks = nb;
+  m->nChunks = nc;
   m->nLong = nl;
   int mx = 0;
   for (int i = 0; i < m_; i++) mx = irp[i + 1] - irp[i] > mx ? irp[i + 1] - irp[i] : mx;

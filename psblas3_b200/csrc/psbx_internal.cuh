@@ -68,10 +68,13 @@ struct CsrDevice {
   int *ja;
   int baseIndex;     // 0 or 1 (d_CSRGDeviceSetMatIndexBase)
   int maxRowLen;     // computed at upload
-  // row blocks for the streaming kernel (built at upload)
-  int *rowBlocks;    // nBlocks+1 row starts
+  // work partition of the adaptive kernel (built at upload)
+  int *rowBlocks;    // 2*nBlocks: start and end row of each row block
   int nBlocks;
-  int *longRows;     // rows handled by the warp-per-row kernel
+  int *chunks;       // 6*nChunks: chunk records of rows longer than a tile
+  int nChunks;
+  double *chunkPart; // one partial sum per chunk
+  unsigned *chunkTicket;  // one counter per long row (kept at zero between calls)
   int nLong;
 };
 

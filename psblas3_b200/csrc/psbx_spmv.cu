@@ -18,10 +18,13 @@
 // (the row blocks are built at upload).  Its threads load the run's values
 // and indices coalesced, form the products val*x(ja) and park them in shared
 // memory; then one thread per row adds its products in stored order -- the
-// same bits as the reference's row loop.  Rows longer than CSR_TILE go to a
-// warp-per-row kernel whose shuffle-tree sum differs from the sequential sum
-// only by rounding (checked against a tolerance).
+// same bits as the reference's row loop.  Rows longer than CSR_TILE are cut
+// into CSR_TILE-entry chunks handled by extra blocks of the same launch;
+// their chunk sums combine in a fixed order, which differs from the
+// sequential sum only by rounding (checked against a tolerance).
 #include "psbx_internal.cuh"
+
+#include <vector>
 
 #define SPMV_T 256
 #define CSR_TILE 2048
@@ -148,9 +151,8 @@ int psbx_launch_hll_spmv_f32(const HllDevice *m, float alpha, const float *x, fl
 // Block b holds rows rowBlocks[2b] .. rowBlocks[2b+1]-1; their entries (at
 // most CSR_TILE) are contiguous in val/ja.
 template <int MODE>
-__global__ void __launch_bounds__(SPMV_T) k_csr_stream(CsrView A, const int *__restrict__ rowBlocks, double alpha,
-                                                       const double *__restrict__ x, double beta,
-                                                       double *__restrict__ y) {
+__device__ __forceinline__ void csr_stream_block(const CsrView &A, const int *__restrict__ rowBlocks, double alpha,
+                                                 const double *__restrict__ x, double beta, double *__restrict__ y) {
   __shared__ double prod[CSR_TILE];
   const int r0 = rowBlocks[2 * blockIdx.x], r1 = rowBlocks[2 * blockIdx.x + 1];
   const int e0 = ld_ro(A.irp + r0) - A.base, e1 = ld_ro(A.irp + r1) - A.base;
@@ -172,25 +174,49 @@ __global__ void __launch_bounds__(SPMV_T) k_csr_stream(CsrView A, const int *__r
   }
 }
 
-// One warp per long row: per-lane partial sums, shuffle tree.
+// Chunks of rows longer than CSR_TILE entries run in the same launch as the
+// row blocks (blocks nBlocks.. of the grid), so a skewed matrix does not wait
+// for a second launch.  Chunk record (6 ints): row, first entry, end entry,
+// index of the row's first chunk, chunks in the row, long-row ordinal.  A
+// chunk block sums its entries (each thread in index order over a stride of
+// the block, then a fixed shuffle tree), stores one partial, and the last
+// chunk of the row to finish adds the row's partials in chunk order.
 template <int MODE>
-__global__ void __launch_bounds__(SPMV_T) k_csr_long(CsrView A, const int *__restrict__ rows, int nrows, double alpha,
-                                                     const double *__restrict__ x, double beta,
-                                                     double *__restrict__ y) {
-  const int w = (blockIdx.x * SPMV_T + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nrows) return;
-  const int r = rows[w];
-  const int b = ld_ro(A.irp + r) - A.base, e = ld_ro(A.irp + r + 1) - A.base;
+__device__ __forceinline__ void csr_chunk(const CsrView &A, const int *__restrict__ rec, double *__restrict__ part,
+                                          unsigned *__restrict__ ticket, double alpha, const double *__restrict__ x,
+                                          double beta, double *__restrict__ y) {
+  __shared__ double sm[32];
+  const int row = rec[0], e0 = rec[1], e1 = rec[2], first = rec[3], nch = rec[4], ord = rec[5];
   const double *xb = x - A.base;
-  double acc = 0.0;
-  for (int k = b + lane; k < e; k += 32) acc = radd(acc, rmul(ld_stream(A.val + k), ld_ro(xb + ld_stream(A.ja + k))));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc = radd(acc, __shfl_down_sync(0xffffffffu, acc, o));
-  if (lane == 0) {
-    const double t = rmul(alpha, acc);
-    y[r] = MODE == 1 ? t : radd(t, rmul(beta, y[r]));
+  double acc[1] = {0.0};
+  for (int k = e0 + threadIdx.x; k < e1; k += SPMV_T)
+    acc[0] = radd(acc[0], rmul(ld_stream(A.val + k), ld_ro(xb + ld_stream(A.ja + k))));
+  block_sum<1>(acc, sm);
+  const int me = first + (e0 - (ld_ro(A.irp + row) - A.base)) / CSR_TILE;
+  if (threadIdx.x == 0) part[me] = acc[0];
+  if (psbx_last_block(ticket + ord, (unsigned)nch)) {
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int c = 0; c < nch; c++) s = radd(s, __ldcg(part + first + c));
+      const double t = rmul(alpha, s);
+      y[row] = MODE == 1 ? t : radd(t, rmul(beta, y[row]));
+      ticket[ord] = 0;
+    }
   }
+}
+
+
+// One launch: blocks [0, nBlocks) are row blocks, the rest long-row chunks.
+template <int MODE>
+__global__ void __launch_bounds__(SPMV_T) k_csr_adaptive(CsrView A, const int *__restrict__ rowBlocks, int nBlocks,
+                                                         const int *__restrict__ chunks, double *__restrict__ part,
+                                                         unsigned *__restrict__ ticket, double alpha,
+                                                         const double *__restrict__ x, double beta,
+                                                         double *__restrict__ y) {
+  if ((int)blockIdx.x < nBlocks)
+    csr_stream_block<MODE>(A, rowBlocks, alpha, x, beta, y);
+  else
+    csr_chunk<MODE>(A, chunks + 6 * (blockIdx.x - nBlocks), part, ticket, alpha, x, beta, y);
 }
 
 int psbx_launch_csr_spmv(const CsrDevice *m, double alpha, const double *x, double beta, double *y,
@@ -198,39 +224,43 @@ int psbx_launch_csr_spmv(const CsrDevice *m, double alpha, const double *x, doub
   if (m->m <= 0) return SPGPU_SUCCESS;
   if (alpha == 0.0) return psbx_launch_scale(m->m, beta, y, st);
   CsrView A = csr_view(m);
-  if (m->nBlocks > 0) {
-    if (beta == 0.0)
-      k_csr_stream<1><<<m->nBlocks, SPMV_T, 0, st>>>(A, m->rowBlocks, alpha, x, beta, y);
-    else
-      k_csr_stream<0><<<m->nBlocks, SPMV_T, 0, st>>>(A, m->rowBlocks, alpha, x, beta, y);
-    PSBX_LAUNCH_CK("k_csr_stream");
-  }
-  if (m->nLong > 0) {
-    const int g = (m->nLong * 32 + SPMV_T - 1) / SPMV_T;
-    if (beta == 0.0)
-      k_csr_long<1><<<g, SPMV_T, 0, st>>>(A, m->longRows, m->nLong, alpha, x, beta, y);
-    else
-      k_csr_long<0><<<g, SPMV_T, 0, st>>>(A, m->longRows, m->nLong, alpha, x, beta, y);
-    PSBX_LAUNCH_CK("k_csr_long");
-  }
+  const int g = m->nBlocks + m->nChunks;
+  if (g <= 0) return SPGPU_SUCCESS;
+  if (beta == 0.0)
+    k_csr_adaptive<1><<<g, SPMV_T, 0, st>>>(A, m->rowBlocks, m->nBlocks, m->chunks, m->chunkPart, m->chunkTicket,
+                                            alpha, x, beta, y);
+  else
+    k_csr_adaptive<0><<<g, SPMV_T, 0, st>>>(A, m->rowBlocks, m->nBlocks, m->chunks, m->chunkPart, m->chunkTicket,
+                                            alpha, x, beta, y);
+  PSBX_LAUNCH_CK("k_csr_adaptive");
   return SPGPU_SUCCESS;
 }
 
-// Row-block partition for the CSR stream kernel (host side, from irp).
-// Greedy: extend a block while it holds <= CSR_TILE entries and <= CSR_ROWS
-// rows; a row with more than CSR_TILE entries is a long row.
-int psbx_csr_partition(int m, const int *irp, int base, int *rowBlocks /*2*m max*/, int *nBlocks, int *longRows,
-                       int *nLong) {
-  int nb = 0, nl = 0;
+// Work partition for k_csr_adaptive (host side, from irp).  Greedy row
+// blocks of <= CSR_TILE entries and <= CSR_ROWS rows; a row with more than
+// CSR_TILE entries becomes ceil(len/CSR_TILE) chunk records.
+void psbx_csr_partition(int m, const int *irp, std::vector<int> &rowBlocks, std::vector<int> &chunks, int *nLong) {
+  rowBlocks.clear();
+  chunks.clear();
+  int nl = 0, nch = 0;
   int r = 0;
   while (r < m) {
     const int len = irp[r + 1] - irp[r];
     if (len > CSR_TILE) {
-      longRows[nl++] = r;
+      const int k = (len + CSR_TILE - 1) / CSR_TILE;
+      const int b = irp[r] - irp[0];
+      for (int c = 0; c < k; c++) {
+        const int e0 = b + c * CSR_TILE;
+        const int e1 = e0 + CSR_TILE < b + len ? e0 + CSR_TILE : b + len;
+        chunks.insert(chunks.end(), {r, e0, e1, nch, k, nl});
+      }
+      nch += k;
+      nl++;
       r++;
       continue;
     }
-    int start = r, cnt = 0;
+    const int start = r;
+    int cnt = 0;
     long long ent = 0;
     while (r < m && cnt < CSR_ROWS) {
       const int l = irp[r + 1] - irp[r];
@@ -239,14 +269,10 @@ int psbx_csr_partition(int m, const int *irp, int base, int *rowBlocks /*2*m max
       cnt++;
       r++;
     }
-    rowBlocks[2 * nb] = start;
-    rowBlocks[2 * nb + 1] = r;
-    nb++;
+    rowBlocks.push_back(start);
+    rowBlocks.push_back(r);
   }
-  (void)base;
-  *nBlocks = nb;
   *nLong = nl;
-  return 0;
 }
 
 #undef SPMV_T

@@ -159,6 +159,58 @@ def powerlaw(nrows, alpha=2.1, kmin=1, kmax=4096, seed=0):
     return (irp + 1).astype(np.int32), (cols + 1).astype(np.int32), vals.astype(np.float64)
 
 
+def powerlaw_spd(nrows, alpha=2.1, kmin=1, kmax=4096, seed=0):
+    """Symmetric positive definite unstructured matrix with power-law row
+    lengths: the off-diagonal pattern of `powerlaw` (k_i uniform columns per
+    row, values N(0,1)) is symmetrised, B + B^T, and the diagonal is set to
+    (row abs sum + 1), which makes it SPD by diagonal dominance."""
+    irp, ja, va = powerlaw(nrows, alpha, kmin, kmax, seed)
+    n = len(irp) - 1
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(irp.astype(np.int64)))
+    cols = ja.astype(np.int64) - 1
+    off = rows != cols
+    r, c, v = rows[off], cols[off], va[off]
+    rr = np.concatenate([r, c])
+    cc = np.concatenate([c, r])
+    vv = np.concatenate([v, v])
+    key = rr * n + cc
+    order = np.argsort(key, kind="stable")
+    key, vv = key[order], vv[order]
+    uniq, start = np.unique(key, return_index=True)
+    vals = np.add.reduceat(vv, start)
+    rr, cc = uniq // n, uniq % n
+    absum = np.bincount(rr, weights=np.abs(vals), minlength=n)
+    rr = np.concatenate([rr, np.arange(n, dtype=np.int64)])
+    cc = np.concatenate([cc, np.arange(n, dtype=np.int64)])
+    vals = np.concatenate([vals, absum + 1.0])
+    o = np.lexsort((cc, rr))
+    rr, cc, vals = rr[o], cc[o], vals[o]
+    irp2 = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(rr, minlength=n), out=irp2[1:])
+    return (irp2 + 1).astype(np.int32), (cc + 1).astype(np.int32), vals
+
+
+def sort_rows_by_length(irp, ja, val):
+    """Symmetric permutation P A P^T with rows (and columns) ordered by
+    decreasing row length (stable).  Keeps an SPD matrix SPD; solves of the
+    permuted system give the permuted solution.  Returns (irp, ja, val,
+    order) with new row i = old row order[i]."""
+    n = len(irp) - 1
+    lens = np.diff(irp.astype(np.int64))
+    order = np.argsort(-lens, kind="stable")
+    inv = np.empty(n, np.int64)
+    inv[order] = np.arange(n)
+    rows_old = np.repeat(np.arange(n), lens)
+    new_rows = inv[rows_old]
+    new_cols = inv[ja.astype(np.int64) - 1]
+    o = np.lexsort((new_cols, new_rows))
+    counts = np.bincount(new_rows, minlength=n)
+    nirp = np.zeros(n + 1, np.int64)
+    np.cumsum(counts, out=nirp[1:])
+    return ((nirp + 1).astype(np.int32), (new_cols[o] + 1).astype(np.int32),
+            np.asarray(val, np.float64)[o], order)
+
+
 def csr_to_coo(irp, ja, val):
     n = len(irp) - 1
     counts = np.diff(irp.astype(np.int64))

@@ -80,6 +80,11 @@ class DVect:
         out = buf[:, : self.n]
         return out[0].copy() if self.count == 1 else out.T.copy()
 
+    @property
+    def data_ptr(self):
+        """Device address of the vector data (int)."""
+        return lib.psbx_multivec_data(self.h)
+
     def set_scal(self, val, first=1, last=None):
         last = self.n if last is None else last
         check(lib.setscalMultiVecDeviceDouble(float(val), int(first), int(last), 1, self.h), "setscal")
@@ -382,6 +387,63 @@ def psb_krylov(method, a, prec, b, x, eps=1e-6, itmax=1000, istop=2, itrace=0, i
     mh = a.h if a.fmt != L.PSBX_FMT_CSR else C.c_void_p(a.h)
     check(lib.psbx_dkrylov(method.upper().encode(), mh, a.fmt, dinv, b.h, x.h, C.byref(opt)), "psbx_dkrylov")
     return opt.iter, opt.err
+
+
+class BatchSolver:
+    """Batched mixed-precision CG engine (psbx_batch_*): FP32 inner Jacobi-CG
+    with FP64-accumulated dots inside FP64 iterative refinement, many
+    systems advancing together; systems join and leave between steps."""
+
+    def __init__(self, max_systems, max_rows_total, nrhs=1):
+        self.nrhs = int(nrhs)
+        h = C.c_void_p()
+        check(lib.psbx_batch_create(C.byref(h), int(max_systems), int(max_rows_total), self.nrhs), "batch_create")
+        self.h = h
+        self.keep = {}
+
+    def add(self, A, d_b, d_x, d_dinv=None, eps=1e-10, inner_tol=1e-4, itmax=100000, keep=None):
+        """A: HllMat (hack 32); d_b, d_x, d_dinv: device pointers (ints) or
+        torch tensors (rows*nrhs doubles, interleaved).  Returns the slot."""
+        def ptr(t):
+            return None if t is None else C.c_void_p(t if isinstance(t, int) else t.data_ptr())
+        slot = C.c_int(-1)
+        check(lib.psbx_batch_add(self.h, A.h, ptr(d_b), ptr(d_x), ptr(d_dinv), float(eps), float(inner_tol),
+                                 int(itmax), C.byref(slot)), "batch_add")
+        self.keep[slot.value] = keep
+        return slot.value
+
+    def step(self, replays=1):
+        n = C.c_int(0)
+        check(lib.psbx_batch_step(self.h, int(replays), C.byref(n)), "batch_step")
+        return n.value
+
+    def poll(self, slot):
+        st, outer = C.c_int(0), C.c_int(0)
+        its = (C.c_int * self.nrhs)()
+        err = (C.c_double * self.nrhs)()
+        check(lib.psbx_batch_poll(self.h, int(slot), C.byref(st), C.byref(outer), its, err), "batch_poll")
+        return st.value, outer.value, list(its), list(err)
+
+    def remove(self, slot):
+        check(lib.psbx_batch_remove(self.h, int(slot)), "batch_remove")
+        self.keep.pop(slot, None)
+
+    def run(self, replays_per_step=4, max_steps=100000):
+        for _ in range(max_steps):
+            if self.step(replays_per_step) == 0:
+                return
+        raise RuntimeError("batch did not finish")
+
+    def free(self):
+        if self.h:
+            lib.psbx_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def kernel_launches() -> int:
