@@ -94,6 +94,18 @@ struct Eng {
 };
 
 // --------------------------------------------------------------- helpers
+// Occupancy targets (blocks of BT threads per SM).  The K = 1 kernels are
+// latency-bound streams over short rows: the SpMV and the short vector
+// kernels want every warp slot (8 blocks, <= 32 registers); the update keeps
+// 4 rows of loads in flight per thread instead (4 blocks, no spills), which
+// measured faster than 1 row per thread at 8 blocks.  The 8-rhs kernels carry
+// 8 accumulators per row.
+template <int K> struct Occ {
+  static constexpr int blocks = K == 1 ? 8 : 2;
+  static constexpr int update_blocks = K == 1 ? 4 : 2;
+  static constexpr int resid_blocks = K == 1 ? 4 : 2;
+};
+
 __device__ __forceinline__ void tile_range(int ntiles, int &t0, int &t1) {
   // contiguous ranges of tiles per block (consecutive tiles of a system stay
   // together); depends only on ntiles and the grid size
@@ -102,15 +114,24 @@ __device__ __forceinline__ void tile_range(int ntiles, int &t0, int &t1) {
   t1 = (int)min((long long)ntiles, per * (blockIdx.x + 1));
 }
 
-// Row sums of one HLL-32 row for K interleaved vectors.
+struct RowRef {               // start of an HLL-32 row and its length
+  int off, n;
+};
+
+__device__ __forceinline__ RowRef row_ref(const int *__restrict__ hkoffs, const int *__restrict__ irn, int r) {
+  RowRef rr;
+  rr.off = __ldg(hkoffs + (r >> 5)) + (r & 31);
+  rr.n = __ldg(irn + r);
+  return rr;
+}
+
+// Row sums of one HLL-32 row for K interleaved vectors, entries in order.
 template <class VT, class XT, int K>
-__device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int *__restrict__ ja,
-                                          const int *__restrict__ hkoffs, const int *__restrict__ irn, int r,
+__device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int *__restrict__ ja, RowRef rr,
                                           const XT *__restrict__ x, double (&acc)[K]) {
-  const int off = __ldg(hkoffs + (r >> 5)) + (r & 31);
-  const int n = __ldg(irn + r);
-  const VT *vp = val + off;
-  const int *jp = ja + off;
+  const VT *vp = val + rr.off;
+  const int *jp = ja + rr.off;
+  const int n = rr.n;
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k] = 0.0;
   constexpr int U = K == 1 ? 8 : 2;
@@ -132,11 +153,25 @@ __device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int 
       for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul((double)v[u], (double)xv[k]));
     }
   }
-  for (; j < n; j++) {
-    const int c = ld_stream(jp + j * 32) - 1;
-    const double v = (double)ld_stream(vp + j * 32);
+  if (j < n) {  // the tail as one predicated group: its loads overlap
+    int c[U];
+    VT v[U];
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)__ldg(x + (size_t)c * K + k)));
+    for (int u = 0; u < U; u++) {
+      const bool ok = j + u < n;
+      c[u] = ok ? ld_stream(jp + (j + u) * 32) - 1 : 0;
+      v[u] = ok ? ld_stream(vp + (j + u) * 32) : VT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (j + u < n) {
+        XT xv[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) xv[k] = __ldg(x + (size_t)c[u] * K + k);
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul((double)v[u], (double)xv[k]));
+      }
+    }
   }
 }
 
@@ -144,17 +179,14 @@ __device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int 
 // takes entries l, l+32, ...; a fixed shuffle tree combines them; the
 // result is valid in every lane.
 template <class VT, class XT, int K>
-__device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const int *__restrict__ ja,
-                                               const int *__restrict__ hkoffs, const int *__restrict__ irn, int r,
+__device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const int *__restrict__ ja, RowRef rr,
                                                const XT *__restrict__ x, double (&acc)[K]) {
   const int lane = threadIdx.x & 31;
-  const int off = __ldg(hkoffs + (r >> 5)) + (r & 31);
-  const int n = __ldg(irn + r);
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k] = 0.0;
-  for (int j = lane; j < n; j += 32) {
-    const int c = ld_stream(ja + off + j * 32) - 1;
-    const double v = (double)ld_stream(val + off + j * 32);
+  for (int j = lane; j < rr.n; j += 32) {
+    const int c = ld_stream(ja + rr.off + j * 32) - 1;
+    const double v = (double)ld_stream(val + rr.off + j * 32);
 #pragma unroll
     for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)__ldg(x + (size_t)c * K + k)));
   }
@@ -162,6 +194,35 @@ __device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const
   for (int k = 0; k < K; k++)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc[k] = radd(acc[k], __shfl_xor_sync(0xffffffffu, acc[k], o));
+}
+
+// Applies f(row, sums) to every row of a tile: thread-per-row tiles (kind 0)
+// walk rows threadIdx.x, +BT, ... with the next row's offset and length
+// loaded while the current row is summed; warp-per-row tiles (kind 1) call
+// f in lane 0 only.
+template <class VT, class XT, int K, class F>
+__device__ __forceinline__ void tile_spmv(const BSys &S, const BTile &T, const VT *__restrict__ val,
+                                          const XT *__restrict__ x, F &&f) {
+  if (T.kind == 1) {
+    for (int i = threadIdx.x >> 5; i < T.nrows; i += BT / 32) {
+      const int r = T.row0 + i;
+      double a[K];
+      row_multi_warp<VT, XT, K>(val, S.ja, row_ref(S.hkoffs, S.irn, r), x, a);
+      if ((threadIdx.x & 31) == 0) f(r, a);
+    }
+    return;
+  }
+  int i = threadIdx.x;
+  RowRef cur = {0, 0};
+  if (i < T.nrows) cur = row_ref(S.hkoffs, S.irn, T.row0 + i);
+  for (; i < T.nrows; i += BT) {
+    RowRef nxt = {0, 0};
+    if (i + BT < T.nrows) nxt = row_ref(S.hkoffs, S.irn, T.row0 + i + BT);
+    double a[K];
+    row_multi<VT, XT, K>(val, S.ja, cur, x, a);
+    f(T.row0 + i, a);
+    cur = nxt;
+  }
 }
 
 // Block-reduce NS sums per rhs (K of each), publish the tile's partials,
@@ -202,59 +263,82 @@ __device__ __forceinline__ bool tile_publish(double (&v)[NS][K], double *part, i
   return last;
 }
 
-// Sum of the system's tile partials, in tile order (thread j < NS*K).
-__device__ __forceinline__ double sys_total(const double *part, int tile0, int ntiles, int idx) {
-  double s = 0.0;
-  for (int t = 0; t < ntiles; t++) s = radd(s, __ldcg(part + (size_t)(tile0 + t) * (2 * MAXK) + idx));
-  return s;
+// Totals of the system's tile partials for NV values (all threads of the
+// finalising block): thread t adds tiles t, t+BT, ... in order, then a fixed
+// shuffle tree and the warps in order.  The order depends only on the
+// system's tile count, so a system's result does not depend on its company.
+// Results in tot[0..NV).
+template <int NV>
+__device__ __forceinline__ void sys_totals(const double *part, int tile0, int ntiles, double *tot,
+                                           double *scratch /* 32*NV */) {
+  double v[NV];
+#pragma unroll
+  for (int m = 0; m < NV; m++) v[m] = 0.0;
+  for (int t = threadIdx.x; t < ntiles; t += BT) {
+    const double *pt = part + (size_t)(tile0 + t) * (2 * MAXK);
+#pragma unroll
+    for (int m = 0; m < NV; m++) v[m] = radd(v[m], __ldcg(pt + m));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < NV; m++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[m] = radd(v[m], __shfl_down_sync(0xffffffffu, v[m], o));
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < NV; m++) scratch[m * 32 + warp] = v[m];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int w = 0; w < BT / 32; w++) s = radd(s, scratch[threadIdx.x * 32 + w]);
+    tot[threadIdx.x] = s;
+  }
+  __syncthreads();
 }
 
 // --------------------------------------------------------------- kernels
 // PH_RESID: r = b - A x (FP64), ||r||^2 and (first time) ||b||^2 per rhs;
 // stop test; next phase PH_INIT or PH_DONE.
 template <int K>
-__global__ void __launch_bounds__(BT) kb_resid(const BSys *__restrict__ sys, BState *state, BSol *sol,
-                                               const BCtl *ctl) {
+__global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys *__restrict__ sys, BState *state,
+                                                                     BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  (void)part;
   for (int t = t0; t < t1; t++) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_RESID) continue;
-    const BSys S = sys[T.sys];
+    const BSys &S = sys[T.sys];
     double v[2][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = v[1][k] = 0.0;
-    const bool wide = T.kind == 1;
-    const int step = wide ? BT / 32 : BT;
-    for (int i = wide ? (threadIdx.x >> 5) : threadIdx.x; i < T.nrows; i += step) {
-      const int r = T.row0 + i;
-      double ax[K];
-      if (wide)
-        row_multi_warp<double, double, K>(S.val64, S.ja, S.hkoffs, S.irn, r, S.x, ax);
-      else
-        row_multi<double, double, K>(S.val64, S.ja, S.hkoffs, S.irn, r, S.x, ax);
-      if (wide && (threadIdx.x & 31)) continue;
+    const double *__restrict__ b = S.b;
+    double *__restrict__ r64 = S.r64;
+    tile_spmv<double, double, K>(S, T, S.val64, S.x, [&](int r, const double (&ax)[K]) {
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        const double bb = S.b[(size_t)r * K + k];
+        const double bb = b[(size_t)r * K + k];
         const double rr = radd(bb, -ax[k]);
-        S.r64[(size_t)r * K + k] = rr;
+        r64[(size_t)r * K + k] = rr;
         v[0][k] = radd(v[0][k], rmul(rr, rr));
         v[1][k] = radd(v[1][k], rmul(bb, bb));
       }
-    }
+    });
     if (tile_publish<K, 2>(v, part, t, st, S.ntiles, sm)) {
+      __shared__ double tot[2 * K];
+      sys_totals<2 * K>(part, S.tile0, S.ntiles, tot, sm);
       if (threadIdx.x < K) {
         const int k = threadIdx.x;
         BSol *so = sol + S.sol0 + k;
-        const double rr = sys_total(part, S.tile0, S.ntiles, k);
+        const double rr = tot[k];
         if (so->first) {
-          so->bn2 = sqrt(sys_total(part, S.tile0, S.ntiles, K + k));
+          so->bn2 = sqrt(tot[K + k]);
           so->first = 0;
         }
         if (so->done == 0) {
@@ -285,19 +369,19 @@ __global__ void __launch_bounds__(BT) kb_resid(const BSys *__restrict__ sys, BSt
 
 // PH_INIT: r32 = r/scale, z = D r32, d = 0; rho = (r32, z).
 template <int K>
-__global__ void __launch_bounds__(BT) kb_init(const BSys *__restrict__ sys, BState *state, BSol *sol,
-                                              const BCtl *ctl) {
+__global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__restrict__ sys, BState *state,
+                                                              BSol *sol, const BCtl *ctl) {
+  constexpr int RB = K == 1 ? 2 : 1;  // rows per thread whose loads are in flight together
   __shared__ double sm[32 * 2 * MAXK];
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  (void)part;
   for (int t = t0; t < t1; t++) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_INIT) continue;
-    const BSys S = sys[T.sys];
+    const BSys &S = sys[T.sys];
     double inv[K];
     bool live[K];
 #pragma unroll
@@ -306,28 +390,49 @@ __global__ void __launch_bounds__(BT) kb_init(const BSys *__restrict__ sys, BSta
       live[k] = so->done == 0;
       inv[k] = live[k] ? 1.0 / so->scale : 0.0;
     }
+    const double *__restrict__ r64 = S.r64;
+    const float *__restrict__ dinv = S.dinv;
+    float *__restrict__ r32 = S.r32;
+    float *__restrict__ z = S.z;
+    float *__restrict__ d = S.d;
     double v[1][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = 0.0;
-    for (int i = threadIdx.x; i < T.nrows; i += BT) {
-      const int r = T.row0 + i;
-      const float dg = S.dinv ? S.dinv[r] : 1.0f;
+    for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
+      double rv64[RB][K];
+      float dg[RB];
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        const size_t o = (size_t)r * K + k;
-        const float rv = live[k] ? (float)rmul(S.r64[o], inv[k]) : 0.0f;
-        const float zv = rmulf(dg, rv);
-        S.r32[o] = rv;
-        S.z[o] = zv;
-        S.d[o] = 0.0f;
-        v[0][k] = radd(v[0][k], rmul((double)rv, (double)zv));
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        const bool in = i < T.nrows;
+        const size_t r = (size_t)T.row0 + i;
+        dg[u] = in ? dinv[r] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; k++) rv64[u][k] = in && live[k] ? r64[r * K + k] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        if (i >= T.nrows) continue;
+        const size_t r = (size_t)T.row0 + i;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const float rv = live[k] ? (float)rmul(rv64[u][k], inv[k]) : 0.0f;
+          const float zv = rmulf(dg[u], rv);
+          r32[r * K + k] = rv;
+          z[r * K + k] = zv;
+          d[r * K + k] = 0.0f;
+          v[0][k] = radd(v[0][k], rmul((double)rv, (double)zv));
+        }
       }
     }
     if (tile_publish<K, 1>(v, part, t, st, S.ntiles, sm)) {
+      __shared__ double tot[K];
+      sys_totals<K>(part, S.tile0, S.ntiles, tot, sm);
       if (threadIdx.x < K) {
         BSol *so = sol + S.sol0 + threadIdx.x;
         if (so->done == 0) {
-          so->rho = sys_total(part, S.tile0, S.ntiles, threadIdx.x);
+          so->rho = tot[threadIdx.x];
           so->it = 1;
           so->active = so->rho > 0.0 ? 1 : 0;
         }
@@ -344,17 +449,16 @@ __global__ void __launch_bounds__(BT) kb_init(const BSys *__restrict__ sys, BSta
 
 // PH_INNER: p = z (it == 1) or p = z + beta p, for active rhs.
 template <int K>
-__global__ void __launch_bounds__(BT) kb_p(const BSys *__restrict__ sys, const BState *state, const BSol *sol,
-                                           const BCtl *ctl) {
+__global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restrict__ sys, const BState *state,
+                                                           const BSol *sol, const BCtl *ctl) {
+  constexpr int RB = K == 1 ? 4 : 1;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
-  double *part = ctl->part;
-  (void)part;
   for (int t = t0; t < t1; t++) {
     const BTile T = tiles[t];
     if (state[T.sys].phase != PH_INNER) continue;
-    const BSys S = sys[T.sys];
+    const BSys &S = sys[T.sys];
     float beta[K];
     bool act[K], first[K];
 #pragma unroll
@@ -364,56 +468,69 @@ __global__ void __launch_bounds__(BT) kb_p(const BSys *__restrict__ sys, const B
       first[k] = so->it == 1;
       beta[k] = (float)so->beta;
     }
-    for (int i = threadIdx.x; i < T.nrows; i += BT) {
-      const size_t o = (size_t)(T.row0 + i) * K;
+    const float *__restrict__ z = S.z;
+    float *__restrict__ p = S.p;
+    for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
+      float zv[RB][K], pv[RB][K];
 #pragma unroll
-      for (int k = 0; k < K; k++)
-        if (act[k]) S.p[o + k] = first[k] ? S.z[o + k] : raddf(S.z[o + k], rmulf(beta[k], S.p[o + k]));
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        const size_t o = ((size_t)T.row0 + i) * K;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const bool need = i < T.nrows && act[k];
+          zv[u][k] = need ? z[o + k] : 0.0f;
+          pv[u][k] = need && !first[k] ? p[o + k] : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        if (i >= T.nrows) continue;
+        const size_t o = ((size_t)T.row0 + i) * K;
+#pragma unroll
+        for (int k = 0; k < K; k++)
+          if (act[k]) p[o + k] = first[k] ? zv[u][k] : raddf(zv[u][k], rmulf(beta[k], pv[u][k]));
+      }
     }
   }
 }
 
 // PH_INNER: q = A32 p ; sigma = (p, q) ; alpha = rho / sigma.
 template <int K>
-__global__ void __launch_bounds__(BT) kb_spmv(const BSys *__restrict__ sys, BState *state, BSol *sol,
-                                              const BCtl *ctl) {
+__global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_spmv(const BSys *__restrict__ sys, BState *state,
+                                                              BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  (void)part;
   for (int t = t0; t < t1; t++) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_INNER) continue;
-    const BSys S = sys[T.sys];
+    const BSys &S = sys[T.sys];
     double v[1][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = 0.0;
-    const bool wide = T.kind == 1;
-    const int step = wide ? BT / 32 : BT;
-    for (int i = wide ? (threadIdx.x >> 5) : threadIdx.x; i < T.nrows; i += step) {
-      const int r = T.row0 + i;
-      double aq[K];
-      if (wide)
-        row_multi_warp<float, float, K>(S.val32, S.ja, S.hkoffs, S.irn, r, S.p, aq);
-      else
-        row_multi<float, float, K>(S.val32, S.ja, S.hkoffs, S.irn, r, S.p, aq);
-      if (wide && (threadIdx.x & 31)) continue;
+    const float *__restrict__ p = S.p;
+    float *__restrict__ q = S.q;
+    tile_spmv<float, float, K>(S, T, S.val32, p, [&](int r, const double (&aq)[K]) {
 #pragma unroll
       for (int k = 0; k < K; k++) {
         const size_t o = (size_t)r * K + k;
         const float qv = (float)aq[k];
-        S.q[o] = qv;
-        v[0][k] = radd(v[0][k], rmul((double)S.p[o], (double)qv));
+        q[o] = qv;
+        v[0][k] = radd(v[0][k], rmul((double)p[o], (double)qv));
       }
-    }
+    });
     if (tile_publish<K, 1>(v, part, t, st, S.ntiles, sm)) {
+      __shared__ double tot[K];
+      sys_totals<K>(part, S.tile0, S.ntiles, tot, sm);
       if (threadIdx.x < K) {
         BSol *so = sol + S.sol0 + threadIdx.x;
         if (so->active) {
-          so->sigma = sys_total(part, S.tile0, S.ntiles, threadIdx.x);
+          so->sigma = tot[threadIdx.x];
           if (so->sigma > 0.0) {
             so->alpha = so->rho / so->sigma;
           } else {
@@ -433,19 +550,19 @@ __global__ void __launch_bounds__(BT) kb_spmv(const BSys *__restrict__ sys, BSta
 // PH_INNER: d += alpha p ; r -= alpha q ; z = D r ; (r,z), (r,r) ; inner stop
 // test per rhs ; all rhs stopped -> PH_XUPD.
 template <int K>
-__global__ void __launch_bounds__(BT) kb_update(const BSys *__restrict__ sys, BState *state, BSol *sol,
-                                                const BCtl *ctl) {
+__global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSys *__restrict__ sys, BState *state,
+                                                                BSol *sol, const BCtl *ctl) {
+  constexpr int RB = K == 1 ? 4 : 1;
   __shared__ double sm[32 * 2 * MAXK];
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  (void)part;
   for (int t = t0; t < t1; t++) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_INNER) continue;
-    const BSys S = sys[T.sys];
+    const BSys &S = sys[T.sys];
     float alpha[K];
     bool act[K];
 #pragma unroll
@@ -454,32 +571,61 @@ __global__ void __launch_bounds__(BT) kb_update(const BSys *__restrict__ sys, BS
       act[k] = so->active;
       alpha[k] = (float)so->alpha;
     }
+    const float *__restrict__ p = S.p;
+    const float *__restrict__ q = S.q;
+    const float *__restrict__ dinv = S.dinv;
+    float *__restrict__ d = S.d;
+    float *__restrict__ r32 = S.r32;
+    float *__restrict__ z = S.z;
     double v[2][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = v[1][k] = 0.0;
-    for (int i = threadIdx.x; i < T.nrows; i += BT) {
-      const int r = T.row0 + i;
-      const float dg = S.dinv ? S.dinv[r] : 1.0f;
+    for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
+      float dv[RB][K], pv[RB][K], rv[RB][K], qv[RB][K], dg[RB];
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        if (!act[k]) continue;
-        const size_t o = (size_t)r * K + k;
-        S.d[o] = raddf(S.d[o], rmulf(alpha[k], S.p[o]));
-        const float rv = raddf(S.r32[o], -rmulf(alpha[k], S.q[o]));
-        const float zv = rmulf(dg, rv);
-        S.r32[o] = rv;
-        S.z[o] = zv;
-        v[0][k] = radd(v[0][k], rmul((double)rv, (double)zv));
-        v[1][k] = radd(v[1][k], rmul((double)rv, (double)rv));
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        const bool in = i < T.nrows;
+        const size_t r = (size_t)T.row0 + i;
+        dg[u] = in ? dinv[r] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const bool need = in && act[k];
+          const size_t o = r * K + k;
+          dv[u][k] = need ? d[o] : 0.0f;
+          pv[u][k] = need ? p[o] : 0.0f;
+          rv[u][k] = need ? r32[o] : 0.0f;
+          qv[u][k] = need ? q[o] : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        if (i >= T.nrows) continue;
+        const size_t r = (size_t)T.row0 + i;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          if (!act[k]) continue;
+          const size_t o = r * K + k;
+          d[o] = raddf(dv[u][k], rmulf(alpha[k], pv[u][k]));
+          const float rn = raddf(rv[u][k], -rmulf(alpha[k], qv[u][k]));
+          const float zn = rmulf(dg[u], rn);
+          r32[o] = rn;
+          z[o] = zn;
+          v[0][k] = radd(v[0][k], rmul((double)rn, (double)zn));
+          v[1][k] = radd(v[1][k], rmul((double)rn, (double)rn));
+        }
       }
     }
     if (tile_publish<K, 2>(v, part, t, st, S.ntiles, sm)) {
+      __shared__ double tot[2 * K];
+      sys_totals<2 * K>(part, S.tile0, S.ntiles, tot, sm);
       if (threadIdx.x < K) {
         const int k = threadIdx.x;
         BSol *so = sol + S.sol0 + k;
         if (so->active) {
-          const double rz = sys_total(part, S.tile0, S.ntiles, k);
-          const double rr = sys_total(part, S.tile0, S.ntiles, K + k);
+          const double rz = tot[k];
+          const double rr = tot[K + k];
           so->it_total += 1;
           if (sqrt(rr) <= so->tau || so->it_total >= so->itmax || rz <= 0.0) {
             so->active = 0;
@@ -503,29 +649,48 @@ __global__ void __launch_bounds__(BT) kb_update(const BSys *__restrict__ sys, BS
 
 // PH_XUPD: x += scale * d (FP64) for rhs still running ; -> PH_RESID.
 template <int K>
-__global__ void __launch_bounds__(BT) kb_xupd(const BSys *__restrict__ sys, BState *state, const BSol *sol,
-                                              const BCtl *ctl) {
+__global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__restrict__ sys, BState *state,
+                                                              const BSol *sol, const BCtl *ctl) {
+  constexpr int RB = K == 1 ? 4 : 1;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
-  double *part = ctl->part;
-  (void)part;
   for (int t = t0; t < t1; t++) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_XUPD) continue;
-    const BSys S = sys[T.sys];
+    const BSys &S = sys[T.sys];
     double sc[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const BSol *so = sol + S.sol0 + k;
       sc[k] = so->done == 0 ? so->scale : 0.0;
     }
-    for (int i = threadIdx.x; i < T.nrows; i += BT) {
-      const size_t o = (size_t)(T.row0 + i) * K;
+    double *__restrict__ x = S.x;
+    const float *__restrict__ d = S.d;
+    for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
+      double xv[RB][K];
+      float dv[RB][K];
 #pragma unroll
-      for (int k = 0; k < K; k++)
-        if (sc[k] != 0.0) S.x[o + k] = radd(S.x[o + k], rmul(sc[k], (double)S.d[o + k]));
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        const size_t o = ((size_t)T.row0 + i) * K;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const bool need = i < T.nrows && sc[k] != 0.0;
+          xv[u][k] = need ? x[o + k] : 0.0;
+          dv[u][k] = need ? d[o + k] : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RB; u++) {
+        const int i = i0 + u * BT;
+        if (i >= T.nrows) continue;
+        const size_t o = ((size_t)T.row0 + i) * K;
+#pragma unroll
+        for (int k = 0; k < K; k++)
+          if (sc[k] != 0.0) x[o + k] = radd(xv[u][k], rmul(sc[k], (double)dv[u][k]));
+      }
     }
     __shared__ bool last;
     __syncthreads();
@@ -628,7 +793,7 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   e->K = nrhs;
   e->max_sys = max_systems;
   e->max_tiles = max_rows_total / TILE_ROWS + max_systems + 1;
-  e->grid = c.sms * 4;
+  e->grid = c.sms * 8;
   e->h_sys.assign(max_systems, BSys());
   e->h_state.assign(max_systems, BState());
   e->used.assign(max_systems, 0);

@@ -383,6 +383,9 @@ __device__ __forceinline__ double row_acc(const VT *__restrict__ vp, const int *
                                           const XT *__restrict__ xb) {
   const int st = STRIDE > 0 ? STRIDE : stride;
   double acc = 0.0;
+  // full groups unpredicated (fewest registers), then the short tail.  (A
+  // predicated last group was measured slower on B200: more registers cost
+  // more occupancy than its extra loads in flight bring.)
   int j = 0;
   for (; j + U <= n; j += U) {
     int c[U];
