@@ -287,8 +287,9 @@ int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x,
  * other systems share the engine.
  *   create : max_systems slots, max_rows_total rows over all slots
  *   add    : d_b, d_x device arrays (rows*nrhs doubles, x = x0 on entry and
- *            the solution on exit, owned by the caller), d_dinv the FP64
- *            inverse diagonal or NULL; *slot receives the slot id
+ *            the solution on exit, owned by the caller; 16-byte aligned
+ *            when nrhs is 8), d_dinv the FP64 inverse diagonal or NULL;
+ *            *slot receives the slot id
  *   step   : replays the captured iterations `replays` times (8 iterations
  *            each), then reports how many slots are still running
  *   poll   : state 0 running / 1 converged / 2 stopped (itmax, breakdown);

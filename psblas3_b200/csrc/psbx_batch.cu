@@ -125,6 +125,88 @@ __device__ __forceinline__ RowRef row_ref(const int *__restrict__ hkoffs, const 
   return rr;
 }
 
+// The K values of one row of an interleaved vector (v[row*K + k]).  Rows of
+// 8 values are 32-byte aligned (vector bases are 16-byte aligned), so they
+// move as float4 / double2.
+template <int K>
+__device__ __forceinline__ void ld_row(const float *p, float (&v)[K]) {
+  if constexpr (K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; q++) {
+      const float4 t = reinterpret_cast<const float4 *>(p)[q];
+      v[4 * q] = t.x, v[4 * q + 1] = t.y, v[4 * q + 2] = t.z, v[4 * q + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = p[k];
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void ld_row_ro(const float *__restrict__ p, float (&v)[K]) {
+  if constexpr (K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; q++) {
+      const float4 t = __ldg(reinterpret_cast<const float4 *>(p) + q);
+      v[4 * q] = t.x, v[4 * q + 1] = t.y, v[4 * q + 2] = t.z, v[4 * q + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = __ldg(p + k);
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void st_row(float *p, const float (&v)[K]) {
+  if constexpr (K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; q++)
+      reinterpret_cast<float4 *>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) p[k] = v[k];
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void ld_row(const double *p, double (&v)[K]) {
+  if constexpr (K % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 2; q++) {
+      const double2 t = reinterpret_cast<const double2 *>(p)[q];
+      v[2 * q] = t.x, v[2 * q + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = p[k];
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void ld_row_ro(const double *__restrict__ p, double (&v)[K]) {
+  if constexpr (K % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 2; q++) {
+      const double2 t = __ldg(reinterpret_cast<const double2 *>(p) + q);
+      v[2 * q] = t.x, v[2 * q + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = __ldg(p + k);
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void st_row(double *p, const double (&v)[K]) {
+  if constexpr (K % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 2; q++) reinterpret_cast<double2 *>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) p[k] = v[k];
+  }
+}
+
 // Row sums of one HLL-32 row for K interleaved vectors, entries in order.
 template <class VT, class XT, int K>
 __device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int *__restrict__ ja, RowRef rr,
@@ -147,8 +229,7 @@ __device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int 
 #pragma unroll
     for (int u = 0; u < U; u++) {
       XT xv[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) xv[k] = __ldg(x + (size_t)c[u] * K + k);
+      ld_row_ro<K>(x + (size_t)c[u] * K, xv);
 #pragma unroll
       for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul((double)v[u], (double)xv[k]));
     }
@@ -166,8 +247,7 @@ __device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int 
     for (int u = 0; u < U; u++) {
       if (j + u < n) {
         XT xv[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) xv[k] = __ldg(x + (size_t)c[u] * K + k);
+        ld_row_ro<K>(x + (size_t)c[u] * K, xv);
 #pragma unroll
         for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul((double)v[u], (double)xv[k]));
       }
@@ -187,8 +267,10 @@ __device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const
   for (int j = lane; j < rr.n; j += 32) {
     const int c = ld_stream(ja + rr.off + j * 32) - 1;
     const double v = (double)ld_stream(val + rr.off + j * 32);
+    XT xv[K];
+    ld_row_ro<K>(x + (size_t)c * K, xv);
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)__ldg(x + (size_t)c * K + k)));
+    for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)xv[k]));
   }
 #pragma unroll
   for (int k = 0; k < K; k++)
@@ -321,14 +403,15 @@ __global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys 
     const double *__restrict__ b = S.b;
     double *__restrict__ r64 = S.r64;
     tile_spmv<double, double, K>(S, T, S.val64, S.x, [&](int r, const double (&ax)[K]) {
+      double bb[K], rr[K];
+      ld_row<K>(b + (size_t)r * K, bb);
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        const double bb = b[(size_t)r * K + k];
-        const double rr = radd(bb, -ax[k]);
-        r64[(size_t)r * K + k] = rr;
-        v[0][k] = radd(v[0][k], rmul(rr, rr));
-        v[1][k] = radd(v[1][k], rmul(bb, bb));
+        rr[k] = radd(bb[k], -ax[k]);
+        v[0][k] = radd(v[0][k], rmul(rr[k], rr[k]));
+        v[1][k] = radd(v[1][k], rmul(bb[k], bb[k]));
       }
+      st_row<K>(r64 + (size_t)r * K, rr);
     });
     if (tile_publish<K, 2>(v, part, t, st, S.ntiles, sm)) {
       __shared__ double tot[2 * K];
@@ -404,26 +487,28 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
-        const bool in = i < T.nrows;
         const size_t r = (size_t)T.row0 + i;
-        dg[u] = in ? dinv[r] : 0.0f;
-#pragma unroll
-        for (int k = 0; k < K; k++) rv64[u][k] = in && live[k] ? r64[r * K + k] : 0.0;
+        if (i < T.nrows) {
+          dg[u] = dinv[r];
+          ld_row<K>(r64 + r * K, rv64[u]);
+        }
       }
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
         const size_t r = (size_t)T.row0 + i;
+        float rv[K], zv[K], dz[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-          const float rv = live[k] ? (float)rmul(rv64[u][k], inv[k]) : 0.0f;
-          const float zv = rmulf(dg[u], rv);
-          r32[r * K + k] = rv;
-          z[r * K + k] = zv;
-          d[r * K + k] = 0.0f;
-          v[0][k] = radd(v[0][k], rmul((double)rv, (double)zv));
+          rv[k] = live[k] ? (float)rmul(rv64[u][k], inv[k]) : 0.0f;
+          zv[k] = rmulf(dg[u], rv[k]);
+          dz[k] = 0.0f;
+          v[0][k] = radd(v[0][k], rmul((double)rv[k], (double)zv[k]));
         }
+        st_row<K>(r32 + r * K, rv);
+        st_row<K>(z + r * K, zv);
+        st_row<K>(d + r * K, dz);
       }
     }
     if (tile_publish<K, 1>(v, part, t, st, S.ntiles, sm)) {
@@ -470,6 +555,15 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
     }
     const float *__restrict__ z = S.z;
     float *__restrict__ p = S.p;
+    // p of a stopped rhs keeps its value; it is read only when some rhs
+    // is past its first inner iteration or stopped
+    bool any_act = false, need_p = false;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      any_act |= act[k];
+      need_p |= !act[k] || !first[k];
+    }
+    if (!any_act) continue;
     for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
       float zv[RB][K], pv[RB][K];
 #pragma unroll
@@ -477,10 +571,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
         const int i = i0 + u * BT;
         const size_t o = ((size_t)T.row0 + i) * K;
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-          const bool need = i < T.nrows && act[k];
-          zv[u][k] = need ? z[o + k] : 0.0f;
-          pv[u][k] = need && !first[k] ? p[o + k] : 0.0f;
+        for (int k = 0; k < K; k++) pv[u][k] = 0.0f;
+        if (i < T.nrows) {
+          ld_row<K>(z + o, zv[u]);
+          if (need_p) ld_row<K>(p + o, pv[u]);
         }
       }
 #pragma unroll
@@ -488,9 +582,11 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
         const size_t o = ((size_t)T.row0 + i) * K;
+        float pn[K];
 #pragma unroll
         for (int k = 0; k < K; k++)
-          if (act[k]) p[o + k] = first[k] ? zv[u][k] : raddf(zv[u][k], rmulf(beta[k], pv[u][k]));
+          pn[k] = !act[k] ? pv[u][k] : first[k] ? zv[u][k] : raddf(zv[u][k], rmulf(beta[k], pv[u][k]));
+        st_row<K>(p + o, pn);
       }
     }
   }
@@ -516,13 +612,14 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_spmv(const BSys *__rest
     const float *__restrict__ p = S.p;
     float *__restrict__ q = S.q;
     tile_spmv<float, float, K>(S, T, S.val32, p, [&](int r, const double (&aq)[K]) {
+      float pv[K], qv[K];
+      ld_row<K>(p + (size_t)r * K, pv);
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        const size_t o = (size_t)r * K + k;
-        const float qv = (float)aq[k];
-        q[o] = qv;
-        v[0][k] = radd(v[0][k], rmul((double)p[o], (double)qv));
+        qv[k] = (float)aq[k];
+        v[0][k] = radd(v[0][k], rmul((double)pv[k], (double)qv[k]));
       }
+      st_row<K>(q + (size_t)r * K, qv);
     });
     if (tile_publish<K, 1>(v, part, t, st, S.ntiles, sm)) {
       __shared__ double tot[K];
@@ -580,41 +677,44 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
     double v[2][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = v[1][k] = 0.0;
-    for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
+    // a stopped rhs keeps d and r; its z is rewritten as D r, the value it
+    // already holds
+    bool any_act = false;
+#pragma unroll
+    for (int k = 0; k < K; k++) any_act |= act[k];
+    for (int i0 = threadIdx.x; any_act && i0 < T.nrows; i0 += RB * BT) {
       float dv[RB][K], pv[RB][K], rv[RB][K], qv[RB][K], dg[RB];
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
-        const bool in = i < T.nrows;
-        const size_t r = (size_t)T.row0 + i;
-        dg[u] = in ? dinv[r] : 0.0f;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          const bool need = in && act[k];
-          const size_t o = r * K + k;
-          dv[u][k] = need ? d[o] : 0.0f;
-          pv[u][k] = need ? p[o] : 0.0f;
-          rv[u][k] = need ? r32[o] : 0.0f;
-          qv[u][k] = need ? q[o] : 0.0f;
+        const size_t o = ((size_t)T.row0 + i) * K;
+        if (i < T.nrows) {
+          dg[u] = dinv[T.row0 + i];
+          ld_row<K>(d + o, dv[u]);
+          ld_row<K>(p + o, pv[u]);
+          ld_row<K>(r32 + o, rv[u]);
+          ld_row<K>(q + o, qv[u]);
         }
       }
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
-        const size_t r = (size_t)T.row0 + i;
+        const size_t o = ((size_t)T.row0 + i) * K;
+        float dn[K], rn[K], zn[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-          if (!act[k]) continue;
-          const size_t o = r * K + k;
-          d[o] = raddf(dv[u][k], rmulf(alpha[k], pv[u][k]));
-          const float rn = raddf(rv[u][k], -rmulf(alpha[k], qv[u][k]));
-          const float zn = rmulf(dg[u], rn);
-          r32[o] = rn;
-          z[o] = zn;
-          v[0][k] = radd(v[0][k], rmul((double)rn, (double)zn));
-          v[1][k] = radd(v[1][k], rmul((double)rn, (double)rn));
+          dn[k] = act[k] ? raddf(dv[u][k], rmulf(alpha[k], pv[u][k])) : dv[u][k];
+          rn[k] = act[k] ? raddf(rv[u][k], -rmulf(alpha[k], qv[u][k])) : rv[u][k];
+          zn[k] = rmulf(dg[u], rn[k]);
+          if (act[k]) {
+            v[0][k] = radd(v[0][k], rmul((double)rn[k], (double)zn[k]));
+            v[1][k] = radd(v[1][k], rmul((double)rn[k], (double)rn[k]));
+          }
         }
+        st_row<K>(d + o, dn);
+        st_row<K>(r32 + o, rn);
+        st_row<K>(z + o, zn);
       }
     }
     if (tile_publish<K, 2>(v, part, t, st, S.ntiles, sm)) {
@@ -668,18 +768,19 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__rest
     }
     double *__restrict__ x = S.x;
     const float *__restrict__ d = S.d;
-    for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < K; k++) any |= sc[k] != 0.0;
+    for (int i0 = threadIdx.x; any && i0 < T.nrows; i0 += RB * BT) {
       double xv[RB][K];
       float dv[RB][K];
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
         const size_t o = ((size_t)T.row0 + i) * K;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          const bool need = i < T.nrows && sc[k] != 0.0;
-          xv[u][k] = need ? x[o + k] : 0.0;
-          dv[u][k] = need ? d[o + k] : 0.0f;
+        if (i < T.nrows) {
+          ld_row<K>(x + o, xv[u]);
+          ld_row<K>(d + o, dv[u]);
         }
       }
 #pragma unroll
@@ -687,9 +788,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__rest
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
         const size_t o = ((size_t)T.row0 + i) * K;
+        double xn[K];
 #pragma unroll
-        for (int k = 0; k < K; k++)
-          if (sc[k] != 0.0) x[o + k] = radd(xv[u][k], rmul(sc[k], (double)dv[u][k]));
+        for (int k = 0; k < K; k++) xn[k] = sc[k] != 0.0 ? radd(xv[u][k], rmul(sc[k], (double)dv[u][k])) : xv[u][k];
+        st_row<K>(x + o, xn);
       }
     }
     __shared__ bool last;
@@ -843,6 +945,8 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   HllDevice *m = (HllDevice *)hllMat;
   if (!e || !m || !d_b || !d_x || !slot) return SPGPU_UNSUPPORTED;
   if (m->elemType != SPGPU_TYPE_DOUBLE || m->hackSize != 32 || m->perm || m->baseIndex != 1) return SPGPU_UNSUPPORTED;
+  // rows of 8 right-hand sides move as 16-byte vectors
+  if (e->K > 1 && (((uintptr_t)d_b | (uintptr_t)d_x) & 15)) return SPGPU_UNSUPPORTED;
   if (!m->cM32) {
     int rc = psbx_hll_make_single(m);
     if (rc) return rc;
