@@ -127,6 +127,26 @@ int  axybzMultiVecDeviceDouble(int n, double alpha, void *devVecA,
 /* dvectordev.c:324-345: b = alpha*|a| ; a = alpha*|a| */
 int  absMultiVecDeviceDouble2(int n, double alpha, void *devVecA, void *devVecB);
 int  absMultiVecDeviceDouble(int n, double alpha, void *devVecA);
+/* dvectordev.h:51-61 / dvectordev.c:127-177 (spgpuDgath, spgpuDscat of
+ * cuda/spgpu/vector.h:620-653): the halo-exchange halves of the vector type
+ * (psb_d_cuda_vect_mod.F90 gthzv / sctb).  Vector vectorId of the
+ * multivector; idx holds n indexBase-based positions starting at entry
+ * first; buf (device memory) starts at entry hfirst.
+ *   gath: buf[i] = v[idx[i]]
+ *   scat: v[idx[i]] = beta*v[idx[i]] + buf[i]   (beta == 0: v not read) */
+int  igathMultiVecDeviceDouble(void *deviceVec, int vectorId, int n, int first,
+                               void *indexes, int hfirst, void *host_values,
+                               int indexBase);
+int  igathMultiVecDeviceDoubleVecIdx(void *deviceVec, int vectorId, int n,
+                                     int first, void *deviceIdx, int hfirst,
+                                     void *host_values, int indexBase);
+int  iscatMultiVecDeviceDouble(void *deviceVec, int vectorId, int n, int first,
+                               void *indexes, int hfirst, void *host_values,
+                               int indexBase, double beta);
+int  iscatMultiVecDeviceDoubleVecIdx(void *deviceVec, int vectorId, int n,
+                                     int first, void *deviceIdx, int hfirst,
+                                     void *host_values, int indexBase,
+                                     double beta);
 
 /* ======================================================================== */
 /* HLL (hacked ELLPACK): cuda/hlldev.h:96-153, cuda/hlldev_mod.F90:37-259    */

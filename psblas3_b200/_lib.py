@@ -60,6 +60,10 @@ _SIGS = {
     "xyzwMultiVecDeviceDouble": (I, [I, D, D, D, D, D, D, P, P, P, P]),
     "axyMultiVecDeviceDouble": (I, [I, D, P, P]), "axybzMultiVecDeviceDouble": (I, [I, D, P, P, D, P]),
     "absMultiVecDeviceDouble2": (I, [I, D, P, P]), "absMultiVecDeviceDouble": (I, [I, D, P]),
+    "igathMultiVecDeviceDouble": (I, [P, I, I, I, P, I, P, I]),
+    "igathMultiVecDeviceDoubleVecIdx": (I, [P, I, I, I, P, I, P, I]),
+    "iscatMultiVecDeviceDouble": (I, [P, I, I, I, P, I, P, I, D]),
+    "iscatMultiVecDeviceDoubleVecIdx": (I, [P, I, I, I, P, I, P, I, D]),
     # HLL
     "FallocHllDevice": (I, [PP, U, U, U, U, U, U]), "freeHllDevice": (None, [P]),
     "getHllDeviceParams": (I, [P, PI, PI, PI, PI, PI, PI, PI]),

@@ -201,6 +201,21 @@ __global__ void k_axybz(int n, double alpha, const double *__restrict__ a, const
   }
 }
 
+// buf[i] = v[idx[i] - base]
+__global__ void k_gath(int n, const int *__restrict__ idx, int base, const double *__restrict__ v,
+                       double *__restrict__ buf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) buf[i] = v[idx[i] - base];
+}
+
+// v[idx[i] - base] = beta * v[idx[i] - base] + buf[i]  (beta == 0: v not read)
+__global__ void k_scat(int n, const int *__restrict__ idx, int base, const double *__restrict__ buf, double beta,
+                       double *__restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int j = idx[i] - base;
+    v[j] = beta == 0.0 ? buf[i] : radd(rmul(beta, v[j]), buf[i]);
+  }
+}
+
 __global__ void k_abs(int n, double alpha, const double *__restrict__ a, double *__restrict__ b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     b[i] = rmul(alpha, fabs(a[i]));
@@ -458,6 +473,52 @@ int absMultiVecDeviceDouble2(int n, double alpha, void *devVecA, void *devVecB) 
 
 int absMultiVecDeviceDouble(int n, double alpha, void *devVecA) {
   return absMultiVecDeviceDouble2(n, alpha, devVecA, devVecA);
+}
+
+// Gather / scatter through an index list: the two halves of a halo exchange
+// (the send buffer is gathered from the owned entries, the received buffer
+// is scattered into the halo entries).  vectorId selects one of the count
+// vectors; first / hfirst are indexBase-based starts in idx / buf.
+int igathMultiVecDeviceDouble(void *deviceVec, int vectorId, int n, int first, void *indexes, int hfirst,
+                              void *host_values, int indexBase) {
+  MultiVectDevice *x = MV(deviceVec);
+  if (!x || (n > 0 && (!indexes || !host_values)) || vectorId < 0 || vectorId >= x->count_) return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  const int *idx = (const int *)indexes + (first - indexBase);
+  double *buf = (double *)host_values + (hfirst - indexBase);
+  const double *v = (const double *)x->v_ + (size_t)vectorId * x->pitch_;
+  k_gath<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, idx, indexBase, v, buf);
+  PSBX_LAUNCH_CK("k_gath");
+  return SPGPU_SUCCESS;
+}
+
+int igathMultiVecDeviceDoubleVecIdx(void *deviceVec, int vectorId, int n, int first, void *deviceIdx, int hfirst,
+                                    void *host_values, int indexBase) {
+  MultiVectDevice *ix = MV(deviceIdx);
+  if (!ix) return SPGPU_UNSUPPORTED;
+  return igathMultiVecDeviceDouble(deviceVec, vectorId, n, first, ix->v_, hfirst, host_values, indexBase);
+}
+
+int iscatMultiVecDeviceDouble(void *deviceVec, int vectorId, int n, int first, void *indexes, int hfirst,
+                              void *host_values, int indexBase, double beta) {
+  MultiVectDevice *x = MV(deviceVec);
+  if (!x || (n > 0 && (!indexes || !host_values)) || vectorId < 0 || vectorId >= x->count_) return SPGPU_UNSUPPORTED;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  const int *idx = (const int *)indexes + (first - indexBase);
+  const double *buf = (const double *)host_values + (hfirst - indexBase);
+  double *v = (double *)x->v_ + (size_t)vectorId * x->pitch_;
+  k_scat<<<psbx_grid_for(n, VT), VT, 0, c.stream>>>(n, idx, indexBase, buf, beta, v);
+  PSBX_LAUNCH_CK("k_scat");
+  return SPGPU_SUCCESS;
+}
+
+int iscatMultiVecDeviceDoubleVecIdx(void *deviceVec, int vectorId, int n, int first, void *deviceIdx, int hfirst,
+                                    void *host_values, int indexBase, double beta) {
+  MultiVectDevice *ix = MV(deviceIdx);
+  if (!ix) return SPGPU_UNSUPPORTED;
+  return iscatMultiVecDeviceDouble(deviceVec, vectorId, n, first, ix->v_, hfirst, host_values, indexBase, beta);
 }
 
 }  // extern "C"

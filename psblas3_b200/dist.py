@@ -1,0 +1,228 @@
+"""Row-block distribution of one matrix over ranks, with a halo exchange.
+
+This is the distributed SpMV of base/psblas/psb_dspmm.f90:196-216: each
+rank owns a contiguous block of rows and the matching entries of x; its
+local matrix is split into the block whose columns it owns (a%ad) and the
+block whose columns belong to other ranks (a%and).  The product is
+
+    send: gather the owned entries other ranks need        (psi_swapdata send)
+    y  = alpha * A_d x_owned + beta * y                    (overlaps the exchange)
+    recv: scatter the received entries into the halo part  (psi_swapdata recv)
+    y  = alpha * A_nd x + 1 * y
+
+with the local vector laid out as in the reference's descriptor: the nl
+owned entries first, then the nh halo entries (global indices sorted), so
+that A_nd's columns are local indices nl .. nl+nh-1.
+
+The host side (partition, halo lists, exchange plan) is plain Python and is
+what every rank computes identically; the device side (gather, SpMV,
+scatter) runs the library's kernels through the C-ABI.  The exchange itself
+is a torch.distributed all_to_all_single of the gathered buffers: NCCL on
+GPUs, gloo on CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = ["partition_rows", "LocalPart", "local_part", "ExchangePlan", "exchange_plan",
+           "build_part_on_rank", "halo_exchange", "DistSpMV"]
+
+
+def partition_rows(n, world):
+    """Contiguous row blocks [lo, hi) whose sizes differ by at most one
+    (the block distribution of psb_cdall with a uniform local size)."""
+    n, world = int(n), int(world)
+    base, extra = divmod(n, world)
+    out, lo = [], 0
+    for r in range(world):
+        hi = lo + base + (1 if r < extra else 0)
+        out.append((lo, hi))
+        lo = hi
+    return out
+
+
+def owner_of(g, blocks):
+    """Rank owning each global index in g (0-based)."""
+    starts = np.array([b[0] for b in blocks], dtype=np.int64)
+    return np.searchsorted(starts, np.asarray(g, dtype=np.int64), side="right") - 1
+
+
+@dataclass
+class LocalPart:
+    """One rank's rows.  ad / and_ are 1-based CSR triples in local column
+    numbering: ad has columns 1..nl, and_ has columns nl+1..nl+nh."""
+    lo: int
+    hi: int
+    halo: np.ndarray                      # global (0-based) ids of the halo entries, sorted
+    ad: tuple = field(repr=False)
+    and_: tuple = field(repr=False)
+
+    @property
+    def nl(self):
+        return self.hi - self.lo
+
+    @property
+    def nh(self):
+        return len(self.halo)
+
+    @property
+    def ncol(self):
+        return self.nl + self.nh
+
+
+def local_part(irp, ja, val, lo, hi):
+    """Split rows lo..hi-1 of a 1-based global CSR into the owned-column
+    block and the halo block (entry order inside each row is kept)."""
+    irp = np.asarray(irp, dtype=np.int64)
+    ja = np.asarray(ja, dtype=np.int64)
+    val = np.asarray(val, dtype=np.float64)
+    s, e = irp[lo] - 1, irp[hi] - 1
+    rows = np.repeat(np.arange(hi - lo), np.diff(irp[lo:hi + 1]))
+    cols = ja[s:e] - 1
+    vals = val[s:e]
+    own = (cols >= lo) & (cols < hi)
+    halo = np.unique(cols[~own])
+    nl = hi - lo
+
+    def csr(mask, local_cols):
+        r = rows[mask]
+        cnt = np.bincount(r, minlength=nl)
+        p = np.zeros(nl + 1, np.int32)
+        p[1:] = np.cumsum(cnt)
+        return p + 1, (local_cols + 1).astype(np.int32), np.ascontiguousarray(vals[mask])
+
+    ad = csr(own, cols[own] - lo)
+    and_ = csr(~own, nl + np.searchsorted(halo, cols[~own]))
+    return LocalPart(int(lo), int(hi), halo.astype(np.int64), ad, and_)
+
+
+@dataclass
+class ExchangePlan:
+    """send_idx: 1-based local (owned) indices to gather, grouped by
+    destination rank in rank order; send_counts / recv_counts per rank.
+    Received entries arrive grouped by source rank in rank order, which is
+    the order of the sorted halo, so they scatter to local nl+1..nl+nh."""
+    send_idx: np.ndarray
+    send_counts: list
+    recv_counts: list
+
+
+def exchange_plan(rank, blocks, halos):
+    """Plan of `rank` from every rank's halo list (global ids, sorted)."""
+    world = len(blocks)
+    lo, hi = blocks[rank]
+    recv_counts = [0] * world
+    own = owner_of(halos[rank], blocks) if len(halos[rank]) else np.zeros(0, np.int64)
+    for q in range(world):
+        recv_counts[q] = int(np.count_nonzero(own == q))
+    assert recv_counts[rank] == 0, "a halo entry is owned by this rank"
+    send, send_counts = [], []
+    for q in range(world):
+        h = np.asarray(halos[q], dtype=np.int64)
+        mine = h[(h >= lo) & (h < hi)] if q != rank else h[:0]
+        send.append(mine - lo + 1)
+        send_counts.append(int(len(mine)))
+    idx = np.concatenate(send).astype(np.int32) if send else np.zeros(0, np.int32)
+    return ExchangePlan(idx, send_counts, recv_counts)
+
+
+def build_part_on_rank(irp, ja, val, rank, world, all_gather=None):
+    """This rank's LocalPart and ExchangePlan.  The rank needs only its own
+    rows; the halo lists of the others come through `all_gather`
+    (obj -> list over ranks; torch.distributed.all_gather_object by default)."""
+    n = len(irp) - 1
+    blocks = partition_rows(n, world)
+    part = local_part(irp, ja, val, *blocks[rank])
+    if world == 1:
+        halos = [part.halo]
+    elif all_gather is None:
+        import torch.distributed as dist
+        halos = [None] * world
+        dist.all_gather_object(halos, part.halo)
+    else:
+        halos = all_gather(part.halo)
+    return part, exchange_plan(rank, blocks, halos), blocks
+
+
+def halo_exchange(sendbuf, recvbuf, plan, async_op=False):
+    """All-to-all of the gathered send buffer into the receive buffer (torch
+    tensors on the process group's device: CUDA under NCCL, CPU under
+    gloo).  Returns the work handle when async_op."""
+    import torch.distributed as dist
+    return dist.all_to_all_single(recvbuf, sendbuf, output_split_sizes=list(plan.recv_counts),
+                                  input_split_sizes=list(plan.send_counts), async_op=async_op)
+
+
+class DistSpMV:
+    """y = alpha*A*x + beta*y for this rank's rows on its GPU.
+
+    x is a DVect of length ncol (owned entries, then halo); y a DVect of
+    length nl.  `exchange(sendbuf, recvbuf, plan)` moves the gathered
+    buffers (torch CUDA tensors) and may return a handle with .wait(); the
+    default is halo_exchange over the default process group, asynchronous,
+    so the A_d product overlaps it."""
+
+    def __init__(self, part: LocalPart, plan: ExchangePlan, hksz=32):
+        import torch
+        from . import psb
+        self.psb, self.part, self.plan = psb, part, plan
+        nl, ncol = part.nl, part.ncol
+        self._keep = []
+
+        def dev_hll(trip, cols):
+            irp, ja, va = trip
+            nz = int(irp[-1] - 1)
+            d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in
+                 (irp.astype(np.int32), ja.astype(np.int32) if nz else np.zeros(1, np.int32),
+                  va if nz else np.zeros(1))]
+            self._keep.append(d)
+            return psb.HllMat.from_csr_device(nl, cols, nz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), hksz)
+
+        self.Ad = dev_hll(part.ad, nl)
+        self.And = dev_hll(part.and_, ncol) if part.nh else None
+        ns, nr = int(sum(plan.send_counts)), int(sum(plan.recv_counts))
+        self.send_idx = torch.from_numpy(np.ascontiguousarray(plan.send_idx)).cuda() if ns else None
+        self.recv_idx = torch.arange(nl + 1, ncol + 1, dtype=torch.int32, device="cuda") if nr else None
+        self.sendbuf = torch.empty(max(ns, 1), dtype=torch.float64, device="cuda")
+        self.recvbuf = torch.empty(max(nr, 1), dtype=torch.float64, device="cuda")
+        self.ns, self.nr = ns, nr
+        self.comm = torch.cuda.Stream() if (ns or nr) else None
+
+    def gather(self, x):
+        if self.ns:
+            self.psb.check(self.psb.lib.igathMultiVecDeviceDouble(
+                x.h, 0, self.ns, 1, C.c_void_p(self.send_idx.data_ptr()), 1, C.c_void_p(self.sendbuf.data_ptr()), 1),
+                "igathMultiVecDeviceDouble")
+
+    def scatter(self, x):
+        if self.nr:
+            self.psb.check(self.psb.lib.iscatMultiVecDeviceDouble(
+                x.h, 0, self.nr, 1, C.c_void_p(self.recv_idx.data_ptr()), 1, C.c_void_p(self.recvbuf.data_ptr()), 1,
+                0.0), "iscatMultiVecDeviceDouble")
+
+    def __call__(self, alpha, x, beta, y, exchange=None):
+        import torch
+        psb = self.psb
+        lib_stream = torch.cuda.ExternalStream(psb.lib.psb_cudaGetStream())
+        self.gather(x)
+        work = None
+        if self.comm is not None:
+            # the exchange runs on its own stream once the gather is done
+            self.comm.wait_stream(lib_stream)
+            with torch.cuda.stream(self.comm):
+                if exchange is None:
+                    work = halo_exchange(self.sendbuf[:self.ns], self.recvbuf[:self.nr], self.plan, async_op=True)
+                else:
+                    work = exchange(self.sendbuf[:self.ns], self.recvbuf[:self.nr], self.plan)
+        self.Ad.spmv(alpha, x, beta, y)          # owned columns, overlapping the exchange
+        if self.comm is not None:
+            with torch.cuda.stream(lib_stream):
+                if work is not None and hasattr(work, "wait"):
+                    work.wait()
+            lib_stream.wait_stream(self.comm)
+        if self.And is not None:
+            self.scatter(x)
+            self.And.spmv(alpha, x, 1.0, y)

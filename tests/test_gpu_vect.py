@@ -121,3 +121,34 @@ def test_elementwise_family(psb, n):
     A.set_scal(3.0, first=1, last=max(1, n // 2))
     got = A.get_vect()
     assert np.all(got[: max(1, n // 2)] == 3.0)
+
+
+def test_gather_scatter_halo_halves(psb):
+    """igath / iscat (dvectordev.c:127-177): buf[i] = v[idx[i]] and
+    v[idx[i]] = beta*v[idx[i]] + buf[i], 1-based indices, with first/hfirst
+    offsets; bit-exact against numpy."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(7)
+    n, m = 5000, 777
+    v = rng.uniform(-1, 1, n)
+    idx = rng.choice(n, m, replace=False).astype(np.int32) + 1
+    V = psb.DVect.bld(v)
+    d_idx = torch.from_numpy(idx).cuda()
+    buf = torch.zeros(m + 3, dtype=torch.float64, device="cuda")
+    # gather entries 3..m of idx into buf starting at entry 4
+    rc = psb.lib.igathMultiVecDeviceDouble(V.h, 0, m - 2, 3, C.c_void_p(d_idx.data_ptr()), 4,
+                                           C.c_void_p(buf.data_ptr()), 1)
+    assert rc == 0
+    got = buf.cpu().numpy()
+    assert np.array_equal(got[3:m + 1], v[idx[2:] - 1]) and not got[:3].any()
+    w = rng.uniform(-1, 1, m)
+    d_w = torch.from_numpy(w).cuda()
+    for beta in (0.0, 1.0, -2.5):
+        V.set_vect(v)
+        rc = psb.lib.iscatMultiVecDeviceDouble(V.h, 0, m, 1, C.c_void_p(d_idx.data_ptr()), 1,
+                                               C.c_void_p(d_w.data_ptr()), 1, beta)
+        assert rc == 0
+        ref = v.copy()
+        ref[idx - 1] = w if beta == 0.0 else beta * v[idx - 1] + w
+        assert np.array_equal(V.get_vect(), ref)
