@@ -71,10 +71,12 @@ class Request:
 
 class Server:
     def __init__(self, pool, hbm_budget=150e9, max_slots=512, max_rows_total=200_000_000, inner_tol=1e-4,
-                 itmax=200_000, replays_per_step=1):
+                 itmax=200_000, replays_per_step=1, engine=None):
+        """engine: a psb.BatchSolver-like object (add/step/poll/remove/free);
+        by default a new 1-rhs batch engine with max_slots slots."""
         self.pool = pool
         self.budget = float(hbm_budget) - pool.device_bytes
-        self.eng = psb.BatchSolver(max_slots, max_rows_total, 1)
+        self.eng = engine if engine is not None else psb.BatchSolver(max_slots, max_rows_total, 1)
         self.max_slots = max_slots
         self.max_rows = max_rows_total
         self.queue = collections.deque()
