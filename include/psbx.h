@@ -249,9 +249,12 @@ int psbx_DefaultSolverOptions(psbx_SolverOptions *opt);
 #define PSBX_FMT_ELL 1
 #define PSBX_FMT_CSR 2
 
-/* Device-resident psb_krylov('CG'|'BICGSTAB') (krylov/psb_dkrylov.f90:
- * 179-210 dispatch, psb_dcg.F90:218-295, psb_dcgstab.f90:226-365) with the
- * diagonal preconditioner (prec/impl/psb_d_diagprec_impl.f90:116):
+/* Device-resident psb_krylov('CG'|'FCG'|'BICGSTAB'|'RGMRES') (krylov/
+ * psb_dkrylov.f90:179-210 dispatch, psb_dcg.F90:218-295, psb_dfcg.F90,
+ * psb_dcgstab.f90:226-365, psb_drgmres.f90) with the diagonal
+ * preconditioner (prec/impl/psb_d_diagprec_impl.f90:116).  RGMRES (also
+ * 'GMRES') restarts every opt->irst steps and takes istop 2 only (the
+ * reference also accepts 1); other method names return 1.
  *   mat   HLL / ELL handle, or a psbx_d_Cmat* for CSR (fmt selects)
  *   dinv  MultiVectDevice with the inverse diagonal, or NULL for no prec
  *   b, x  MultiVectDevice (x holds x0 on entry, the solution on exit)

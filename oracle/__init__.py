@@ -65,11 +65,16 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
-        for name in ("or_cg", "or_bicgstab"):
+        for name in ("or_cg", "or_bicgstab", "or_fcg"):
             f = getattr(L, name)
             f.restype = I
             f.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I,
                           C.POINTER(I), C.POINTER(D), C.c_void_p]
+        L.or_rgmres.restype = I
+        L.or_rgmres.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I, I,
+                                C.POINTER(I), C.POINTER(D), C.c_void_p]
+        L.or_drotg.restype = None
+        L.or_drotg.argtypes = [C.POINTER(D)] * 4
         _lib = L
     return _lib
 
@@ -222,18 +227,23 @@ def diag_prec_build(diag):
 
 # ---------------------------------------------------------------- Krylov
 def krylov(method, irp, ja, val, b, x0=None, dinv=None, eps=1e-6, itmax=1000, istop=2,
-           history=False):
-    """psb_krylov('CG'|'BICGSTAB') restated; returns (x, iter, err[, hist])."""
+           history=False, irst=10):
+    """psb_krylov('CG'|'FCG'|'BICGSTAB'|'RGMRES') restated; returns
+    (x, iter, err[, hist]).  irst is the GMRES restart length."""
     n = len(irp) - 1
     x = np.zeros(n) if x0 is None else _f64(x0).copy()
     it, err = C.c_int(0), C.c_double(0.0)
-    hist = np.full(itmax + 1, np.nan) if history else None
+    hist = np.full(itmax + irst + 2, np.nan) if history else None
     d = None if dinv is None else _f64(dinv)
-    f = {"CG": lib().or_cg, "BICGSTAB": lib().or_bicgstab}[method.upper()]
-    rc = f(n, _i32(irp), _i32(ja), _f64(val),
-           None if d is None else d.ctypes.data_as(C.c_void_p),
-           _f64(b), x, float(eps), int(itmax), int(istop), C.byref(it), C.byref(err),
-           None if hist is None else hist.ctypes.data_as(C.c_void_p))
+    m = method.upper()
+    args = [n, _i32(irp), _i32(ja), _f64(val), None if d is None else d.ctypes.data_as(C.c_void_p),
+            _f64(b), x, float(eps), int(itmax), int(istop)]
+    if m in ("RGMRES", "GMRES"):
+        args.append(int(irst))
+        f = lib().or_rgmres
+    else:
+        f = {"CG": lib().or_cg, "BICGSTAB": lib().or_bicgstab, "FCG": lib().or_fcg}[m]
+    rc = f(*args, C.byref(it), C.byref(err), None if hist is None else hist.ctypes.data_as(C.c_void_p))
     if rc != 0:
         raise ValueError(f"oracle krylov failed rc={rc}")
     if history:

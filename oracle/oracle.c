@@ -668,3 +668,189 @@ done:
   free(q); free(r); free(p); free(v); free(s); free(t); free(z); free(f);
   return rc;
 }
+
+/* krylov/psb_dfcg.F90 (psb_dfcg_vect): flexible CG, restart loop included.
+ * init_conv runs once before the restart loop; each restart recomputes
+ * r = b - A x; beta == 0 after a restart ends the solve, delta == 0 inside
+ * the iteration goes back to the restart. */
+int or_fcg(int n, const int *irp, const int *ja, const double *val,
+           const double *dinv, const double *b, double *x, double eps,
+           int itmax, int istop, int *iter, double *err, double *res_hist)
+{
+  double *v = (double *)calloc(n, sizeof(double));
+  double *w = (double *)calloc(n, sizeof(double));
+  double *d = (double *)calloc(n, sizeof(double));
+  double *q = (double *)calloc(n, sizeof(double));
+  double *r = (double *)calloc(n, sizeof(double));
+  conv_t c;
+  int itx = 0, rc = 0;
+  double alpha, beta, gamma, delta, theta;
+  if (init_conv(&c, istop, itmax, eps, n, irp, ja, val, b, x)) { rc = 1; goto done; }
+  for (;;) {
+    if (itx >= itmax) break;
+    or_axpby(n, 1.0, b, 0.0, r);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    if (check_conv(&c, itx, n, x, r)) break;
+    if (res_hist) res_hist[itx] = end_err(&c);
+    prec_apply(n, dinv, r, v);
+    or_csr_csmv('N', n, n, irp, ja, val, 1.0, v, 0.0, w);
+    alpha = or_dot(n, r, v);
+    beta = or_dot(n, w, v);
+    if (beta == 0.0) break;
+    or_axpby(n, 1.0, v, 0.0, d);
+    or_axpby(n, 1.0, w, 0.0, q);
+    delta = beta;
+    theta = alpha / delta;
+    or_axpby(n, theta, d, 1.0, x);
+    or_axpby(n, -theta, q, 1.0, r);
+    int conv = 0;
+    for (;;) {
+      itx++;
+      int stop = check_conv(&c, itx, n, x, r);
+      if (res_hist && itx <= itmax) res_hist[itx] = end_err(&c);
+      if (stop) { conv = 1; break; }
+      prec_apply(n, dinv, r, v);
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, v, 0.0, w);
+      alpha = or_dot(n, r, v);
+      beta = or_dot(n, w, v);
+      gamma = or_dot(n, q, v);
+      theta = gamma / delta;
+      or_axpby(n, 1.0, v, -theta, d);
+      or_axpby(n, 1.0, w, -theta, q);
+      delta = beta - (gamma * gamma) / delta;
+      if (delta == 0.0) break;
+      theta = alpha / delta;
+      or_axpby(n, theta, d, 1.0, x);
+      or_axpby(n, -theta, q, 1.0, r);
+    }
+    if (conv) break;
+  }
+  *iter = itx;
+  *err = end_err(&c);
+done:
+  free(v); free(w); free(d); free(q); free(r);
+  return rc;
+}
+
+/* Plane rotations and the triangular solve that the reference takes from
+ * external BLAS (third party, version not pinned): restated from the
+ * classic netlib reference BLAS (drotg of LAPACK <= 3.9, drot, dtrsm
+ * 'L','U','N','N' with one right-hand side), with rounded operations. */
+void or_drotg(double *a, double *b, double *c, double *s)
+{
+  const double roe = fabs(*a) > fabs(*b) ? *a : *b;
+  const double scale = fabs(*a) + fabs(*b);
+  double r, z;
+  if (scale == 0.0) {
+    *c = 1.0; *s = 0.0; r = 0.0; z = 0.0;
+  } else {
+    const double ta = *a / scale, tb = *b / scale;
+    r = scale * sqrt(ta * ta + tb * tb);
+    r = (roe >= 0.0 ? 1.0 : -1.0) * r;
+    *c = *a / r;
+    *s = *b / r;
+    z = 1.0;
+    if (fabs(*a) > fabs(*b)) z = *s;
+    if (fabs(*b) >= fabs(*a) && *c != 0.0) z = 1.0 / *c;
+  }
+  *a = r;
+  *b = z;
+}
+
+static inline void drot1(double *x, double *y, double c, double s)
+{
+  const double t = c * *x + s * *y;
+  *y = c * *y - s * *x;
+  *x = t;
+}
+
+/* B(1:m) = U(1:m,1:m)^-1 B, U upper triangular column-major, leading dim ld */
+static void trsm_upper(int m, const double *u, int ld, double *bv)
+{
+  for (int k = m - 1; k >= 0; k--) {
+    if (bv[k] != 0.0) {
+      bv[k] = bv[k] / u[k + (size_t)k * ld];
+      for (int i = 0; i < k; i++) bv[i] = bv[i] - bv[k] * u[i + (size_t)k * ld];
+    }
+  }
+}
+
+/* krylov/psb_drgmres.f90 (psb_drgmres_vect): restarted right-preconditioned
+ * GMRES(nl), modified Gram-Schmidt, Givens rotations, stop test istop 2
+ * (||r||_2 <= eps ||b||_2 with the rotated residual estimate |rs(i+1)|).
+ * The cosine is stored through cmplx(tmp, dzero) without a KIND argument
+ * (psb_drgmres.f90, after drotg), which makes it default (single)
+ * precision: c(i) = (double)(float)tmp here as well.  istop other than 2
+ * returns 2 (the reference accepts 1 and 2; its istop 1 branch keeps
+ * adding into xt across inner iterations and restarts). */
+int or_rgmres(int n, const int *irp, const int *ja, const double *val,
+              const double *dinv, const double *b, double *x, double eps,
+              int itmax, int istop, int irst, int *iter, double *err,
+              double *res_hist)
+{
+  if (istop != 2) return 2;
+  if (irst <= 0) return 1;
+  const int nl = irst, ld = irst + 1;
+  double *V = (double *)calloc((size_t)(nl + 1) * n + 1, sizeof(double));
+  double *w = (double *)calloc(n + 1, sizeof(double));
+  double *w1 = (double *)calloc(n + 1, sizeof(double));
+  double *h = (double *)calloc((size_t)ld * ld, sizeof(double));
+  double *cs = (double *)calloc(ld, sizeof(double));
+  double *sn = (double *)calloc(ld, sizeof(double));
+  double *rs = (double *)calloc(ld, sizeof(double));
+  const double bn2 = or_nrm2(n, b);
+  double errnum = 0.0, errden = 1.0;
+  int itx = 0;
+#define VK(k) (V + (size_t)(k) * n)
+#define H(r, c) h[(r) + (size_t)(c) * ld]
+  for (;;) {
+    double *v1 = VK(0);
+    or_axpby(n, 1.0, b, 0.0, v1);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, v1);
+    rs[0] = or_nrm2(n, v1);
+    for (int k = 1; k < ld; k++) rs[k] = 0.0;
+    double scal = 1.0 / rs[0];
+    errnum = or_nrm2(n, v1);
+    errden = bn2;
+    if (res_hist && itx <= itmax) res_hist[itx] = errden == 0.0 ? errnum : errnum / errden;
+    if (errnum <= eps * errden) break;
+    for (int j = 0; j < n; j++) v1[j] = scal * v1[j];
+    if (itx >= itmax) break;
+    int conv = 0, m = nl;
+    for (int i = 1; i <= nl; i++) {
+      itx++;
+      prec_apply(n, dinv, VK(i - 1), w1);
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, w1, 0.0, w);
+      for (int k = 1; k <= i; k++) {
+        H(k - 1, i - 1) = or_dot(n, VK(k - 1), w);
+        or_axpby(n, -H(k - 1, i - 1), VK(k - 1), 1.0, w);
+      }
+      H(i, i - 1) = or_nrm2(n, w);
+      scal = 1.0 / H(i, i - 1);
+      or_axpby(n, scal, w, 0.0, VK(i));
+      for (int k = 2; k <= i; k++) drot1(&H(k - 2, i - 1), &H(k - 1, i - 1), cs[k - 2], sn[k - 2]);
+      double rti = H(i - 1, i - 1), rti1 = H(i, i - 1), tmp;
+      or_drotg(&rti, &rti1, &tmp, &sn[i - 1]);
+      cs[i - 1] = (double)(float)tmp;
+      drot1(&H(i - 1, i - 1), &H(i, i - 1), cs[i - 1], sn[i - 1]);
+      H(i, i - 1) = 0.0;
+      drot1(&rs[i - 1], &rs[i], cs[i - 1], sn[i - 1]);
+      errnum = fabs(rs[i]);
+      errden = bn2;
+      if (res_hist && itx <= itmax) res_hist[itx] = errden == 0.0 ? errnum : errnum / errden;
+      if (errnum <= eps * errden) { conv = 1; m = i; break; }
+    }
+    trsm_upper(m, h, ld, rs);
+    for (int j = 0; j < n; j++) w1[j] = 0.0;
+    for (int k = 1; k <= m; k++) or_axpby(n, rs[k - 1], VK(k - 1), 1.0, w1);
+    prec_apply(n, dinv, w1, w);
+    or_axpby(n, 1.0, w, 1.0, x);
+    if (conv) break;
+  }
+#undef VK
+#undef H
+  *iter = itx;
+  *err = errden == 0.0 ? errnum : errnum / errden;
+  free(V); free(w); free(w1); free(h); free(cs); free(sn); free(rs);
+  return 0;
+}

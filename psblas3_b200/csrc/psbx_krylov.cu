@@ -30,30 +30,25 @@
 #include <strings.h>
 #include <vector>
 
-enum { ST_RUN = 0, ST_DONE = 1, ST_BREAK = 2 };
+// ST_XUPD: a GMRES cycle ended (converged or nl steps); x is updated next.
+enum { ST_RUN = 0, ST_DONE = 1, ST_BREAK = 2, ST_XUPD = 3 };
 
 struct KState {
   double rho, rho_old, sigma, alpha, beta, omega, tau;
   double bn2, bni, ani, r0n2;
   double errnum, errden, eps;
+  double gamma, delta, theta1, theta2;  // FCG
+  double scal;                          // GMRES: scale of the next basis vector
   int itmax, istop;
   int it, itx;
   int status;
   int r0set;
+  int first;                            // FCG: first step after a restart
+  int gm_m, gm_conv;                    // GMRES: basis vectors in the x update; converged
 };
 
 #define KT 256
 #define KLANES 4
-
-struct KWork {
-  int n = 0;
-  int grid = 0;
-  double *vec = nullptr;     // nvec * n doubles
-  KState *S = nullptr;       // device
-  KState *hS = nullptr;      // pinned host mirror
-  double *part = nullptr;    // KLANES * grid
-  unsigned *ticket = nullptr;  // 8
-};
 
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ bool stopped(const KState *S) { return *((volatile const int *)&S->status) != ST_RUN; }
@@ -480,6 +475,381 @@ __global__ void __launch_bounds__(KT) k_bcg_update(KState *S, int n, const doubl
   }
 }
 
+// ---------------------------------------------------------------- FCG
+// krylov/psb_dfcg.F90: per iteration w = A v and three dots (one kernel),
+// then d, q, x, r updates, v = M^-1 r and the stop-test norms (one kernel).
+
+// restart: r = b - A*x ; v = M^-1 r ; stop test at itx (no increment)
+template <class View>
+__global__ void __launch_bounds__(KT) k_fcg_init(View A, KState *S, const double *__restrict__ b,
+                                                 const double *__restrict__ x, const double *__restrict__ dinv,
+                                                 double *__restrict__ r, double *__restrict__ v,
+                                                 double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                 int grid) {
+  __shared__ double sm[192];
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double ax = row_dot(A, s, x);
+    const int i = out_row(A, s);
+    const double ri = radd(rmul(-1.0, ax), b[i]);
+    r[i] = ri;
+    v[i] = prec(dinv, i, ri);
+    dd_add_prod(acc[0], ri, ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(ld_ro(x + i)));
+  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      const double rr = dd_value(o[0]);
+      if (S->istop == 3 && !S->r0set) {  // psb_init_conv runs once, before the restart loop
+        S->r0n2 = sqrt(rr);
+        S->r0set = 1;
+      }
+      S->status = check_conv(S, rr, m[0], m[1]) ? ST_DONE : ST_RUN;
+      S->first = 1;
+      *ticket = 0;
+    }
+  }
+}
+
+// w = A*v ; alpha = (r,v), beta = (w,v), gamma = (q,v) ; new delta and the
+// two step lengths (psb_dfcg.F90 restart block and iteration block)
+template <class View>
+__global__ void __launch_bounds__(KT) k_fcg_spmv(View A, KState *S, const double *__restrict__ v,
+                                                 const double *__restrict__ r, const double *__restrict__ q,
+                                                 double *__restrict__ w, double *__restrict__ part,
+                                                 unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[192];
+  if (stopped(S)) return;
+  const bool first = S->first;
+  dd_t acc[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double wi = row_dot(A, s, v);
+    const int i = out_row(A, s);
+    const double vi = ld_ro(v + i);
+    w[i] = wi;
+    dd_add_prod(acc[0], ld_ro(r + i), vi);
+    dd_add_prod(acc[1], wi, vi);
+    if (!first) dd_add_prod(acc[2], ld_ro(q + i), vi);
+  }
+  block_sum_dd<3>(acc, sm);
+  publish_sums<3>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[3];
+    final_sum_dd<3>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      const double alpha = dd_value(o[0]), beta = dd_value(o[1]);
+      if (first) {
+        if (beta == 0.0) {
+          S->status = ST_DONE;  // exit restart on beta == 0
+        } else {
+          S->delta = beta;
+          S->theta2 = alpha / S->delta;
+        }
+      } else {
+        const double gamma = dd_value(o[2]);
+        S->theta1 = gamma / S->delta;
+        S->delta = beta - (gamma * gamma) / S->delta;
+        if (S->delta == 0.0) S->status = ST_BREAK;  // exit iteration: back to the restart
+        else S->theta2 = alpha / S->delta;
+      }
+      *ticket = 0;
+    }
+  }
+}
+
+// d = v (first) or d = v - theta1 d ; q = w (first) or q = w - theta1 q ;
+// x = theta2 d + x ; r = -theta2 q + r ; v = M^-1 r ; itx += 1 ; stop test
+__global__ void __launch_bounds__(KT) k_fcg_update(KState *S, int n, const double *__restrict__ w,
+                                                   const double *__restrict__ dinv, double *__restrict__ v,
+                                                   double *__restrict__ d, double *__restrict__ q,
+                                                   double *__restrict__ x, double *__restrict__ r,
+                                                   double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                   int grid) {
+  __shared__ double sm[192];
+  if (stopped(S)) return;
+  const bool first = S->first;
+  const double mt1 = -S->theta1, t2 = S->theta2, mt2 = -S->theta2;
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    double di, qi;
+    if (first) {
+      di = v[i];
+      qi = w[i];
+    } else {
+      di = radd(v[i], rmul(mt1, d[i]));
+      qi = radd(w[i], rmul(mt1, q[i]));
+    }
+    const double xi = radd(rmul(t2, di), x[i]);
+    const double ri = radd(rmul(mt2, qi), r[i]);
+    d[i] = di;
+    q[i] = qi;
+    x[i] = xi;
+    r[i] = ri;
+    v[i] = prec(dinv, i, ri);
+    dd_add_prod(acc[0], ri, ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(xi));
+  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      S->first = 0;
+      S->itx += 1;
+      if (check_conv(S, dd_value(o[0]), m[0], m[1])) S->status = ST_DONE;
+      *ticket = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- RGMRES
+// krylov/psb_drgmres.f90, istop 2: one restart cycle of nl inner steps is
+// resid | (next, SpMV + h(1,i), MGS steps k = 2..i, last MGS + ||w||) x nl
+// | triangular solve | x update.  The small Hessenberg problem (h, c, s, rs)
+// lives in device memory and is updated by one thread in the finalisers.
+struct GmSmall {
+  int ld;        // nl + 1
+  double *h;     // ld*ld, column-major
+  double *c, *s, *rs;  // ld each
+};
+
+// plane rotation of netlib drot with one element
+__device__ __forceinline__ void drot1(double &x, double &y, double c, double s) {
+  const double t = radd(rmul(c, x), rmul(s, y));
+  y = radd(rmul(c, y), -rmul(s, x));
+  x = t;
+}
+
+// netlib drotg (LAPACK <= 3.9); a <- r, b <- z
+__device__ __forceinline__ void drotg(double &a, double &b, double &c, double &s) {
+  const double roe = fabs(a) > fabs(b) ? a : b;
+  const double scale = radd(fabs(a), fabs(b));
+  double r, z;
+  if (scale == 0.0) {
+    c = 1.0;
+    s = 0.0;
+    r = 0.0;
+    z = 0.0;
+  } else {
+    const double ta = a / scale, tb = b / scale;
+    r = rmul(scale, sqrt(radd(rmul(ta, ta), rmul(tb, tb))));
+    r = rmul(roe >= 0.0 ? 1.0 : -1.0, r);
+    c = a / r;
+    s = b / r;
+    z = 1.0;
+    if (fabs(a) > fabs(b)) z = s;
+    if (fabs(b) >= fabs(a) && c != 0.0) z = 1.0 / c;
+  }
+  a = r;
+  b = z;
+}
+
+// restart: v1 = b - A*x ; rs(1) = ||v1|| ; stop test ; scal = 1/rs(1)
+template <class View>
+__global__ void __launch_bounds__(KT) k_gm_resid(View A, KState *S, GmSmall G, const double *__restrict__ b,
+                                                 const double *__restrict__ x, double *__restrict__ v1,
+                                                 double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                 int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double ax = row_dot(A, s, x);
+    const int i = out_row(A, s);
+    const double vi = radd(rmul(-1.0, ax), b[i]);
+    v1[i] = vi;
+    dd_add_prod(acc[0], vi, vi);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      const double rn = sqrt(dd_value(o[0]));
+      G.rs[0] = rn;
+      for (int k = 1; k < G.ld; k++) G.rs[k] = 0.0;
+      S->scal = 1.0 / rn;
+      S->errnum = rn;
+      S->errden = S->bn2;
+      if (S->errnum <= S->eps * S->errden || S->itx >= S->itmax) S->status = ST_DONE;
+      *ticket = 0;
+    }
+  }
+}
+
+// v_i = scal * src (src = v_1 for i = 1, else w) ; w1 = M^-1 v_i
+__global__ void __launch_bounds__(KT) k_gm_next(KState *S, int n, const double *src, double *vi,
+                                                const double *__restrict__ dinv, double *__restrict__ w1) {
+  if (stopped(S)) return;
+  const double scal = S->scal;
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    const double t = rmul(scal, src[i]);
+    vi[i] = t;
+    w1[i] = prec(dinv, i, t);
+  }
+}
+
+// w = A*w1 ; h(1,i) = (v_1, w)
+template <class View>
+__global__ void __launch_bounds__(KT) k_gm_spmv(View A, KState *S, GmSmall G, int i, const double *__restrict__ w1,
+                                                const double *__restrict__ v1, double *__restrict__ w,
+                                                double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double wi = row_dot(A, s, w1);
+    const int r = out_row(A, s);
+    w[r] = wi;
+    dd_add_prod(acc[0], ld_ro(v1 + r), wi);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      G.h[(size_t)(i - 1) * G.ld] = dd_value(o[0]);
+      *ticket = 0;
+    }
+  }
+}
+
+// MGS step k (2 <= k <= i): w = -h(k-1,i) v_{k-1} + w ; h(k,i) = (v_k, w)
+__global__ void __launch_bounds__(KT) k_gm_mgs(KState *S, GmSmall G, int i, int k, int n,
+                                               const double *__restrict__ vprev, const double *__restrict__ vk,
+                                               double *__restrict__ w, double *__restrict__ part,
+                                               unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  const double mh = -G.h[(k - 2) + (size_t)(i - 1) * G.ld];
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int j = blockIdx.x * KT + threadIdx.x; j < n; j += gridDim.x * KT) {
+    double wj = w[j];
+    if (mh != 0.0) {  // psi_daxpby reads nothing for alpha == 0
+      wj = radd(rmul(mh, vprev[j]), wj);
+      w[j] = wj;
+    }
+    dd_add_prod(acc[0], ld_ro(vk + j), wj);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      G.h[(k - 1) + (size_t)(i - 1) * G.ld] = dd_value(o[0]);
+      *ticket = 0;
+    }
+  }
+}
+
+// last MGS step: w = -h(i,i) v_i + w ; h(i+1,i) = ||w|| ; scal = 1/h(i+1,i);
+// rotations of column i, new rotation, rs update, stop test on |rs(i+1)|
+__global__ void __launch_bounds__(KT) k_gm_norm(KState *S, GmSmall G, int i, int nl, int n,
+                                                const double *__restrict__ vi, double *__restrict__ w,
+                                                double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  const int ld = G.ld;
+  const double mh = -G.h[(i - 1) + (size_t)(i - 1) * ld];
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int j = blockIdx.x * KT + threadIdx.x; j < n; j += gridDim.x * KT) {
+    double wj = w[j];
+    if (mh != 0.0) {
+      wj = radd(rmul(mh, vi[j]), wj);
+      w[j] = wj;
+    }
+    dd_add_prod(acc[0], wj, wj);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      double *hc = G.h + (size_t)(i - 1) * ld;  // column i
+      hc[i] = sqrt(dd_value(o[0]));
+      S->scal = 1.0 / hc[i];
+      for (int k = 2; k <= i; k++) drot1(hc[k - 2], hc[k - 1], G.c[k - 2], G.s[k - 2]);
+      double rti = hc[i - 1], rti1 = hc[i], tmp;
+      drotg(rti, rti1, tmp, G.s[i - 1]);
+      G.c[i - 1] = (double)(float)tmp;  // cmplx(tmp, dzero) without KIND: default precision
+      drot1(hc[i - 1], hc[i], G.c[i - 1], G.s[i - 1]);
+      hc[i] = 0.0;
+      drot1(G.rs[i - 1], G.rs[i], G.c[i - 1], G.s[i - 1]);
+      S->itx += 1;
+      S->errnum = fabs(G.rs[i]);
+      S->errden = S->bn2;
+      if (S->errnum <= S->eps * S->errden) {
+        S->gm_m = i;
+        S->gm_conv = 1;
+        S->status = ST_XUPD;
+      } else if (i == nl) {
+        S->gm_m = nl;
+        S->gm_conv = 0;
+        S->status = ST_XUPD;
+      }
+      *ticket = 0;
+    }
+  }
+}
+
+// rs(1:m) = H(1:m,1:m)^-1 rs(1:m)  (netlib dtrsm 'L','U','N','N', one column)
+__global__ void k_gm_trsm(KState *S, GmSmall G) {
+  if (threadIdx.x != 0 || *((volatile const int *)&S->status) != ST_XUPD) return;
+  const int m = S->gm_m, ld = G.ld;
+  for (int k = m - 1; k >= 0; k--) {
+    if (G.rs[k] != 0.0) {
+      G.rs[k] = G.rs[k] / G.h[k + (size_t)k * ld];
+      for (int i = 0; i < k; i++) G.rs[i] = radd(G.rs[i], -rmul(G.rs[k], G.h[i + (size_t)k * ld]));
+    }
+  }
+}
+
+// w1 = sum_k rs(k) v_k (k in order, from zero) ; x = M^-1 w1 + x ; then the
+// solve stops (converged) or the next cycle restarts
+__global__ void __launch_bounds__(KT) k_gm_xupd(KState *S, GmSmall G, int n, const double *__restrict__ V,
+                                                const double *__restrict__ dinv, double *__restrict__ x,
+                                                unsigned *__restrict__ ticket) {
+  if (*((volatile const int *)&S->status) != ST_XUPD) return;
+  const int m = S->gm_m;
+  for (int j = blockIdx.x * KT + threadIdx.x; j < n; j += gridDim.x * KT) {
+    double acc = 0.0;
+    for (int k = 0; k < m; k++) {
+      const double a = G.rs[k];
+      if (a != 0.0) acc = radd(rmul(a, V[(size_t)k * n + j]), acc);
+    }
+    x[j] = radd(prec(dinv, j, acc), x[j]);
+  }
+  if (psbx_last_block(ticket, gridDim.x)) {
+    if (threadIdx.x == 0) {
+      S->status = S->gm_conv ? ST_DONE : ST_RUN;
+      *ticket = 0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- prec build
 // psb_d_diag_precbld (prec/impl/psb_d_diagprec_impl.f90:229-292) with the
 // diagonal of psb_d_hll_get_diag (ext/impl/psb_d_hll_get_diag.f90:89-107):
@@ -664,16 +1034,217 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
   return rc;
 }
 
+// FCG driver: restart kernel on the host loop, then a graph of
+// KGRAPH_ITERS x (SpMV + dots | updates) replayed until the status changes.
+template <class View>
+static int solve_fcg(const View &A, const double *dinv, const double *b, double *x, int n, psbx_SolverOptions *opt) {
+  PsbxCtx &c = psbx_ctx();
+  cudaStream_t st = c.stream;
+  int grid = (n + KT - 1) / KT;
+  if (grid > c.sms * 8) grid = c.sms * 8;
+  if (grid < 1) grid = 1;
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  double *vec = nullptr, *part = nullptr;
+  KState *S = nullptr;
+  unsigned *ticket = nullptr;
+  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * 5 * nn, st));
+  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
+  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * 5 * nn, st));
+  KState *hS = (KState *)c.h_res;
+  KState init;
+  memset(&init, 0, sizeof(init));
+  init.eps = opt->eps;
+  init.itmax = opt->itmax;
+  init.istop = opt->istop;
+  init.status = ST_RUN;
+  PSBX_CK(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  double *v = vec, *w = vec + nn, *d = vec + 2 * nn, *q = vec + 3 * nn, *r = vec + 4 * nn;
+
+  k_kry_setup<<<grid, KT, 0, st>>>(n, b, S, part, ticket, grid);
+  psbx_count_launch();
+  if (opt->istop == 1) {
+    k_kry_normi<View><<<grid, KT, 0, st>>>(A, S, part, ticket, grid);
+    psbx_count_launch();
+  }
+  int rc = SPGPU_SUCCESS;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
+  if (!rc) {
+    for (int k = 0; k < KGRAPH_ITERS; k++) {
+      k_fcg_spmv<View><<<grid, KT, 0, st>>>(A, S, v, r, q, w, part, ticket, grid);
+      k_fcg_update<<<grid, KT, 0, st>>>(S, n, w, dinv, v, d, q, x, r, part, ticket, grid);
+    }
+    e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "EndCapture");
+  }
+  if (!rc) {
+    e = cudaGraphInstantiate(&gexec, graph, 0);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+  }
+  auto fetch = [&]() -> int {
+    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    return SPGPU_SUCCESS;
+  };
+  // restart loop of psb_dfcg.F90
+  while (!rc) {
+    k_fcg_init<View><<<grid, KT, 0, st>>>(A, S, b, x, dinv, r, v, part, ticket, grid);
+    psbx_count_launch();
+    if ((rc = fetch())) break;
+    if (hS->status == ST_DONE) break;
+    for (;;) {
+      e = cudaGraphLaunch(gexec, st);
+      if (e != cudaSuccess) {
+        rc = psbx_cuda_status(e, "GraphLaunch");
+        break;
+      }
+      psbx_count_launch(2 * KGRAPH_ITERS);
+      if ((rc = fetch())) break;
+      if (hS->status != ST_RUN) break;
+    }
+    if (rc || hS->status == ST_DONE) break;
+    // ST_BREAK (delta == 0): back to the restart, whose kernel resets the status
+  }
+  if (!rc) {
+    opt->iter = hS->itx;
+    opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(S, st);
+  cudaFreeAsync(ticket, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (!rc && e2 != cudaSuccess) rc = psbx_cuda_status(e2, "solve_fcg");
+  return rc;
+}
+
+// RGMRES driver (istop 2): one graph per restart cycle, replayed until the
+// status word says done.
+template <class View>
+static int solve_gmres(const View &A, const double *dinv, const double *b, double *x, int n,
+                       psbx_SolverOptions *opt) {
+  PsbxCtx &c = psbx_ctx();
+  cudaStream_t st = c.stream;
+  const int nl = opt->irst, ld = nl + 1;
+  int grid = (n + KT - 1) / KT;
+  if (grid > c.sms * 8) grid = c.sms * 8;
+  if (grid < 1) grid = 1;
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  double *vec = nullptr, *part = nullptr, *small = nullptr;
+  KState *S = nullptr;
+  unsigned *ticket = nullptr;
+  // V (ld vectors), w, w1
+  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * (size_t)(ld + 2) * nn, st));
+  PSBX_CK(cudaMallocAsync(&small, sizeof(double) * ((size_t)ld * ld + 3 * (size_t)ld), st));
+  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
+  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * (size_t)(ld + 2) * nn, st));
+  PSBX_CK(cudaMemsetAsync(small, 0, sizeof(double) * ((size_t)ld * ld + 3 * (size_t)ld), st));
+  KState *hS = (KState *)c.h_res;
+  KState init;
+  memset(&init, 0, sizeof(init));
+  init.eps = opt->eps;
+  init.itmax = opt->itmax;
+  init.istop = opt->istop;
+  init.status = ST_RUN;
+  PSBX_CK(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  GmSmall G;
+  G.ld = ld;
+  G.h = small;
+  G.c = small + (size_t)ld * ld;
+  G.s = G.c + ld;
+  G.rs = G.s + ld;
+  double *V = vec, *w = vec + (size_t)ld * nn, *w1 = w + nn;
+  auto Vk = [&](int k) { return V + (size_t)k * nn; };  // 0-based basis vector
+
+  k_kry_setup<<<grid, KT, 0, st>>>(n, b, S, part, ticket, grid);
+  psbx_count_launch();
+  int rc = SPGPU_SUCCESS, per_graph = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
+  if (!rc) {
+    k_gm_resid<View><<<grid, KT, 0, st>>>(A, S, G, b, x, Vk(0), part, ticket, grid);
+    per_graph++;
+    for (int i = 1; i <= nl; i++) {
+      k_gm_next<<<grid, KT, 0, st>>>(S, n, i == 1 ? Vk(0) : w, Vk(i - 1), dinv, w1);
+      k_gm_spmv<View><<<grid, KT, 0, st>>>(A, S, G, i, w1, Vk(0), w, part, ticket, grid);
+      for (int k = 2; k <= i; k++)
+        k_gm_mgs<<<grid, KT, 0, st>>>(S, G, i, k, n, Vk(k - 2), Vk(k - 1), w, part, ticket, grid);
+      k_gm_norm<<<grid, KT, 0, st>>>(S, G, i, nl, n, Vk(i - 1), w, part, ticket, grid);
+      per_graph += 3 + (i - 1);
+    }
+    k_gm_trsm<<<1, 32, 0, st>>>(S, G);
+    k_gm_xupd<<<grid, KT, 0, st>>>(S, G, n, V, dinv, x, ticket);
+    per_graph += 2;
+    e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "EndCapture");
+  }
+  if (!rc) {
+    e = cudaGraphInstantiate(&gexec, graph, 0);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+  }
+  while (!rc) {
+    e = cudaGraphLaunch(gexec, st);
+    if (e != cudaSuccess) {
+      rc = psbx_cuda_status(e, "GraphLaunch");
+      break;
+    }
+    psbx_count_launch(per_graph);
+    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    if (hS->status == ST_DONE) break;
+  }
+  if (!rc) {
+    opt->iter = hS->itx;
+    opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(small, st);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(S, st);
+  cudaFreeAsync(ticket, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (!rc && e2 != cudaSuccess) rc = psbx_cuda_status(e2, "solve_gmres");
+  return rc;
+}
+
+template <class View>
+static int run_method(int meth, const View &A, const double *dinv, const double *b, double *x, int n,
+                      psbx_SolverOptions *opt) {
+  if (meth == 2) return solve_fcg(A, dinv, b, x, n, opt);
+  if (meth == 3) return solve_gmres(A, dinv, b, x, n, opt);
+  return solve(A, meth == 1, dinv, b, x, n, opt);
+}
+
 extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, void *b, void *x,
                             psbx_SolverOptions *opt) {
   int rc = psbx_ensure_init();
   if (rc) return rc;
   if (!method || !mat || !b || !x || !opt) return SPGPU_UNSUPPORTED;
-  bool bicg;
-  if (!strcasecmp(method, "CG")) bicg = false;
-  else if (!strcasecmp(method, "BICGSTAB")) bicg = true;
+  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES (psb_dkrylov.f90:179-210)
+  int meth;
+  if (!strcasecmp(method, "CG")) meth = 0;
+  else if (!strcasecmp(method, "BICGSTAB")) meth = 1;
+  else if (!strcasecmp(method, "FCG")) meth = 2;
+  else if (!strcasecmp(method, "RGMRES") || !strcasecmp(method, "GMRES")) meth = 3;
   else return SPGPU_UNSUPPORTED;  // other methods are outside this library
   if (opt->istop < 1 || opt->istop > 3) return SPGPU_UNSUPPORTED;  // psb_err_invalid_istop_
+  // RGMRES: the reference accepts istop 1 and 2 (psb_drgmres.f90); istop 1
+  // is not provided here, and irst must be positive (psb_err_invalid_irst_)
+  if (meth == 3 && (opt->istop != 2 || opt->irst <= 0)) return SPGPU_UNSUPPORTED;
   MultiVectDevice *B = (MultiVectDevice *)b, *X = (MultiVectDevice *)x, *D = (MultiVectDevice *)dinv;
   const int n = mat_rows(mat, fmt);
   if (n < 0 || B->size_ < n || X->size_ < n || (D && D->size_ < n)) return SPGPU_UNSUPPORTED;
@@ -688,13 +1259,13 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
     HllDevice *m = (HllDevice *)mat;
     if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
     if (m->hackSize == 32)
-      return solve(hll32_view(hll_view(m)), bicg, dv, (const double *)B->v_, (double *)X->v_, n, opt);
-    return solve(hll_view(m), bicg, dv, (const double *)B->v_, (double *)X->v_, n, opt);
+      return run_method(meth, hll32_view(hll_view(m)), dv, (const double *)B->v_, (double *)X->v_, n, opt);
+    return run_method(meth, hll_view(m), dv, (const double *)B->v_, (double *)X->v_, n, opt);
   }
   if (fmt == PSBX_FMT_ELL)
-    return solve(ell_view((EllDevice *)mat), bicg, dv, (const double *)B->v_, (double *)X->v_, n, opt);
+    return run_method(meth, ell_view((EllDevice *)mat), dv, (const double *)B->v_, (double *)X->v_, n, opt);
   if (fmt == PSBX_FMT_CSR)
-    return solve(csr_view((CsrDevice *)((psbx_d_Cmat *)mat)->mat), bicg, dv, (const double *)B->v_,
-                 (double *)X->v_, n, opt);
+    return run_method(meth, csr_view((CsrDevice *)((psbx_d_Cmat *)mat)->mat), dv, (const double *)B->v_,
+                      (double *)X->v_, n, opt);
   return SPGPU_UNSUPPORTED;
 }

@@ -378,7 +378,8 @@ class DiagPrec:
 
 def psb_krylov(method, a, prec, b, x, eps=1e-6, itmax=1000, istop=2, itrace=0, irst=10):
     """psb_krylov(method, a, prec, b, x, eps, desc_a, info, itmax, iter, err,
-    itrace, irst, istop) for 'CG' and 'BICGSTAB', device-resident.
+    itrace, irst, istop) for 'CG', 'FCG', 'BICGSTAB' and 'RGMRES' (irst = restart
+    length), device-resident.
     Returns (iter, err); raises PsbxError on failure."""
     opt = L.SolverOptions()
     lib.psbx_DefaultSolverOptions(C.byref(opt))

@@ -1,5 +1,5 @@
 """GPU parity of the device-resident Krylov solvers against the oracle's
-restatement of psb_dcg / psb_dcgstab.
+restatement of psb_dcg / psb_dfcg / psb_dcgstab / psb_drgmres.
 
 Bar (from the reference's own behaviour): same stop test; iteration count
 within +-2 of the oracle's; final error estimate <= eps; the true residual
@@ -25,12 +25,12 @@ def _mats(psb, irp, ja, va, fmt):
     return psb.CsrMat(n, irp, ja, va)
 
 
-def _solve_both(psb, method, irp, ja, va, b, fmt="HLL", eps=1e-9, itmax=1000, istop=2, prec=True):
+def _solve_both(psb, method, irp, ja, va, b, fmt="HLL", eps=1e-9, itmax=1000, istop=2, prec=True, irst=10):
     n = len(irp) - 1
     A = _mats(psb, irp, ja, va, fmt)
     P = psb.DiagPrec("DIAG" if prec else "NONE").build(A)
     B, X = psb.DVect.bld(b), psb.DVect.bld(np.zeros(n))
-    it, err = psb.psb_krylov(method, A, P, B, X, eps=eps, itmax=itmax, istop=istop)
+    it, err = psb.psb_krylov(method, A, P, B, X, eps=eps, itmax=itmax, istop=istop, irst=irst)
     x = X.get_vect()
     dinv = None
     if prec:
@@ -38,7 +38,7 @@ def _solve_both(psb, method, irp, ja, va, b, fmt="HLL", eps=1e-9, itmax=1000, is
         h = O.hll_from_coo(n, ia, ja, va, 32)
         dinv = O.diag_prec_build(O.hll_get_diag(h, n))
         assert np.array_equal(P.dv.get_vect(), dinv)  # prec build is bit-exact
-    xo, ito, erro = O.krylov(method, irp, ja, va, b, dinv=dinv, eps=eps, itmax=itmax, istop=istop)
+    xo, ito, erro = O.krylov(method, irp, ja, va, b, dinv=dinv, eps=eps, itmax=itmax, istop=istop, irst=irst)
     return (x, it, err), (xo, ito, erro)
 
 
@@ -94,7 +94,7 @@ def test_cg_no_prec_and_itmax(psb):
 def test_zero_rhs_returns_at_once(psb):
     irp, ja, va = gen.poisson7(8)
     n = len(irp) - 1
-    for method in ("CG", "BICGSTAB"):
+    for method in ("CG", "BICGSTAB", "FCG", "RGMRES"):
         (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, np.zeros(n))
         assert np.all(x == 0)
         assert it == ito
@@ -106,6 +106,61 @@ def test_unknown_method_is_an_error(psb):
     A = _mats(psb, irp, ja, va, "HLL")
     from psblas3_b200._lib import PsbxError
     with pytest.raises(PsbxError):
-        psb.psb_krylov("GMRES", A, None, psb.DVect.bld(np.ones(n)), psb.DVect(n))
+        psb.psb_krylov("QMR", A, None, psb.DVect.bld(np.ones(n)), psb.DVect(n))
     with pytest.raises(PsbxError):
         psb.psb_krylov("CG", A, None, psb.DVect.bld(np.ones(n)), psb.DVect(n), istop=7)
+    # RGMRES: only istop 2 here; irst must be positive
+    for istop, irst in ((1, 10), (3, 10), (2, 0)):
+        with pytest.raises(PsbxError):
+            psb.psb_krylov("RGMRES", A, None, psb.DVect.bld(np.ones(n)), psb.DVect(n), istop=istop, irst=irst)
+
+
+@pytest.mark.parametrize("fmt", ["HLL", "ELL", "CSR"])
+@pytest.mark.parametrize("irst", [4, 10, 30])
+def test_rgmres_c1(psb, fmt, irst):
+    """RGMRES (psb_drgmres.f90) on the nonsymmetric C1 operator with DIAG:
+    iterations within +-2 of the oracle, the estimated and the true residual
+    at the tolerance, the solution close to the oracle's."""
+    irp, ja, va = gen.pde3d(20, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    b = O.csr_csmv(irp, ja, va, 1.0, np.ones(n), 0.0, np.zeros(n))
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "RGMRES", irp, ja, va, b, fmt=fmt, eps=1e-9, irst=irst)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-9 and erro <= 1e-9
+    r = b - gen.csr_matvec(irp, ja, va, x)
+    assert np.linalg.norm(r) <= 2e-9 * np.linalg.norm(b)
+    assert np.max(np.abs(x - xo)) <= 1e-6
+
+
+@pytest.mark.parametrize("istop", [1, 2, 3])
+@pytest.mark.parametrize("fmt", ["HLL", "CSR"])
+def test_fcg_spd(psb, istop, fmt):
+    """FCG (psb_dfcg.F90) on an SPD 7-point operator: iterations within +-2
+    of the oracle, error at the tolerance; FCG and CG agree on SPD input."""
+    irp, ja, va = gen.poisson7(22)
+    n = len(irp) - 1
+    b = np.random.default_rng(11).uniform(-1, 1, n)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "FCG", irp, ja, va, b, fmt=fmt, eps=1e-9, istop=istop)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-9
+    ia, _, _ = gen.csr_to_coo(irp, ja, va)
+    dinv = O.diag_prec_build(O.hll_get_diag(O.hll_from_coo(n, ia, ja, va, 32), n))
+    _, ito_cg, _ = O.krylov("CG", irp, ja, va, b, dinv=dinv, eps=1e-9, istop=istop)
+    assert abs(ito_cg - ito) <= 2, (ito_cg, ito)
+    r = b - gen.csr_matvec(irp, ja, va, x)
+    assert np.linalg.norm(r) <= 1e-6 * np.linalg.norm(b)
+
+
+def test_itmax_fcg_and_rgmres(psb):
+    """itmax: FCG stops at itmax; RGMRES tests itmax only at a restart, so
+    it finishes the running cycle (irst = 10 -> 10 iterations for itmax 7),
+    as the reference does."""
+    irp, ja, va = gen.poisson7(16)
+    n = len(irp) - 1
+    b = np.random.default_rng(5).uniform(-1, 1, n)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "FCG", irp, ja, va, b, eps=1e-14, itmax=7)
+    assert it == 7 and ito == 7 and err > 1e-14
+    assert abs(err - erro) <= 1e-6 * erro
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "RGMRES", irp, ja, va, b, eps=1e-14, itmax=7, irst=10)
+    assert it == 10 and ito == 10 and err > 1e-14
+    assert abs(err - erro) <= 1e-6 * erro

@@ -207,3 +207,37 @@ def test_oracle_itmax_and_zero_rhs():
     # b = 0 with x0 = 0: ||b|| = 0 so the test is ||r|| <= eps at once
     _, it, err = O.krylov("BICGSTAB", irp, ja, va, np.zeros(n), eps=1e-9, itmax=50)
     assert it == 0 and err == 0.0
+
+
+def test_oracle_fcg_and_rgmres():
+    """FCG equals CG on an SPD operator (same iterations, same error to a
+    few ulps of the tolerance); RGMRES converges on the nonsymmetric C1-type
+    operator with its estimated residual equal to the true one; the
+    restated drotg gives the rotation of (3, 4) to rounding."""
+    import ctypes as C
+    from psblas3_b200 import gen
+    irp, ja, va = gen.poisson7(12)
+    n = len(irp) - 1
+    b = np.random.default_rng(2).uniform(-1, 1, n)
+    ia, _, _ = gen.csr_to_coo(irp, ja, va)
+    dinv = O.diag_prec_build(O.hll_get_diag(O.hll_from_coo(n, ia, ja, va, 32), n))
+    _, it_cg, e_cg = O.krylov("CG", irp, ja, va, b, dinv=dinv, eps=1e-10)
+    x, it_f, e_f = O.krylov("FCG", irp, ja, va, b, dinv=dinv, eps=1e-10)
+    assert it_f == it_cg and abs(e_f - e_cg) <= 1e-3 * e_cg
+    irp, ja, va = gen.pde3d(10, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    b = O.csr_csmv(irp, ja, va, 1.0, np.ones(n), 0.0, np.zeros(n))
+    # the reference keeps the rotation cosines in single precision, so over
+    # long cycles its residual estimate drifts from the true residual; up to
+    # 30 steps per cycle they agree here
+    for irst in (3, 10, 30):
+        x, it, err = O.krylov("RGMRES", irp, ja, va, b, eps=1e-10, itmax=2000, irst=irst)
+        r = b - O.csr_csmv(irp, ja, va, 1.0, x, 0.0, np.zeros(n))
+        assert err <= 1e-10
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.5e-10
+    a, bb, c, s = (C.c_double(v) for v in (3.0, 4.0, 0.0, 0.0))
+    O.lib().or_drotg(C.byref(a), C.byref(bb), C.byref(c), C.byref(s))
+    assert np.allclose((a.value, c.value, s.value), (5.0, 0.6, 0.8), rtol=4e-16, atol=0)
+    assert abs(c.value ** 2 + s.value ** 2 - 1.0) <= 1e-15
+    with pytest.raises(ValueError):
+        O.krylov("RGMRES", irp, ja, va, b, istop=1)
