@@ -338,62 +338,67 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
         return {"gpu_ms": 1e3 * statistics.median(times[1:]), "iters": its, "err": err, "cpu_ms": 1e3 * tcpu,
                 "cpu_iters": ito, "cpu_err": erro, "cpu_threads": os.cpu_count()}
 
-    def c3_cg():
-        qi, qj, qv = gen.poisson7(256)
-        n3 = len(qi) - 1
-        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (qi, qj, qv))
-        A3 = psb.HllMat.from_csr_device(n3, n3, len(qj), d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
-        del d_irp, d_ja, d_va
-        P3 = psb.DiagPrec("DIAG").build(A3)
-        ustar = np.random.default_rng(0).uniform(0, 1, n3)
-        U, B3, X3 = psb.DVect.bld(ustar), psb.DVect(n3), psb.DVect(n3)
-        A3.spmv(1.0, U, 0.0, B3)
-        times = []
-        for _ in range(2):
-            X3.zero()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            it3, err3 = psb.psb_krylov("CG", A3, P3, B3, X3, eps=1e-10, itmax=20000)
-            times.append(time.perf_counter() - t0)
-        x64 = X3.get_vect()
-        res = {"rows": n3, "nnz": len(qj),
-               "fp64": {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "iters": it3, "err": err3,
-                        "max_abs_err_vs_ustar": float(np.max(np.abs(x64 - ustar)))}}
-        # mixed precision: FP32 inner CG, FP64-accumulated dots, FP64 refinement
-        A3.make_single()
-        eng = psb.BatchSolver(1, n3, 1)
-        dx = torch.zeros(n3, dtype=torch.float64, device="cuda")
-        db = torch.from_numpy(B3.get_vect()).cuda()
-        times = []
-        for _ in range(2):
-            dx.zero_()
-            s = eng.add(A3, db, dx, P3.dv.data_ptr, eps=1e-10)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            eng.run(replays_per_step=8)
-            times.append(time.perf_counter() - t0)
-            st, outer, its, err = eng.poll(s)
-            eng.remove(s)
-        xm = dx.cpu().numpy()
-        res["mixed"] = {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "inner_iters": its[0],
-                        "outer": outer, "converged": st == 1, "err": err[0],
-                        "max_abs_err_vs_ustar": float(np.max(np.abs(xm - ustar))),
-                        "max_abs_diff_vs_fp64_solve": float(np.max(np.abs(xm - x64)))}
-        res["mixed_speedup_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
-        eng.free()
-        A3.free()
-        return res
-
     _part(out, "c2a_formats", c2a_formats)
     _part(out, "c2b_powerlaw", c2b_powerlaw)
     _part(out, "c1_bicgstab", c1_bicgstab)
     if not args.skip_c3:
-        _part(out, "c3_cg", c3_cg)
+        _part(out, "c3_cg", lambda: c3_cg(psb, gen))
     if not args.skip_c4:
         _part(out, "c4_batched", lambda: c4_batched(psb, gen))
     if not args.skip_c5:
         _part(out, "c5_serving", lambda: c5_serving(psb, gen))
     return out
+
+
+def c3_cg(psb, gen):
+    """C3: SPD 7-point Poisson 256^3, b = A u* (u* uniform [0, 1]); plain FP64
+    device CG to 1e-10 beside the mixed-precision engine (FP32 inner CG,
+    FP64-accumulated dots, FP64 refinement) to the same FP64 tolerance."""
+    import torch
+    qi, qj, qv = gen.poisson7(256)
+    n3 = len(qi) - 1
+    d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (qi, qj, qv))
+    A3 = psb.HllMat.from_csr_device(n3, n3, len(qj), d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+    del d_irp, d_ja, d_va
+    P3 = psb.DiagPrec("DIAG").build(A3)
+    ustar = np.random.default_rng(0).uniform(0, 1, n3)
+    U, B3, X3 = psb.DVect.bld(ustar), psb.DVect(n3), psb.DVect(n3)
+    A3.spmv(1.0, U, 0.0, B3)
+    times = []
+    for _ in range(2):
+        X3.zero()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it3, err3 = psb.psb_krylov("CG", A3, P3, B3, X3, eps=1e-10, itmax=20000)
+        times.append(time.perf_counter() - t0)
+    x64 = X3.get_vect()
+    res = {"rows": n3, "nnz": len(qj),
+           "fp64": {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "iters": it3, "err": err3,
+                    "max_abs_err_vs_ustar": float(np.max(np.abs(x64 - ustar)))}}
+    # mixed precision: FP32 inner CG, FP64-accumulated dots, FP64 refinement
+    A3.make_single()
+    eng = psb.BatchSolver(1, n3, 1)
+    dx = torch.zeros(n3, dtype=torch.float64, device="cuda")
+    db = torch.from_numpy(B3.get_vect()).cuda()
+    times = []
+    for _ in range(2):
+        dx.zero_()
+        s = eng.add(A3, db, dx, P3.dv.data_ptr, eps=1e-10)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.run(replays_per_step=8)
+        times.append(time.perf_counter() - t0)
+        st, outer, its, err = eng.poll(s)
+        eng.remove(s)
+    xm = dx.cpu().numpy()
+    res["mixed"] = {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "inner_iters": its[0],
+                    "outer": outer, "converged": st == 1, "err": err[0],
+                    "max_abs_err_vs_ustar": float(np.max(np.abs(xm - ustar))),
+                    "max_abs_diff_vs_fp64_solve": float(np.max(np.abs(xm - x64)))}
+    res["mixed_speedup_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+    eng.free()
+    A3.free()
+    return res
 
 
 def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
@@ -644,11 +649,26 @@ def main():
     ap.add_argument("--skip-c3", action="store_true", help="skip the 256^3 CG solves among the secondaries")
     ap.add_argument("--skip-c4", action="store_true", help="skip the batched 512-system solve")
     ap.add_argument("--skip-c5", action="store_true", help="skip the serving stream")
+    ap.add_argument("--only", choices=["c3", "c4", "c5"], default=None,
+                    help="run one secondary workload alone on one GPU and print its result (profiling runs)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.only:
+        run_only(args.only)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
+
+
+def run_only(name):
+    """One secondary workload by itself (C3 CG solves, C4 batched, C5
+    serving) on cuda:0; prints {"only": name, "result": {...}}."""
+    import torch
+    from psblas3_b200 import gen, psb
+    psb.init(0)
+    torch.cuda.set_device(0)
+    fn = {"c3": c3_cg, "c4": c4_batched, "c5": c5_serving}[name]
+    print(json.dumps({"only": name, "result": fn(psb, gen)}), flush=True)
 
 
 if __name__ == "__main__":

@@ -99,9 +99,13 @@ struct Eng {
 // kernels want every warp slot (8 blocks, <= 32 registers); the update keeps
 // 4 rows of loads in flight per thread instead (4 blocks, no spills), which
 // measured faster than 1 row per thread at 8 blocks.  The 8-rhs kernels carry
-// 8 accumulators per row.
+// 8 accumulators per row; their SpMV runs 4 blocks per SM even though that
+// spills a few registers: on the 512 anisotropic systems 534 us, against
+// 672 us at 2 blocks, 712 us at 3, 655 us at 3 blocks with 4 entries per
+// load group, and 750-850 us when the 8 sums are formed as two halves of 4.
 template <int K> struct Occ {
   static constexpr int blocks = K == 1 ? 8 : 2;
+  static constexpr int spmv_blocks = K == 1 ? 8 : 4;
   static constexpr int update_blocks = K == 1 ? 4 : 2;
   static constexpr int resid_blocks = K == 1 ? 4 : 2;
 };
@@ -594,7 +598,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
 
 // PH_INNER: q = A32 p ; sigma = (p, q) ; alpha = rho / sigma.
 template <int K>
-__global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_spmv(const BSys *__restrict__ sys, BState *state,
+__global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *__restrict__ sys, BState *state,
                                                               BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
   int t0, t1;
