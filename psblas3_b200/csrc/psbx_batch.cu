@@ -73,6 +73,7 @@ struct BCtl {                 // read by every kernel at launch; lets the tile
   int ntiles, cap;            // table grow without re-capturing the graph
   const BTile *tiles;
   double *part;               // cap * 2*MAXK partial sums
+  int *count;                 // systems in each phase (kept by the kernels)
 };
 
 struct Eng {
@@ -82,6 +83,7 @@ struct Eng {
   BSol *d_sol = nullptr;
   BTile *d_tiles = nullptr;
   BCtl *d_ctl = nullptr;
+  int *d_count = nullptr;     // [8] systems per phase
   double *d_part = nullptr;   // max_tiles * K * 2
   std::vector<BSys> h_sys;
   std::vector<BState> h_state;
@@ -116,6 +118,23 @@ __device__ __forceinline__ void tile_range(int ntiles, int &t0, int &t1) {
   const long long per = ((long long)ntiles + gridDim.x - 1) / gridDim.x;
   t0 = (int)min((long long)ntiles, per * blockIdx.x);
   t1 = (int)min((long long)ntiles, per * (blockIdx.x + 1));
+}
+
+// A kernel whose phase no system is in returns after one load (instead of
+// walking the tile table); the finalisers move systems between phases and
+// keep the counts.
+// (one read by thread 0, shared with the block, so the block decides as one)
+__device__ __forceinline__ bool phase_idle(const BCtl *ctl, int ph) {
+  __shared__ int idle;
+  if (threadIdx.x == 0) idle = *((volatile const int *)ctl->count + ph) == 0;
+  __syncthreads();
+  return idle;
+}
+
+__device__ __forceinline__ void move_phase(const BCtl *ctl, BState *st, int to) {
+  atomicSub(ctl->count + st->phase, 1);
+  atomicAdd(ctl->count + to, 1);
+  st->phase = to;
 }
 
 struct RowRef {               // start of an HLL-32 row and its length
@@ -392,6 +411,7 @@ template <int K>
 __global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys *__restrict__ sys, BState *state,
                                                                      BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
+  if (phase_idle(ctl, PH_RESID)) return;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
@@ -446,7 +466,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys 
       if (threadIdx.x == 0) {
         int all = 1;
         for (int k = 0; k < K; k++) all &= sol[S.sol0 + k].done != 0;
-        st->phase = all ? PH_DONE : PH_INIT;
+        move_phase(ctl, st, all ? PH_DONE : PH_INIT);
         st->done_flag = all;
         st->ticket = 0;
       }
@@ -460,6 +480,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
                                                               BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 2 : 1;  // rows per thread whose loads are in flight together
   __shared__ double sm[32 * 2 * MAXK];
+  if (phase_idle(ctl, PH_INIT)) return;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
@@ -528,7 +549,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
       }
       __syncthreads();
       if (threadIdx.x == 0) {
-        st->phase = PH_INNER;
+        move_phase(ctl, st, PH_INNER);
         st->outer += 1;
         st->ticket = 0;
       }
@@ -541,6 +562,7 @@ template <int K>
 __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restrict__ sys, const BState *state,
                                                            const BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
+  if (phase_idle(ctl, PH_INNER)) return;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
@@ -601,6 +623,7 @@ template <int K>
 __global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *__restrict__ sys, BState *state,
                                                               BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
+  if (phase_idle(ctl, PH_INNER)) return;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
@@ -655,6 +678,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
                                                                 BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
   __shared__ double sm[32 * 2 * MAXK];
+  if (phase_idle(ctl, PH_INNER)) return;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
@@ -744,7 +768,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
       if (threadIdx.x == 0) {
         int any = 0;
         for (int k = 0; k < K; k++) any |= sol[S.sol0 + k].active;
-        if (!any) st->phase = PH_XUPD;
+        if (!any) move_phase(ctl, st, PH_XUPD);
         st->ticket = 0;
       }
     }
@@ -756,6 +780,7 @@ template <int K>
 __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__restrict__ sys, BState *state,
                                                               const BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
+  if (phase_idle(ctl, PH_XUPD)) return;
   int t0, t1;
   tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
@@ -804,10 +829,22 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__rest
     __syncthreads();
     if (last && threadIdx.x == 0) {
       __threadfence();
-      st->phase = PH_RESID;
+      move_phase(ctl, st, PH_RESID);
       st->ticket = 0;
     }
   }
+}
+
+// A slot joins (phase PH_RESID) or leaves (PH_IDLE) between replays: fresh
+// state, and the per-phase counts follow.  One thread.
+__global__ void kb_set_phase(BState *state, int *count, int slot, int phase) {
+  BState &b = state[slot];
+  if (b.phase != PH_IDLE) atomicSub(count + b.phase, 1);
+  b.phase = phase;
+  b.ticket = 0;
+  b.outer = 0;
+  b.done_flag = 0;
+  if (phase != PH_IDLE) atomicAdd(count + phase, 1);
 }
 
 __global__ void kb_d2f_inv(int n, const double *__restrict__ dinv, float *__restrict__ out) {
@@ -878,6 +915,7 @@ static int upload_tables(Eng *e, cudaStream_t st) {
   c.cap = e->max_tiles;
   c.tiles = e->d_tiles;
   c.part = e->d_part;
+  c.count = e->d_count;
   if (!tiles.empty())
     PSBX_CK(cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(BTile) * tiles.size(), cudaMemcpyHostToDevice, st));
   PSBX_CK(cudaMemcpyAsync(e->d_sys, e->h_sys.data(), sizeof(BSys) * e->max_sys, cudaMemcpyHostToDevice, st));
@@ -912,6 +950,8 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   if (err == cudaSuccess) err = cudaMalloc(&e->d_sol, sizeof(BSol) * max_systems * nrhs);
   if (err == cudaSuccess) err = cudaMalloc(&e->d_tiles, sizeof(BTile) * e->max_tiles);
   if (err == cudaSuccess) err = cudaMalloc(&e->d_ctl, sizeof(BCtl));
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_count, sizeof(int) * 8);
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->d_count, 0, sizeof(int) * 8, c.stream);
   if (err == cudaSuccess) err = cudaMalloc(&e->d_part, sizeof(double) * 2 * MAXK * (size_t)e->max_tiles);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_state_pinned, sizeof(BState) * max_systems, 0);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sol_pinned, sizeof(BSol) * max_systems * nrhs, 0);
@@ -1011,14 +1051,12 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
     so[k].outer_max = 64;
     so[k].first = 1;
   }
-  BState bs;
-  memset(&bs, 0, sizeof(bs));
-  bs.phase = PH_RESID;
   e->h_sys[s] = S;
   e->used[s] = 1;
   e->owned[s] = buf;
   PSBX_CK(cudaMemcpyAsync(e->d_sol + (size_t)s * K, so.data(), sizeof(BSol) * K, cudaMemcpyHostToDevice, c.stream));
-  PSBX_CK(cudaMemcpyAsync(e->d_state + s, &bs, sizeof(BState), cudaMemcpyHostToDevice, c.stream));
+  kb_set_phase<<<1, 1, 0, c.stream>>>(e->d_state, e->d_count, s, PH_RESID);
+  psbx_count_launch();
   int rc = upload_tables(e, c.stream);
   if (rc) return rc;
   *slot = s;
@@ -1076,9 +1114,8 @@ int psbx_batch_remove(void *eng, int slot) {
   Eng *e = (Eng *)eng;
   if (!e || slot < 0 || slot >= e->max_sys || !e->used[slot]) return SPGPU_UNSUPPORTED;
   PsbxCtx &c = psbx_ctx();
-  BState bs;
-  memset(&bs, 0, sizeof(bs));
-  PSBX_CK(cudaMemcpyAsync(e->d_state + slot, &bs, sizeof(BState), cudaMemcpyHostToDevice, c.stream));
+  kb_set_phase<<<1, 1, 0, c.stream>>>(e->d_state, e->d_count, slot, PH_IDLE);
+  psbx_count_launch();
   cudaFreeAsync(e->owned[slot], c.stream);
   e->owned[slot] = nullptr;
   e->used[slot] = 0;
@@ -1100,6 +1137,7 @@ int psbx_batch_destroy(void *eng) {
   cudaFree(e->d_sol);
   cudaFree(e->d_tiles);
   cudaFree(e->d_ctl);
+  cudaFree(e->d_count);
   cudaFree(e->d_part);
   cudaFreeHost(e->h_state_pinned);
   cudaFreeHost(e->h_sol_pinned);

@@ -917,6 +917,27 @@ extern "C" int psbx_diag_prec_build(void *mat, int fmt, void *dinv) {
 // ---------------------------------------------------------------- driver
 #define KGRAPH_ITERS 8
 
+// Replays a captured batch of iterations until running(status) is false,
+// with 1, 2, 4, then 8 replays between two reads of the status word: a long
+// solve pays one host round trip per 64 iterations, and the kernels of the
+// replays queued after the stop return at once (they test the status).
+template <class Pred>
+static int replay_until(cudaGraphExec_t gexec, cudaStream_t st, int per_graph, KState *S, KState *hS,
+                        Pred running) {
+  int batch = 1;
+  for (;;) {
+    for (int k = 0; k < batch; k++) {
+      cudaError_t e = cudaGraphLaunch(gexec, st);
+      if (e != cudaSuccess) return psbx_cuda_status(e, "GraphLaunch");
+      psbx_count_launch(per_graph);
+    }
+    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    if (!running(*hS)) return SPGPU_SUCCESS;
+    if (batch < 8) batch *= 2;
+  }
+}
+
 template <class View>
 static int solve(const View &A, bool bicg, const double *dinv, const double *b, double *x, int n,
                  psbx_SolverOptions *opt) {
@@ -1006,16 +1027,7 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     if (hS->status == ST_DONE) break;
     if (hS->status == ST_BREAK) continue;
     // iteration loop: replay the captured batch until the status changes
-    for (;;) {
-      e = cudaGraphLaunch(gexec, st);
-      if (e != cudaSuccess) {
-        rc = psbx_cuda_status(e, "GraphLaunch");
-        break;
-      }
-      psbx_count_launch(per_graph);
-      if ((rc = fetch())) break;
-      if (hS->status != ST_RUN) break;
-    }
+    rc = replay_until(gexec, st, per_graph, S, hS, [](const KState &k) { return k.status == ST_RUN; });
     if (rc || hS->status == ST_DONE) break;
     // ST_BREAK: back to the restart test
   }
@@ -1097,16 +1109,7 @@ static int solve_fcg(const View &A, const double *dinv, const double *b, double 
     psbx_count_launch();
     if ((rc = fetch())) break;
     if (hS->status == ST_DONE) break;
-    for (;;) {
-      e = cudaGraphLaunch(gexec, st);
-      if (e != cudaSuccess) {
-        rc = psbx_cuda_status(e, "GraphLaunch");
-        break;
-      }
-      psbx_count_launch(2 * KGRAPH_ITERS);
-      if ((rc = fetch())) break;
-      if (hS->status != ST_RUN) break;
-    }
+    rc = replay_until(gexec, st, 2 * KGRAPH_ITERS, S, hS, [](const KState &k) { return k.status == ST_RUN; });
     if (rc || hS->status == ST_DONE) break;
     // ST_BREAK (delta == 0): back to the restart, whose kernel resets the status
   }
@@ -1194,17 +1197,8 @@ static int solve_gmres(const View &A, const double *dinv, const double *b, doubl
     e = cudaGraphInstantiate(&gexec, graph, 0);
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
   }
-  while (!rc) {
-    e = cudaGraphLaunch(gexec, st);
-    if (e != cudaSuccess) {
-      rc = psbx_cuda_status(e, "GraphLaunch");
-      break;
-    }
-    psbx_count_launch(per_graph);
-    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
-    PSBX_CK(cudaStreamSynchronize(st));
-    if (hS->status == ST_DONE) break;
-  }
+  // each replay is one restart cycle; the solve ends when the status says done
+  if (!rc) rc = replay_until(gexec, st, per_graph, S, hS, [](const KState &k) { return k.status != ST_DONE; });
   if (!rc) {
     opt->iter = hS->itx;
     opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
