@@ -207,7 +207,55 @@ def run_reference(args):
                          "sample": f"{args.steps} steps x up to 10 full-matrix SpMVs (<= 4 s each)"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
+    g = gpu_reference_kernel(irp, ja, va, x, steps=max(args.steps, 10))
+    if g is not None:
+        line["gpu_reference_kernel"] = g
     print(json.dumps(line), flush=True)
+
+
+def gpu_reference_kernel(irp, ja, va, x, steps=20):
+    """The reference's own GPU HLL SpMV (SPGPU spgpuDhellspmv, compiled from
+    the psblas3 sources for sm_100a into oracle/_ref/) on the same matrix,
+    timed with CUDA events on its handle's stream; None when it is not built
+    or no GPU is present.  The HLL arrays come from the oracle's restatement
+    of the reference's CPU converter, so nothing of this library runs here."""
+    try:
+        import torch
+        import oracle as O
+    except ImportError:
+        return None
+    if not torch.cuda.is_available():
+        return None
+    ref = O.ref_gpu()
+    if ref is None:
+        return None
+    try:
+        n, nnz = len(irp) - 1, len(ja)
+        from psblas3_b200 import gen
+        ia, _, _ = gen.csr_to_coo(irp, ja, va)
+        h = O.hll_from_coo(n, ia, ja, va, 32)
+        dv = {k: torch.from_numpy(np.ascontiguousarray(h[k])).cuda() for k in ("val", "ja", "hkoffs", "irn")}
+        del h, ia
+        dx = torch.from_numpy(x).cuda()
+        dy = torch.zeros(n, dtype=torch.float64, device="cuda")
+        st = torch.cuda.ExternalStream(ref.stream)
+        args = (dy.data_ptr(), dy.data_ptr(), 1.0, dv["val"].data_ptr(), dv["ja"].data_ptr(), 32,
+                dv["hkoffs"].data_ptr(), dv["irn"].data_ptr(), -(-nnz // n), n, dx.data_ptr(), 0.0)
+        torch.cuda.synchronize()
+        for _ in range(3):
+            ref.hll_spmv(*args)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            ref.hll_spmv(*args)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        return {"value": algorithmic_bytes(n, nnz) / ms / 1e6, "unit": "GB/s", "ms_per_spmv": ms, "steps": steps,
+                "kernel": "spgpuDhellspmv (cuda/spgpu/kernels/hell_dspmv.cu) built for sm_100a, HLL hack 32"}
+    finally:
+        ref.close()
 
 
 def _time_spmv(mat, X, Y, steps, stream):

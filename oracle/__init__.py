@@ -7,6 +7,12 @@ and the CPU-baseline leg of ``bench.py`` may import it; the product library
 never calls it and has no CPU fallback.
 
 All index arrays are 1-based int32 like the reference Fortran; values FP64.
+
+``ref_gpu()`` loads the reference's own GPU HLL SpMV kernel (SPGPU
+``spgpuDhellspmv``), compiled from the psblas3 sources for sm_100a into
+``oracle/_ref/`` by ``make -C oracle ref``: a second, executed reference for
+the GPU SpMV (tests) and its timing beside the CPU path (bench.py's
+reference arm).
 """
 from __future__ import annotations
 
@@ -28,6 +34,62 @@ def build() -> str:
     """Compile liboracle.so with the committed Makefile (CPU only)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
+
+
+_REF_GPU_PATH = os.path.join(_HERE, "_ref", "libspgpu_hell.so")
+_REF_SRC = "/root/reference/cuda/spgpu/kernels/hell_dspmv.cu"
+
+
+def build_ref() -> bool:
+    """Compile the reference's SPGPU HLL SpMV into oracle/_ref/ when the
+    psblas3 sources are present (they are not on every machine)."""
+    if not os.path.exists(_REF_SRC):
+        return os.path.exists(_REF_GPU_PATH)
+    subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    return True
+
+
+class RefGpu:
+    """ctypes handle on spgpuCreate / spgpuDhellspmv / spgpuGetStream
+    (cuda/spgpu/core.h, cuda/spgpu/hell.h:74-107)."""
+
+    def __init__(self, path, device=0):
+        L = C.CDLL(path)
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        L.spgpuCreate.restype = I
+        L.spgpuCreate.argtypes = [C.POINTER(P), I]
+        L.spgpuDestroy.restype = None
+        L.spgpuDestroy.argtypes = [P]
+        L.spgpuGetStream.restype = P
+        L.spgpuGetStream.argtypes = [P]
+        L.spgpuDhellspmv.restype = None
+        L.spgpuDhellspmv.argtypes = [P, P, P, D, P, P, I, P, P, P, I, I, P, D, I]
+        self.L = L
+        self.h = P()
+        if L.spgpuCreate(C.byref(self.h), int(device)) != 0:
+            raise RuntimeError("spgpuCreate failed")
+
+    @property
+    def stream(self):
+        return self.L.spgpuGetStream(self.h)
+
+    def hll_spmv(self, z, y, alpha, cM, rP, hksz, hkoffs, rS, avg_nzr, rows, x, beta, base=1):
+        """z = alpha*A*x + beta*y exactly as spmvHllDeviceDouble calls it
+        (cuda/hlldev.c:185-207: no row permutation); device pointers (int)."""
+        self.L.spgpuDhellspmv(self.h, z, y, float(alpha), cM, rP, int(hksz), hkoffs, rS, None, int(avg_nzr),
+                              int(rows), x, float(beta), int(base))
+
+    def close(self):
+        if self.h:
+            self.L.spgpuDestroy(self.h)
+            self.h = C.c_void_p()
+
+
+def ref_gpu(device=0):
+    """The reference's GPU HLL SpMV, or None when oracle/_ref/ holds no build."""
+    if not os.path.exists(_REF_GPU_PATH):
+        return None
+    return RefGpu(_REF_GPU_PATH, device)
 
 
 def lib():
