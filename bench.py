@@ -210,7 +210,47 @@ def run_reference(args):
     g = gpu_reference_kernel(irp, ja, va, x, steps=max(args.steps, 10))
     if g is not None:
         line["gpu_reference_kernel"] = g
+        del irp, ja, va
+        line["gpu_reference_cg_c3"] = gpu_reference_cg_c3()
     print(json.dumps(line), flush=True)
+
+
+def gpu_reference_cg_c3():
+    """C3's plain FP64 CG (7-point Poisson 256^3, b = A u*, DIAG, 1e-10) on
+    the reference's own GPU kernels driven in psb_dcg's call sequence
+    (oracle/ref_cg.c): one kernel per PSBLAS call, dots and norms read back
+    to the host.  The matrix comes from the oracle's restatement of the
+    reference's CPU converter."""
+    import torch
+    import oracle as O
+    from psblas3_b200 import gen
+    ref = O.ref_gpu()
+    try:
+        irp, ja, va = gen.poisson7(256)
+        n, nnz = len(irp) - 1, len(ja)
+        ia, _, _ = gen.csr_to_coo(irp, ja, va)
+        h = O.hll_from_coo(n, ia, ja, va, 32)
+        dinv = O.diag_prec_build(O.hll_get_diag(h, n))
+        del ia
+        dv = {k: torch.from_numpy(np.ascontiguousarray(h[k])).cuda() for k in ("val", "ja", "hkoffs", "irn")}
+        del h
+        ustar = np.random.default_rng(0).uniform(0, 1, n)
+        d_b = torch.from_numpy(O.csr_csmv(irp, ja, va, 1.0, ustar, 0.0, np.zeros(n))).cuda()
+        d_dinv = torch.from_numpy(dinv).cuda()
+        d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ptrs = (dv["val"].data_ptr(), dv["ja"].data_ptr(), dv["hkoffs"].data_ptr(), dv["irn"].data_ptr())
+        ref.cg(n, *ptrs, -(-nnz // n), d_dinv.data_ptr(), d_b.data_ptr(), d_x.data_ptr(), 1e-10, 5)  # warm-up
+        d_x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, err = ref.cg(n, *ptrs, -(-nnz // n), d_dinv.data_ptr(), d_b.data_ptr(), d_x.data_ptr(), 1e-10, 20000)
+        t = time.perf_counter() - t0
+        xr = d_x.cpu().numpy()
+        return {"solve_ms": t * 1e3, "solves_per_s": 1.0 / t, "iters": it, "err": err,
+                "max_abs_err_vs_ustar": float(np.max(np.abs(xr - ustar))),
+                "path": "psb_dcg call sequence over SPGPU hell/dot/nrm2/axpby/maxypbz built for sm_100a"}
+    finally:
+        ref.close()
 
 
 def gpu_reference_kernel(irp, ja, va, x, steps=20):

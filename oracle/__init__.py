@@ -8,10 +8,11 @@ never calls it and has no CPU fallback.
 
 All index arrays are 1-based int32 like the reference Fortran; values FP64.
 
-``ref_gpu()`` loads the reference's own GPU HLL SpMV kernel (SPGPU
-``spgpuDhellspmv``), compiled from the psblas3 sources for sm_100a into
-``oracle/_ref/`` by ``make -C oracle ref``: a second, executed reference for
-the GPU SpMV (tests) and its timing beside the CPU path (bench.py's
+``ref_gpu()`` loads the reference's own GPU kernels (SPGPU HLL SpMV, dot,
+nrm2, axpby, diagonal product), compiled from the psblas3 sources for sm_100a
+into ``oracle/_ref/`` by ``make -C oracle ref``, with ``ref_cg.c`` driving
+them in psb_dcg's call sequence: a second, executed reference for the GPU
+SpMV (tests) and the reference's GPU timings beside the CPU path (bench.py's
 reference arm).
 """
 from __future__ import annotations
@@ -36,7 +37,7 @@ def build() -> str:
     return _LIB_PATH
 
 
-_REF_GPU_PATH = os.path.join(_HERE, "_ref", "libspgpu_hell.so")
+_REF_GPU_PATH = os.path.join(_HERE, "_ref", "libspgpu_ref.so")
 _REF_SRC = "/root/reference/cuda/spgpu/kernels/hell_dspmv.cu"
 
 
@@ -64,6 +65,8 @@ class RefGpu:
         L.spgpuGetStream.argtypes = [P]
         L.spgpuDhellspmv.restype = None
         L.spgpuDhellspmv.argtypes = [P, P, P, D, P, P, I, P, P, P, I, I, P, D, I]
+        L.refg_cg.restype = I
+        L.refg_cg.argtypes = [I, P, P, P, P, I, P, P, P, D, I, C.POINTER(I), C.POINTER(D)]
         self.L = L
         self.h = P()
         if L.spgpuCreate(C.byref(self.h), int(device)) != 0:
@@ -79,6 +82,16 @@ class RefGpu:
         self.L.spgpuDhellspmv(self.h, z, y, float(alpha), cM, rP, int(hksz), hkoffs, rS, None, int(avg_nzr),
                               int(rows), x, float(beta), int(base))
 
+    def cg(self, n, cM, rP, hkoffs, rS, avg_nzr, dinv, b, x, eps, itmax):
+        """psb_dcg on the reference's GPU kernels (ref_cg.c); device pointers
+        (int; dinv may be None); returns (iter, err)."""
+        it, err = C.c_int(0), C.c_double(0.0)
+        rc = self.L.refg_cg(int(n), cM, rP, hkoffs, rS, int(avg_nzr), dinv, b, x, float(eps), int(itmax),
+                            C.byref(it), C.byref(err))
+        if rc != 0:
+            raise RuntimeError(f"refg_cg failed rc={rc}")
+        return it.value, err.value
+
     def close(self):
         if self.h:
             self.L.spgpuDestroy(self.h)
@@ -86,7 +99,7 @@ class RefGpu:
 
 
 def ref_gpu(device=0):
-    """The reference's GPU HLL SpMV, or None when oracle/_ref/ holds no build."""
+    """The reference's GPU kernels, or None when oracle/_ref/ holds no build."""
     if not os.path.exists(_REF_GPU_PATH):
         return None
     return RefGpu(_REF_GPU_PATH, device)

@@ -58,3 +58,36 @@ def test_hll_spmv_matches_reference_gpu_kernel(psb, alpha, beta):
             assert np.array_equal(y, O.csr_csmv(irp, ja, va, alpha, x, beta, y0)), name
     finally:
         ref.close()
+
+
+def test_cg_matches_reference_gpu_path(psb):
+    """psb_dcg run on the reference's own GPU kernels (oracle/ref_cg.c over
+    SPGPU) and this library's device CG reach the same tolerance within +-2
+    iterations on an SPD 7-point operator with DIAG, and agree on x."""
+    import torch
+    ref = O.ref_gpu()
+    if ref is None:
+        pytest.skip("reference GPU kernels not built (psblas3 sources absent when building)")
+    try:
+        irp, ja, va = gen.poisson7(24)
+        n = len(irp) - 1
+        ia, _, _ = gen.csr_to_coo(irp, ja, va)
+        h = O.hll_from_coo(n, ia, ja, va, 32)
+        dinv = O.diag_prec_build(O.hll_get_diag(h, n))
+        b = np.random.default_rng(9).uniform(-1, 1, n)
+        dv = {k: torch.from_numpy(np.ascontiguousarray(h[k])).cuda() for k in ("val", "ja", "hkoffs", "irn")}
+        d_dinv, d_b = torch.from_numpy(dinv).cuda(), torch.from_numpy(b).cuda()
+        d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        it_ref, err_ref = ref.cg(n, dv["val"].data_ptr(), dv["ja"].data_ptr(), dv["hkoffs"].data_ptr(),
+                                 dv["irn"].data_ptr(), -(-len(ja) // n), d_dinv.data_ptr(), d_b.data_ptr(),
+                                 d_x.data_ptr(), 1e-9, 1000)
+        x_ref = d_x.cpu().numpy()
+        A = psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])
+        P = psb.DiagPrec("DIAG").build(A)
+        B, X = psb.DVect.bld(b), psb.DVect.bld(np.zeros(n))
+        it, err = psb.psb_krylov("CG", A, P, B, X, eps=1e-9, itmax=1000)
+        assert abs(it - it_ref) <= 2, (it, it_ref)
+        assert err <= 1e-9 and err_ref <= 1e-9
+        assert np.max(np.abs(X.get_vect() - x_ref)) <= 1e-7
+    finally:
+        ref.close()
