@@ -289,47 +289,153 @@ __global__ void k_hll_widths(int nr, int hksz, const int *__restrict__ irp, cons
   if (lane == 0) width[h] = mx;
 }
 
-// Single-block exclusive scan of width[0..n) * hksz into offs[0..n], 64-bit
-// accumulation; flags overflow of the int32 offsets the format uses.
-__global__ void k_scan_offsets(int n, int hksz, const int *__restrict__ width, int *__restrict__ offs,
-                               long long *__restrict__ total) {
-  __shared__ long long warp_tot[32];
-  __shared__ long long carry;
-  if (threadIdx.x == 0) carry = 0;
+// Hack offsets: exclusive scan of width[0..n) * hksz in 64-bit, in three
+// launches (chunk sums | scan of the chunk sums | chunk scans), plus the
+// widest hack.  SCAN_CHUNK = 256 threads x 16 hacks.
+enum { SCAN_T = 256, SCAN_PER = 16, SCAN_CHUNK = SCAN_T * SCAN_PER };
+
+__device__ __forceinline__ long long block_excl_scan(long long v, long long *sh /* [SCAN_T/32] */,
+                                                     long long &block_total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  long long incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) sh[wid] = incl;
   __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int base = 0; base < n; base += blockDim.x) {
-    const int i = base + threadIdx.x;
-    long long v = i < n ? (long long)width[i] * hksz : 0;
-    long long incl = v;
+  long long before = 0, tot = 0;
+  for (int w = 0; w < SCAN_T / 32; w++) {
+    if (w < wid) before += sh[w];
+    tot += sh[w];
+  }
+  __syncthreads();
+  block_total = tot;
+  return before + incl - v;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_chunks(int n, int hksz, const int *__restrict__ width,
+                                                        long long *__restrict__ csum, int *__restrict__ cmax) {
+  __shared__ long long sh[SCAN_T / 32];
+  const int i0 = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER;
+  long long s = 0;
+  int m = 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      long long t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) warp_tot[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-      long long t = lane < nw ? warp_tot[lane] : 0;
-      long long it = t;
+  for (int k = 0; k < SCAN_PER; k++) {
+    const int w = i0 + k < n ? width[i0 + k] : 0;
+    s += (long long)w * hksz;
+    m = max(m, w);
+  }
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        long long u = __shfl_up_sync(0xffffffffu, it, o);
-        if (lane >= o) it += u;
-      }
-      if (lane < nw) warp_tot[lane] = it - t;  // exclusive warp prefix
-    }
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  long long tot;
+  block_excl_scan(s, sh, tot);
+  if (threadIdx.x == 0) csum[blockIdx.x] = tot;
+  if ((threadIdx.x & 31) == 0) atomicMax(cmax + blockIdx.x, m);
+}
+
+// one block: exclusive scan of the nb chunk sums in place; total and widest
+// hack into res[0], res[1]
+__global__ void __launch_bounds__(SCAN_T) k_scan_top(int nb, long long *__restrict__ csum,
+                                                     const int *__restrict__ cmax, long long *__restrict__ res) {
+  __shared__ long long sh[SCAN_T / 32];
+  __shared__ long long carry;
+  __shared__ int mx;
+  if (threadIdx.x == 0) {
+    carry = 0;
+    mx = 0;
+  }
+  __syncthreads();
+  for (int b0 = 0; b0 < nb; b0 += SCAN_T) {
+    const int b = b0 + threadIdx.x;
+    const long long v = b < nb ? csum[b] : 0;
+    if (b < nb) atomicMax(&mx, cmax[b]);
+    long long tot;
+    const long long ex = block_excl_scan(v, sh, tot);
+    if (b < nb) csum[b] = carry + ex;
     __syncthreads();
-    const long long excl = carry + warp_tot[wid] + incl - v;
-    if (i < n) offs[i] = (int)excl;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    if (threadIdx.x == 0) carry += tot;
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    offs[n] = (int)carry;
-    *total = carry;
+    res[0] = carry;
+    res[1] = mx;
   }
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_apply(int n, int hksz, const int *__restrict__ width,
+                                                       const long long *__restrict__ csum, int *__restrict__ offs) {
+  __shared__ long long sh[SCAN_T / 32];
+  const int i0 = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER;
+  long long w[SCAN_PER];
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; k++) {
+    w[k] = i0 + k < n ? (long long)width[i0 + k] * hksz : 0;
+    s += w[k];
+  }
+  long long tot;
+  long long run = csum[blockIdx.x] + block_excl_scan(s, sh, tot);
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; k++) {
+    if (i0 + k < n) offs[i0 + k] = (int)run;
+    run += w[k];
+    if (i0 + k == n - 1) offs[n] = (int)run;
+  }
+}
+
+// HLL fill for hack size 32: one warp per hack, lane = row of the hack.  A
+// lane reads its row's start and length once and writes entry j of its row
+// at hkoffs + j*32 + lane (each j a coalesced 32-entry run); padding as
+// psi_d_xtr_ell_from_coo.f90:53-60 (the row's last column, or the hack's
+// first stored column for an empty row; ja = nr past the last row), idiag the
+// 1-based position of the diagonal or 0.
+__global__ void __launch_bounds__(256) k_hll_fill32(int nr, int base, const int *__restrict__ irp,
+                                                    const int *__restrict__ cja, const double *__restrict__ cval,
+                                                    const int *__restrict__ perm, const int *__restrict__ irn,
+                                                    const int *__restrict__ hkoffs, int nhacks,
+                                                    int *__restrict__ hja, double *__restrict__ hval,
+                                                    int *__restrict__ idiag) {
+  const int h = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (h >= nhacks) return;
+  const int off = hkoffs[h];
+  const int width = (hkoffs[h + 1] - off) >> 5;
+  const int s = h * 32 + lane;
+  const bool valid = s < nr;
+  const int r = valid ? (perm ? perm[s] : s) : 0;
+  const int len = valid ? irn[s] : 0;
+  const int p0 = valid ? irp[r] - base : 0;
+  // first stored column of the hack, needed only when one of its rows is empty
+  const unsigned full = __ballot_sync(0xffffffffu, valid && len > 0);
+  const unsigned rows = __ballot_sync(0xffffffffu, valid);
+  int first_col = nr;
+  if (full != rows && full != 0u) {
+    const int f = __ffs(full) - 1;
+    const int c0 = len > 0 ? cja[p0] : 0;
+    first_col = __shfl_sync(0xffffffffu, c0, f);
+  }
+  int diag = 0;
+  const int last = len > 0 ? cja[p0 + len - 1] : first_col;
+  for (int j = 0; j < width; j++) {
+    int col;
+    double v;
+    if (!valid) {
+      col = nr;
+      v = 0.0;
+    } else if (j < len) {
+      col = cja[p0 + j];
+      v = cval[p0 + j];
+      if (col == r + base) diag = j + 1;
+    } else {
+      col = last;
+      v = 0.0;
+    }
+    hja[(size_t)off + (size_t)j * 32 + lane] = col;
+    hval[(size_t)off + (size_t)j * 32 + lane] = v;
+  }
+  if (valid) idiag[s] = diag;
 }
 
 __global__ void k_hll_fill(int nr, int hksz, int base, const int *__restrict__ irp, const int *__restrict__ cja,
@@ -400,22 +506,29 @@ extern "C" int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, in
   if (!deviceMat || rows < 0 || hksz <= 0 || !d_irp) return SPGPU_UNSUPPORTED;
   PsbxCtx &c = psbx_ctx();
   const int nh = (rows + hksz - 1) / hksz;
-  int *width = nullptr, *irn = nullptr, *hk = nullptr;
-  long long *dtot = nullptr;
+  int *width = nullptr, *irn = nullptr, *hk = nullptr, *cmax = nullptr;
+  long long *dtot = nullptr, *csum = nullptr;
+  const int nb = (nh + SCAN_CHUNK - 1) / SCAN_CHUNK;
   rc = dmalloc((void **)&width, sizeof(int) * (size_t)(nh + 1));
   if (!rc) rc = dmalloc((void **)&irn, sizeof(int) * (size_t)(rows + 1));
   if (!rc) rc = dmalloc((void **)&hk, sizeof(int) * (size_t)(nh + 1));
-  if (!rc) rc = dmalloc((void **)&dtot, sizeof(long long));
-  long long total = 0;
+  if (!rc) rc = dmalloc((void **)&dtot, 2 * sizeof(long long));
+  if (!rc) rc = dmalloc((void **)&csum, sizeof(long long) * (size_t)(nb > 0 ? nb : 1));
+  if (!rc) rc = dmalloc((void **)&cmax, sizeof(int) * (size_t)(nb > 0 ? nb : 1));
+  long long res[2] = {0, 0};
   if (!rc && nh > 0) {
+    PSBX_CK(cudaMemsetAsync(cmax, 0, sizeof(int) * (size_t)nb, c.stream));
     k_hll_widths<<<(nh + 7) / 8, 256, 0, c.stream>>>(rows, hksz, d_irp, d_perm, irn, width, nh);
-    k_scan_offsets<<<1, 1024, 0, c.stream>>>(nh, hksz, width, hk, dtot);
-    psbx_count_launch(2);
+    k_scan_chunks<<<nb, SCAN_T, 0, c.stream>>>(nh, hksz, width, csum, cmax);
+    k_scan_top<<<1, SCAN_T, 0, c.stream>>>(nb, csum, cmax, dtot);
+    k_scan_apply<<<nb, SCAN_T, 0, c.stream>>>(nh, hksz, width, csum, hk);
+    psbx_count_launch(4);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "hll widths/scan");
-    if (!rc) rc = d2h(&total, dtot, sizeof(long long));
+    if (!rc) rc = d2h(res, dtot, 2 * sizeof(long long));
     if (!rc) rc = sync_stream();
   }
+  const long long total = res[0];
   if (!rc && total > 0x7fffffffLL) rc = SPGPU_UNSUPPORTED;  // int32 offsets, as psb_ipk_
   HllDevice *m = nullptr;
   if (!rc) rc = FallocHllDevice((void **)&m, (unsigned)hksz, (unsigned)rows, (unsigned)nnz, (unsigned)total,
@@ -435,26 +548,27 @@ extern "C" int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, in
     }
   }
   if (!rc && nh > 0) {
-    k_zero_int<<<psbx_grid_for(rows, 256), 256, 0, c.stream>>>(rows, m->diag);
-    k_hll_fill<<<nh, 256, 0, c.stream>>>(rows, hksz, 1, d_irp, d_ja, d_val, m->perm, m->rS, m->hackOffs, m->rP,
-                                        (double *)m->cM, m->diag);
-    psbx_count_launch(2);
+    if (hksz == 32) {
+      k_hll_fill32<<<(nh + 7) / 8, 256, 0, c.stream>>>(rows, 1, d_irp, d_ja, d_val, m->perm, m->rS, m->hackOffs, nh,
+                                                       m->rP, (double *)m->cM, m->diag);
+      psbx_count_launch(1);
+    } else {
+      k_zero_int<<<psbx_grid_for(rows, 256), 256, 0, c.stream>>>(rows, m->diag);
+      k_hll_fill<<<nh, 256, 0, c.stream>>>(rows, hksz, 1, d_irp, d_ja, d_val, m->perm, m->rS, m->hackOffs, m->rP,
+                                          (double *)m->cM, m->diag);
+      psbx_count_launch(2);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "k_hll_fill");
   }
-  if (!rc) {
-    // longest row, for the solver's choice of kernels
-    std::vector<int> hw(nh > 0 ? nh : 1);
-    if (nh > 0) rc = d2h(hw.data(), width, sizeof(int) * (size_t)nh);
-    if (!rc) rc = sync_stream();
-    int mx = 0;
-    for (int h = 0; h < nh; h++) mx = hw[h] > mx ? hw[h] : mx;
-    if (m) m->maxRowLen = mx;
-  }
+  // longest row (the widest hack), for the solver's choice of kernels
+  if (!rc && m) m->maxRowLen = (int)res[1];
   cudaFree(width);
   cudaFree(irn);
   cudaFree(hk);
   cudaFree(dtot);
+  cudaFree(csum);
+  cudaFree(cmax);
   if (rc) {
     if (m) freeHllDevice(m);
     *deviceMat = nullptr;

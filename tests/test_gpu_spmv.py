@@ -100,6 +100,64 @@ def test_device_hll_build_matches_cpu_converter(psb):
         assert np.all(g["idiag"][~has] == 0)
 
 
+def _drop_rows(irp, ja, va, rows):
+    """CSR with the entries of `rows` (0-based) removed (empty rows)."""
+    keep = np.ones(len(ja), bool)
+    for r in rows:
+        keep[irp[r] - 1:irp[r + 1] - 1] = False
+    cnt = np.diff(irp).copy()
+    cnt[rows] = 0
+    nirp = np.concatenate([[1], 1 + np.cumsum(cnt)]).astype(np.int32)
+    return nirp, ja[keep].copy(), va[keep].copy()
+
+
+def _permute_rows(irp, ja, va, perm):
+    cnt = np.diff(irp)[perm]
+    nirp = np.concatenate([[1], 1 + np.cumsum(cnt)]).astype(np.int32)
+    idx = np.concatenate([np.arange(irp[r] - 1, irp[r + 1] - 1) for r in perm])
+    return nirp, ja[idx].copy(), va[idx].copy()
+
+
+def test_device_hll_build_large_empty_rows_and_perm(psb):
+    """The device build over more than one scan chunk (4,394 hacks), with
+    empty rows (padding from the hack's first stored column, including hacks
+    whose first rows are empty) and with a row permutation (hack rows taken
+    in perm order == the CPU converter on the row-permuted matrix)."""
+    import torch
+    irp, ja, va = gen.pde3d(52)
+    n = len(irp) - 1
+    rng = np.random.default_rng(12)
+    empty = np.unique(np.concatenate([rng.choice(n, n // 20, replace=False), np.arange(64, 70), [n - 1]]))
+    irp, ja, va = _drop_rows(irp, ja, va, empty)
+    for perm in (None, rng.permutation(n).astype(np.int32)):
+        if perm is None:
+            h = _host_hll(irp, ja, va)
+        else:
+            h = _host_hll(*_permute_rows(irp, ja, va, perm))
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        d_perm = None if perm is None else torch.from_numpy(perm).cuda()
+        A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32,
+                                       None if d_perm is None else d_perm.data_ptr())
+        g = A.read()
+        assert np.array_equal(g["hkoffs"], h["hkoffs"])
+        assert np.array_equal(g["irn"], h["irn"])
+        assert np.array_equal(g["ja"], h["ja"])
+        assert np.array_equal(g["val"].view(np.uint64), h["val"].view(np.uint64))
+        if perm is None:
+            want = np.where(h["idiag"] > 0, h["idiag"], 0)
+        else:  # idiag points at the diagonal of the original row held in each slot
+            want = np.zeros(n, np.int32)
+            for slot, r in enumerate(perm):
+                pos = np.nonzero(ja[irp[r] - 1:irp[r + 1] - 1] == r + 1)[0]
+                want[slot] = pos[0] + 1 if len(pos) else 0
+        assert np.array_equal(g["idiag"], want)
+        # and the SpMV through the permuted layout gives y in the original row order
+        x = rng.uniform(-1, 1, n)
+        X, Y = psb.DVect.bld(x), psb.DVect(n)
+        A.spmv(1.0, X, 0.0, Y)
+        assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, 1.0, x, 0.0, np.zeros(n)))
+
+
 def test_psi_copy_coo_to_hlg(psb):
     """GPU conversion variant (psi_cuda_CopyCooToHlg.cuh): same offsets, row
     lengths, stored entries and diagonal positions as the CPU converter;
