@@ -29,6 +29,7 @@
 #define SPMV_T 256
 #define CSR_TILE 2048
 #define CSR_ROWS 256
+static_assert(CSR_TILE % SPMV_T == 0, "a CSR row block is a whole number of passes of the block");
 
 HllView hll_view(const HllDevice *m) {
   HllView v;
@@ -158,10 +159,21 @@ __device__ __forceinline__ void csr_stream_block(const CsrView &A, const int *__
   const int e0 = ld_ro(A.irp + r0) - A.base, e1 = ld_ro(A.irp + r1) - A.base;
   const int ne = e1 - e0;
   const double *xb = x - A.base;
-  for (int k = threadIdx.x; k < ne; k += SPMV_T) {
-    const int c = ld_stream(A.ja + e0 + k);
-    const double v = ld_stream(A.val + e0 + k);
-    prod[k] = rmul(v, ld_ro(xb + c));
+  // all of a thread's index and value loads first, then its gathers (a block
+  // holds at most CSR_TILE = CSR_U * SPMV_T entries)
+  constexpr int CSR_U = CSR_TILE / SPMV_T;
+  int c[CSR_U];
+  double v[CSR_U];
+#pragma unroll
+  for (int u = 0; u < CSR_U; u++) {
+    const int k = threadIdx.x + u * SPMV_T;
+    c[u] = k < ne ? ld_stream(A.ja + e0 + k) : A.base;
+    v[u] = k < ne ? ld_stream(A.val + e0 + k) : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < CSR_U; u++) {
+    const int k = threadIdx.x + u * SPMV_T;
+    if (k < ne) prod[k] = rmul(v[u], ld_ro(xb + c[u]));
   }
   __syncthreads();
   const int r = r0 + threadIdx.x;
