@@ -394,6 +394,19 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
         short = lens <= 2048
         res["csr_equals_hll_on_short_rows"] = bool(np.array_equal(yh[short], y_csr[short]))
         H.free()
+        # HLL holding the rows in decreasing-length order through a row
+        # permutation (y comes back in the original order): hacks of similar
+        # rows, the wide ones summed by a block each
+        order = np.argsort(-lens, kind="stable").astype(np.int32)
+        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
+        d_perm = torch.from_numpy(order).cuda()
+        H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32,
+                                       d_perm.data_ptr())
+        del d_irp, d_ja, d_va, d_perm
+        ms = _time_spmv(H, X2, Y2, steps, stream)
+        res["hll_row_sorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2,
+                                 "bitexact_vs_unsorted_hll": bool(np.array_equal(Y2.get_vect(), yh))}
+        H.free()
         return res
 
     def c1_bicgstab():
@@ -543,11 +556,15 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
     for i, j in pairs:
         irp, ja, va, rhs, A, P, db, dx = mats[i]
         B, X = psb.DVect.bld(rhs[:, j]), psb.DVect(len(irp) - 1)
-        X.zero()
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        it, err = psb.psb_krylov("CG", A, P, B, X, eps=1e-10, itmax=100000)
-        t64 += time.perf_counter() - t1
+        best = None
+        for _ in range(2):  # best of two: the baseline at its fastest
+            X.zero()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            it, err = psb.psb_krylov("CG", A, P, B, X, eps=1e-10, itmax=100000)
+            dt = time.perf_counter() - t1
+            best = dt if best is None else min(best, dt)
+        t64 += best
         it64.append(it)
     solves = n_sys * k
     return {"systems": n_sys, "rhs_per_system": k, "rows_total": total, "batched_s": tb,
@@ -559,14 +576,15 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
             "speedup_vs_fp64_one_at_a_time": (solves / tb) / (len(pairs) / t64)}
 
 
-def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0, fp64_sample=16):
+def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0):
     """C5: Poisson arrivals (rate per second, for `window` seconds) of solve
     requests drawn 50/50 from 3-D 7-point Poisson grids (side uniform in
     [10, 128]) and power-law unstructured SPD matrices (rows log-uniform in
     [1e3, 2e6], alpha 2.1, diagonally dominant), one seeded right-hand side
     each, FP64 tolerance 1e-10, admitted by a 150 GB HBM budget into the
     continuous-batching server; the matrices stay resident in a device pool.
-    Beside it: the plain FP64 device CG one request at a time on a sample."""
+    Beside it: the plain FP64 device CG one request at a time over the same
+    request mix (one timed solve per pool matrix, weighted by its requests)."""
     import torch
     import oracle as O
     from psblas3_b200 import serve
@@ -610,22 +628,38 @@ def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0, fp64_samp
         res = O.csr_csmv(irp, ja, va, -1.0, r.x, 1.0, b)
         worst = max(worst, np.linalg.norm(res) / np.linalg.norm(b))
     srv.close()
-    # plain FP64 GPU path, one request at a time
-    t64, sample = 0.0, done[:: max(1, len(done) // fp64_sample)][:fp64_sample]
-    for r in sample:
-        m = pool.mats[r.mat]
+    # plain FP64 GPU path, one request at a time, over the same mix: one timed
+    # solve per pool matrix (the first request naming it; best of two),
+    # weighted by how many requests of the stream name that matrix
+    counts = {}
+    first = {}
+    for r in sorted(done, key=lambda q: q.rid):
+        counts[r.mat] = counts.get(r.mat, 0) + 1
+        first.setdefault(r.mat, r)
+    t64, per_mat = 0.0, {}
+    for mi, r in sorted(first.items()):
+        m = pool.mats[mi]
         b = serve.request_rhs(r, m["n"]).cpu().numpy()
         B, X = psb.DVect.bld(b), psb.DVect(m["n"])
-        X.zero()
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        psb.psb_krylov("CG", m["A"], m["P"], B, X, eps=1e-10, itmax=100000)
-        t64 += time.perf_counter() - t1
+        best = None
+        for _ in range(2):
+            X.zero()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            psb.psb_krylov("CG", m["A"], m["P"], B, X, eps=1e-10, itmax=100000)
+            dt = time.perf_counter() - t1
+            best = dt if best is None else min(best, dt)
+        per_mat[mi] = best
+        t64 += best * counts[mi]
     out = {"arrival_rate_per_s": rate, "window_s": window, "requests": len(reqs), "completed": len(done),
            "converged": ok, "wall_s": wall, "solves_per_s": len(done) / wall, "latency": stats,
            "host_checked_max_relres": worst, "pool_matrices": len(pool.mats),
            "pool_rows": [m["n"] for m in pool.mats], "kernel_launches": int(launches),
-           "fp64_one_at_a_time_solves_per_s": len(sample) / t64 if t64 else None, "fp64_sample": len(sample)}
+           "fp64_one_at_a_time_solves_per_s": len(done) / t64 if t64 else None,
+           "fp64_method": "one timed FP64 CG per pool matrix (best of 2) x its request count",
+           "fp64_ms_per_matrix": {str(k): round(v * 1e3, 3) for k, v in per_mat.items()}}
+    if t64:
+        out["speedup_vs_fp64_one_at_a_time"] = out["solves_per_s"] / out["fp64_one_at_a_time_solves_per_s"]
     for m in pool.mats:
         m["A"].free()
     return out

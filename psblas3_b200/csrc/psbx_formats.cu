@@ -91,6 +91,8 @@ void freeHllDevice(void *deviceMat) {
   cudaFree(m->cM);
   if (m->cM32) cudaFree(m->cM32);
   if (m->perm) cudaFree(m->perm);
+  cudaFree(m->longHacks);
+  cudaFree(m->lres);
   free(m);
 }
 
@@ -124,6 +126,7 @@ static int hll_copy(void *deviceMat, void *val, int *ja, int *hkoffs, int *irn, 
       for (size_t i = 0; i < nr; i++) mx = irn[i] > mx ? irn[i] : mx;
       m->maxRowLen = mx;
     }
+    if (!rc) rc = psbx_hll_index_long(m);
   } else {
     rc = d2h(val, m->cM, as * vsize(type));
     if (!rc) rc = d2h(ja, m->rP, as * sizeof(int));
@@ -255,6 +258,7 @@ extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int no
     m->maxRowLen = mx;
   }
   if (!rc) rc = sync_stream();
+  if (!rc) rc = psbx_hll_index_long(m);
   cudaFree(dIdisp);
   cudaFree(dJa);
   cudaFree(dVal);
@@ -563,6 +567,7 @@ extern "C" int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, in
   }
   // longest row (the widest hack), for the solver's choice of kernels
   if (!rc && m) m->maxRowLen = (int)res[1];
+  if (!rc && m) rc = psbx_hll_index_long(m);
   cudaFree(width);
   cudaFree(irn);
   cudaFree(hk);

@@ -42,7 +42,16 @@ struct HllDevice {
   float *cM32;       // optional FP32 copy of FP64 values (mixed precision)
   int *perm;         // optional storage-row -> matrix-row map (NULL: identity)
   int maxRowLen;     // longest stored row (-1: unknown)
+  // hacks wider than PSBX_LONG_W (hack size 32 only): their row sums are
+  // formed by a block per hack before each product (psbx_hll_long_rows) and
+  // read back from lres by the row kernels
+  int *longHacks;    // hack ids, nLong of them
+  int nLong;
+  double *lres;      // rows entries (storage order), allocated when nLong > 0
 };
+
+// A hack of 32 rows whose width exceeds this is summed by a whole block.
+#define PSBX_LONG_W 256
 
 struct EllDevice {
   void *cM;
@@ -343,6 +352,9 @@ struct HllView {
   const int *hkoffs;
   const int *perm;   // storage row -> matrix row (NULL identity)
   int rows, hksz, base;
+  const int *longHacks;  // hack size 32: hacks wider than PSBX_LONG_W
+  const double *lres;    // their row sums, formed before the row kernel runs
+  int nLong;
 };
 
 struct HllViewF {  // FP32 values, FP32 x
@@ -410,7 +422,11 @@ __device__ __forceinline__ double row_acc(const VT *__restrict__ vp, const int *
 }
 
 __device__ __forceinline__ double row_dot(const Hll32View &A, int s, const double *__restrict__ x) {
-  const int off = ld_ro(A.hkoffs + (s >> 5)) + (s & 31);
+  const int h0 = ld_ro(A.hkoffs + (s >> 5));
+  // a row of a wide hack was summed (same order, same roundings) by the
+  // long-row kernel launched just before with the same x
+  if (A.nLong && ((ld_ro(A.hkoffs + (s >> 5) + 1) - h0) >> 5) > PSBX_LONG_W) return __ldcg(A.lres + s);
+  const int off = h0 + (s & 31);
   return row_acc<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base);
 }
 
@@ -467,10 +483,22 @@ __device__ __forceinline__ int out_row(const EllView &, int r) { return r; }
 __device__ __forceinline__ int out_row(const CsrView &, int r) { return r; }
 
 HllView hll_view(const HllDevice *m);
+// Finds the wide hacks of a hack-32 matrix after its arrays are written.
+int psbx_hll_index_long(HllDevice *m);
+// Row sums of the wide hacks of a hack-32 matrix into lres, to be launched
+// before any row kernel that reads them with the same x; status (nullable)
+// makes it return at once when *status != 0.
+int psbx_long_rows32(const Hll32View &A, const double *x, const int *status, cudaStream_t st);
 static inline Hll32View hll32_view(const HllView &v) {
   Hll32View w;
   static_cast<HllView &>(w) = v;
   return w;
+}
+
+template <class View>
+static inline int psbx_long_rows(const View &, const double *, const int *, cudaStream_t) { return 0; }
+static inline int psbx_long_rows(const Hll32View &A, const double *x, const int *status, cudaStream_t st) {
+  return A.nLong ? psbx_long_rows32(A, x, status, st) : 0;
 }
 EllView ell_view(const EllDevice *m);
 CsrView csr_view(const CsrDevice *m);

@@ -917,6 +917,11 @@ extern "C" int psbx_diag_prec_build(void *mat, int fmt, void *dinv) {
 // ---------------------------------------------------------------- driver
 #define KGRAPH_ITERS 8
 
+// 1 when the matrix has wide hacks, whose rows a separate kernel sums before
+// each product (psbx_long_rows); 0 otherwise.
+template <class View> static inline int long_launch(const View &) { return 0; }
+static inline int long_launch(const Hll32View &A) { return A.nLong > 0 ? 1 : 0; }
+
 // Replays a captured batch of iterations until running(status) is false,
 // with 1, 2, 4, then 8 replays between two reads of the status word: a long
 // solve pays one host round trip per 64 iterations, and the kernels of the
@@ -989,12 +994,15 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     for (int k = 0; k < KGRAPH_ITERS; k++) {
       if (!bicg) {
         k_cg_p<<<grid, KT, 0, st>>>(S, n, v3, v0);
+        psbx_long_rows(A, v0, &S->status, st);
         k_cg_spmv<View><<<grid, KT, 0, st>>>(A, S, v0, v1, part, ticket, grid);
         k_cg_update<<<grid, KT, 0, st>>>(S, n, v0, v1, dinv, x, v2, v3, part, ticket, grid);
       } else {
         k_bcg_p<<<grid, KT, 0, st>>>(S, n, v1, v3, dinv, v2, v7);
+        psbx_long_rows(A, v7, &S->status, st);
         k_bcg_spmv1<View><<<grid, KT, 0, st>>>(A, S, v7, v0, v3, part, ticket, grid);
         k_bcg_s<<<grid, KT, 0, st>>>(S, n, v1, v3, dinv, v4, v6);
+        psbx_long_rows(A, v6, &S->status, st);
         k_bcg_spmv2<View><<<grid, KT, 0, st>>>(A, S, v6, v4, v5, part, ticket, grid);
         k_bcg_update<<<grid, KT, 0, st>>>(S, n, v7, v6, v4, v5, v0, x, v1, part, ticket, grid);
       }
@@ -1006,7 +1014,7 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     e = cudaGraphInstantiate(&gexec, graph, 0);
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
   }
-  const int per_graph = KGRAPH_ITERS * (bicg ? 5 : 3);
+  const int per_graph = KGRAPH_ITERS * ((bicg ? 5 : 3) + (bicg ? 2 : 1) * long_launch(A));
 
   auto fetch = [&]() -> int {
     PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
@@ -1018,11 +1026,12 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
   // restart loop (psb_dcg.F90:218-225 / psb_dcgstab.f90:226-237)
   while (!rc) {
     if (hS->itx >= opt->itmax) break;
+    if ((rc = psbx_long_rows(A, x, nullptr, st))) break;
     if (!bicg)
       k_cg_init<View><<<grid, KT, 0, st>>>(A, S, b, x, dinv, v2, v3, part, ticket, grid);
     else
       k_bcg_init<View><<<grid, KT, 0, st>>>(A, S, b, x, v1, v0, part, ticket, grid);
-    psbx_count_launch();
+    psbx_count_launch(1 + long_launch(A));
     if ((rc = fetch())) break;
     if (hS->status == ST_DONE) break;
     if (hS->status == ST_BREAK) continue;
@@ -1088,6 +1097,7 @@ static int solve_fcg(const View &A, const double *dinv, const double *b, double 
   if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
   if (!rc) {
     for (int k = 0; k < KGRAPH_ITERS; k++) {
+      psbx_long_rows(A, v, &S->status, st);
       k_fcg_spmv<View><<<grid, KT, 0, st>>>(A, S, v, r, q, w, part, ticket, grid);
       k_fcg_update<<<grid, KT, 0, st>>>(S, n, w, dinv, v, d, q, x, r, part, ticket, grid);
     }
@@ -1105,11 +1115,13 @@ static int solve_fcg(const View &A, const double *dinv, const double *b, double 
   };
   // restart loop of psb_dfcg.F90
   while (!rc) {
+    if ((rc = psbx_long_rows(A, x, nullptr, st))) break;
     k_fcg_init<View><<<grid, KT, 0, st>>>(A, S, b, x, dinv, r, v, part, ticket, grid);
-    psbx_count_launch();
+    psbx_count_launch(1 + long_launch(A));
     if ((rc = fetch())) break;
     if (hS->status == ST_DONE) break;
-    rc = replay_until(gexec, st, 2 * KGRAPH_ITERS, S, hS, [](const KState &k) { return k.status == ST_RUN; });
+    rc = replay_until(gexec, st, (2 + long_launch(A)) * KGRAPH_ITERS, S, hS,
+                      [](const KState &k) { return k.status == ST_RUN; });
     if (rc || hS->status == ST_DONE) break;
     // ST_BREAK (delta == 0): back to the restart, whose kernel resets the status
   }
@@ -1177,15 +1189,17 @@ static int solve_gmres(const View &A, const double *dinv, const double *b, doubl
   cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
   if (!rc) {
+    psbx_long_rows(A, x, &S->status, st);
     k_gm_resid<View><<<grid, KT, 0, st>>>(A, S, G, b, x, Vk(0), part, ticket, grid);
-    per_graph++;
+    per_graph += 1 + long_launch(A);
     for (int i = 1; i <= nl; i++) {
       k_gm_next<<<grid, KT, 0, st>>>(S, n, i == 1 ? Vk(0) : w, Vk(i - 1), dinv, w1);
+      psbx_long_rows(A, w1, &S->status, st);
       k_gm_spmv<View><<<grid, KT, 0, st>>>(A, S, G, i, w1, Vk(0), w, part, ticket, grid);
       for (int k = 2; k <= i; k++)
         k_gm_mgs<<<grid, KT, 0, st>>>(S, G, i, k, n, Vk(k - 2), Vk(k - 1), w, part, ticket, grid);
       k_gm_norm<<<grid, KT, 0, st>>>(S, G, i, nl, n, Vk(i - 1), w, part, ticket, grid);
-      per_graph += 3 + (i - 1);
+      per_graph += 3 + (i - 1) + long_launch(A);
     }
     k_gm_trsm<<<1, 32, 0, st>>>(S, G);
     k_gm_xupd<<<grid, KT, 0, st>>>(S, G, n, V, dinv, x, ticket);

@@ -41,7 +41,95 @@ HllView hll_view(const HllDevice *m) {
   v.rows = m->rows;
   v.hksz = m->hackSize;
   v.base = m->baseIndex;
+  const bool wide = m->hackSize == 32 && m->nLong > 0;
+  v.longHacks = wide ? m->longHacks : nullptr;
+  v.lres = wide ? m->lres : nullptr;
+  v.nLong = wide ? m->nLong : 0;
   return v;
+}
+
+// --------------------------------------------------------------- wide hacks
+// A hack whose width exceeds PSBX_LONG_W would hold its warp for thousands
+// of dependent steps (the tail of a row-sorted power-law matrix).  One block
+// per such hack: in chunks of LONG_CH entries per row, all 256 threads load
+// the chunk's values and indices (entry j of the 32 rows is one contiguous
+// run) and form the products in shared memory, then lane r of warp 0 adds
+// row r's products in entry order from 0 -- the same roundings as the
+// thread-per-row sum, so results are unchanged bit for bit.
+#define LONG_CH 128
+__global__ void __launch_bounds__(256) k_hll_long(Hll32View A, const double *__restrict__ x,
+                                                  double *__restrict__ lres, const int *status) {
+  if (status && *((volatile const int *)status) != 0) return;
+  __shared__ double prod[LONG_CH * 32];
+  __shared__ int len[32];
+  const int h = A.longHacks[blockIdx.x];
+  const int off = A.hkoffs[h];
+  const int width = (A.hkoffs[h + 1] - off) >> 5;
+  const int s = h * 32 + (threadIdx.x & 31);
+  if (threadIdx.x < 32) len[threadIdx.x] = s < A.rows ? A.irn[s] : 0;
+  __syncthreads();
+  const double *xb = x - A.base;
+  double acc = 0.0;
+  constexpr int PER = LONG_CH * 32 / 256;  // products per thread per chunk
+  for (int c0 = 0; c0 < width; c0 += LONG_CH) {
+    int c[PER];
+    double v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int idx = threadIdx.x + u * 256;
+      const int j = c0 + (idx >> 5), r = idx & 31;
+      const bool ok = j < len[r];
+      const size_t p = (size_t)off + (size_t)j * 32 + r;
+      c[u] = ok ? ld_stream(A.ja + p) : A.base;
+      v[u] = ok ? ld_stream(A.val + p) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int idx = threadIdx.x + u * 256;
+      if (c0 + (idx >> 5) < len[idx & 31]) prod[idx] = rmul(v[u], ld_ro(xb + c[u]));
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int n = min(LONG_CH, len[threadIdx.x] - c0);
+      for (int k = 0; k < n; k++) acc = radd(acc, prod[k * 32 + threadIdx.x]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 32 && s < A.rows) lres[s] = acc;
+}
+
+int psbx_long_rows32(const Hll32View &A, const double *x, const int *status, cudaStream_t st) {
+  if (A.nLong <= 0) return SPGPU_SUCCESS;
+  k_hll_long<<<A.nLong, 256, 0, st>>>(A, x, const_cast<double *>(A.lres), status);
+  PSBX_LAUNCH_CK("k_hll_long");
+  return SPGPU_SUCCESS;
+}
+
+// Lists the hacks wider than PSBX_LONG_W (hack size 32) from the offsets and
+// allocates their row-sum buffer; called whenever an HLL object's arrays are
+// (re)written.
+int psbx_hll_index_long(HllDevice *m) {
+  cudaFree(m->longHacks);
+  cudaFree(m->lres);
+  m->longHacks = nullptr;
+  m->lres = nullptr;
+  m->nLong = 0;
+  if (m->hackSize != 32 || m->rows <= 0 || !m->hackOffs) return SPGPU_SUCCESS;
+  const int nh = (m->rows + 31) / 32;
+  PsbxCtx &c = psbx_ctx();
+  std::vector<int> hk((size_t)nh + 1);
+  PSBX_CK(cudaMemcpyAsync(hk.data(), m->hackOffs, sizeof(int) * ((size_t)nh + 1), cudaMemcpyDeviceToHost, c.stream));
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  std::vector<int> wide;
+  for (int h = 0; h < nh; h++)
+    if (((hk[h + 1] - hk[h]) >> 5) > PSBX_LONG_W) wide.push_back(h);
+  if (wide.empty()) return SPGPU_SUCCESS;
+  PSBX_CK(cudaMalloc(&m->longHacks, sizeof(int) * wide.size()));
+  PSBX_CK(cudaMalloc(&m->lres, sizeof(double) * (size_t)m->rows));
+  PSBX_CK(cudaMemcpyAsync(m->longHacks, wide.data(), sizeof(int) * wide.size(), cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  m->nLong = (int)wide.size();
+  return SPGPU_SUCCESS;
 }
 
 EllView ell_view(const EllDevice *m) {
@@ -93,6 +181,8 @@ template <class View>
 static int launch_rows(const View &A, double alpha, const double *x, double beta, double *y, cudaStream_t st) {
   if (A.rows <= 0) return SPGPU_SUCCESS;
   if (alpha == 0.0) return psbx_launch_scale(A.rows, beta, y, st);
+  int rc = psbx_long_rows(A, x, nullptr, st);
+  if (rc) return rc;
   const int g = (A.rows + SPMV_T - 1) / SPMV_T;
   if (beta == 0.0)
     k_spmv_rows<View, 1><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);

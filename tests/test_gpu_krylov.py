@@ -164,3 +164,19 @@ def test_itmax_fcg_and_rgmres(psb):
     (x, it, err), (xo, ito, erro) = _solve_both(psb, "RGMRES", irp, ja, va, b, eps=1e-14, itmax=7, irst=10)
     assert it == 10 and ito == 10 and err > 1e-14
     assert abs(err - erro) <= 1e-6 * erro
+
+
+@pytest.mark.parametrize("method", ["CG", "FCG", "BICGSTAB", "RGMRES"])
+def test_wide_hacks_in_solvers(psb, method):
+    """Row-sorted SPD power-law matrix whose leading hacks are wider than 256
+    (summed by a block each before every product): every method matches the
+    oracle's iteration count within +-2 and reaches the tolerance."""
+    irp, ja, va = gen.powerlaw_spd(40000, kmax=3000, seed=8)
+    irp, ja, va, _ = gen.sort_rows_by_length(irp, ja, va)
+    n = len(irp) - 1
+    b = np.random.default_rng(6).uniform(-1, 1, n)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, b, eps=1e-10, itmax=2000)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-10
+    r = b - gen.csr_matvec(irp, ja, va, x)
+    assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(b)

@@ -354,3 +354,35 @@ def test_distributed_parts_on_device(psb):
     glob = O.csr_csmv(irp, ja, va, alpha, x, beta, y0)
     scale = O.csr_csmv(irp, ja, np.abs(va), abs(alpha), np.abs(x), abs(beta), np.abs(y0))
     assert np.all(np.abs(y_all - glob) <= TOL * scale)
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0), (2.5, -0.5)])
+def test_hll_wide_hacks_bitexact(psb, alpha, beta):
+    """Row-sorted power-law matrix (rows up to 4,000 entries at the front):
+    hacks wider than 256 are summed by a block each, in entry order, so the
+    HLL SpMV stays bit-identical to the CPU csmv; host-written, device-built
+    and permuted (perm = the length order) layouts alike."""
+    import torch
+    irp, ja, va = gen.powerlaw(60000, kmax=4000, seed=21)
+    sirp, sja, sva, order = gen.sort_rows_by_length(irp, ja, va)
+    n = len(irp) - 1
+    rng = np.random.default_rng(4)
+    x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    h = _host_hll(sirp, sja, sva)
+    assert np.any(np.diff(h["hkoffs"]) // 32 > 256)
+    mats = [psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"])]
+    d = [torch.from_numpy(a).cuda() for a in (sirp, sja, sva)]
+    mats.append(psb.HllMat.from_csr_device(n, n, len(sja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32))
+    want = O.csr_csmv(sirp, sja, sva, alpha, x, beta, y0)
+    for A in mats:
+        X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+        A.spmv(alpha, X, beta, Y)
+        assert np.array_equal(Y.get_vect(), want)
+    # the unsorted matrix stored in length order through a permutation
+    e = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+    d_perm = torch.from_numpy(np.ascontiguousarray(order, dtype=np.int32)).cuda()
+    P = psb.HllMat.from_csr_device(n, n, len(ja), e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(), 32,
+                                   d_perm.data_ptr())
+    X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+    P.spmv(alpha, X, beta, Y)
+    assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, alpha, x, beta, y0))
