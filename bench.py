@@ -370,6 +370,14 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
         ms = _time_spmv(Cm, X, Y, steps, stream)
         res["csr"] = {"gb_s": B / ms / 1e6, "ms": ms, "bitexact_vs_hll": bool(np.array_equal(Y.get_vect(), y_ref))}
         Cm.free()
+        # autotuned HLL layout (hack size and wide-hack threshold)
+        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (irp, ja, va))
+        T, info = psb.HllMat.autotune_from_csr_device(n, n, nnz, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr())
+        del d_irp, d_ja, d_va
+        ms = _time_spmv(T, X, Y, steps, stream)
+        res["hll_autotuned"] = dict(info, gb_s=B / ms / 1e6, ms=ms,
+                                    bitexact_vs_hll=bool(np.array_equal(Y.get_vect(), y_ref)))
+        T.free()
         return res
 
     def c2b_powerlaw():
@@ -407,6 +415,15 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
         res["hll_row_sorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2,
                                  "bitexact_vs_unsorted_hll": bool(np.array_equal(Y2.get_vect(), yh))}
         H.free()
+        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
+        d_perm = torch.from_numpy(order).cuda()
+        T, info = psb.HllMat.autotune_from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(),
+                                                      d_va.data_ptr(), d_perm.data_ptr())
+        del d_irp, d_ja, d_va, d_perm
+        ms = _time_spmv(T, X2, Y2, steps, stream)
+        res["hll_row_sorted_autotuned"] = dict(info, gb_s=B2 / ms / 1e6, ms=ms,
+                                               bitexact_vs_unsorted_hll=bool(np.array_equal(Y2.get_vect(), yh)))
+        T.free()
         return res
 
     def c1_bicgstab():

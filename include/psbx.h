@@ -281,6 +281,21 @@ int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, int nnz,
                              const int *d_irp, const int *d_ja,
                              const double *d_val, int hksz, const int *d_perm);
 
+/* Autotuned device CSR -> HLL (the "autotuned hack size and threads per
+ * row" of the GPU HLL SpMV; the reference fixes hksz = 32,
+ * psb_d_cuda_cp_hlg_from_coo.F90:60): builds each candidate layout -- hack
+ * size 32, 64 or 128 and, for hack size 32, the width above which a hack's
+ * 32 rows are summed by a block of 256 threads (128, 256, 512, 1024 or
+ * never) -- times its SpMV on the library stream and keeps the fastest.
+ * All candidates sum every row in stored order, so the products are the
+ * same bits; *hksz, *wide_w (-1 never, 0 not applicable) and *ms (one SpMV)
+ * describe the choice.  Arguments otherwise as psbx_hll_from_csr_device. */
+int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int cols,
+                                      int nnz, const int *d_irp,
+                                      const int *d_ja, const double *d_val,
+                                      const int *d_perm, int *hksz,
+                                      int *wide_w, double *ms);
+
 /* Adds an FP32 copy of the values of an FP64 HLL handle (for the FP32 inner
  * iterations of the mixed-precision solver). */
 int psbx_hll_make_single(void *deviceMat);

@@ -89,6 +89,7 @@ _SIGS = {
     "psbx_dkrylov": (I, [CH, P, I, P, P, P, C.POINTER(SolverOptions)]),
     "psbx_diag_prec_build": (I, [P, I, P]),
     "psbx_hll_from_csr_device": (I, [PP, I, I, I, P, P, P, I, P]),
+    "psbx_hll_autotune_from_csr_device": (I, [PP, I, I, I, P, P, P, P, PI, PI, PD]),
     "psbx_hll_make_single": (I, [P]),
     "psbx_wrapMultiVecDevice": (I, [PP, P, U, U]), "psbx_multivec_data": (P, [P]),
     "psbx_hll_spmv_raw": (I, [P, D, P, D, P]),

@@ -896,3 +896,98 @@ int d_spmvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX, double beta,
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ HLL autotune
+// Builds the HLL form of a device CSR matrix for each candidate layout and
+// keeps the one with the fastest SpMV (CUDA events on the library stream,
+// 2 warm-up and 5 timed products with x = 0): hack size 32, 64 or 128 and,
+// for hack size 32, the width above which a hack's rows are summed by a
+// whole block (threads per row 8 instead of 1): 128, 256, 512, 1024 or never.
+// Every candidate sums each row in stored order, so all give the same bits;
+// the choice changes time only.
+static int cst(cudaError_t e, const char *where) { return e == cudaSuccess ? 0 : psbx_cuda_status(e, where); }
+
+static int time_hll(HllDevice *m, const double *x, double *y, double *ms) {
+  PsbxCtx &c = psbx_ctx();
+  cudaEvent_t e0, e1;
+  PSBX_CK(cudaEventCreate(&e0));
+  PSBX_CK(cudaEventCreate(&e1));
+  int rc = SPGPU_SUCCESS;
+  for (int k = 0; k < 2 && !rc; k++) rc = psbx_launch_hll_spmv(m, 1.0, x, 0.0, y, c.stream);
+  if (!rc) rc = cst(cudaEventRecord(e0, c.stream), "autotune");
+  for (int k = 0; k < 5 && !rc; k++) rc = psbx_launch_hll_spmv(m, 1.0, x, 0.0, y, c.stream);
+  if (!rc) rc = cst(cudaEventRecord(e1, c.stream), "autotune");
+  if (!rc) rc = cst(cudaEventSynchronize(e1), "autotune");
+  float t = 0.0f;
+  if (!rc) rc = cst(cudaEventElapsedTime(&t, e0, e1), "autotune");
+  *ms = t / 5.0;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int cols, int nnz, const int *d_irp,
+                                                 const int *d_ja, const double *d_val, const int *d_perm,
+                                                 int *hksz, int *wide_w, double *ms) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!deviceMat || rows <= 0 || !d_irp) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  double *x = nullptr, *y = nullptr;
+  rc = dmalloc((void **)&x, sizeof(double) * (size_t)(cols > rows ? cols : rows));
+  if (!rc) rc = dmalloc((void **)&y, sizeof(double) * (size_t)rows);
+  if (!rc) rc = cst(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)(cols > rows ? cols : rows), c.stream),
+                    "autotune");
+  HllDevice *best = nullptr;
+  double best_ms = 0.0;
+  int best_w = 0;
+  static const int hks[] = {32, 64, 128};
+  static const int ws[] = {128, 256, 512, 1024, -1};
+  for (int hi = 0; hi < 3 && !rc; hi++) {
+    HllDevice *m = nullptr;
+    rc = psbx_hll_from_csr_device((void **)&m, rows, cols, nnz, d_irp, d_ja, d_val, hks[hi], d_perm);
+    if (rc) break;
+    const int nw = hks[hi] == 32 ? 5 : 1;
+    int m_best_w = 0;
+    double m_best = -1.0;
+    for (int wi = 0; wi < nw && !rc; wi++) {
+      if (hks[hi] == 32) {
+        // thresholds at or above the longest row leave nothing to sum by blocks
+        if (ws[wi] > 0 && m->maxRowLen >= 0 && ws[wi] >= m->maxRowLen && wi + 1 < nw) continue;
+        m->longW = ws[wi];
+        rc = psbx_hll_index_long(m);
+        if (rc) break;
+      }
+      double t = 0.0;
+      rc = time_hll(m, x, y, &t);
+      if (!rc && (m_best < 0.0 || t < m_best)) {
+        m_best = t;
+        m_best_w = hks[hi] == 32 ? ws[wi] : 0;
+      }
+    }
+    if (!rc && (!best || m_best < best_ms)) {
+      if (best) freeHllDevice(best);
+      best = m;
+      best_ms = m_best;
+      best_w = m_best_w;
+    } else {
+      freeHllDevice(m);
+    }
+  }
+  if (!rc && best && best->hackSize == 32) {
+    best->longW = best_w;
+    rc = psbx_hll_index_long(best);
+  }
+  cudaFree(x);
+  cudaFree(y);
+  if (rc) {
+    if (best) freeHllDevice(best);
+    *deviceMat = nullptr;
+    return rc;
+  }
+  *deviceMat = best;
+  if (hksz) *hksz = best->hackSize;
+  if (wide_w) *wide_w = best->hackSize == 32 ? best_w : 0;
+  if (ms) *ms = best_ms;
+  return SPGPU_SUCCESS;
+}

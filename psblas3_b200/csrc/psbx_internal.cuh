@@ -42,15 +42,16 @@ struct HllDevice {
   float *cM32;       // optional FP32 copy of FP64 values (mixed precision)
   int *perm;         // optional storage-row -> matrix-row map (NULL: identity)
   int maxRowLen;     // longest stored row (-1: unknown)
-  // hacks wider than PSBX_LONG_W (hack size 32 only): their row sums are
-  // formed by a block per hack before each product (psbx_hll_long_rows) and
-  // read back from lres by the row kernels
+  // hacks wider than longW (hack size 32 only): their row sums are formed by
+  // a block per hack before each product (psbx_long_rows32) and read back
+  // from lres by the row kernels
   int *longHacks;    // hack ids, nLong of them
   int nLong;
   double *lres;      // rows entries (storage order), allocated when nLong > 0
+  int longW;         // 0: PSBX_LONG_W; < 0: never
 };
 
-// A hack of 32 rows whose width exceeds this is summed by a whole block.
+// Default width above which a hack of 32 rows is summed by a whole block.
 #define PSBX_LONG_W 256
 
 struct EllDevice {
@@ -352,9 +353,9 @@ struct HllView {
   const int *hkoffs;
   const int *perm;   // storage row -> matrix row (NULL identity)
   int rows, hksz, base;
-  const int *longHacks;  // hack size 32: hacks wider than PSBX_LONG_W
+  const int *longHacks;  // hack size 32: hacks wider than longW
   const double *lres;    // their row sums, formed before the row kernel runs
-  int nLong;
+  int nLong, longW;
 };
 
 struct HllViewF {  // FP32 values, FP32 x
@@ -384,6 +385,10 @@ struct CsrView {
 // psb_d_cuda_cp_hlg_from_coo.F90:60): hack and lane come from shifts and the
 // entry stride is a compile-time constant.
 struct Hll32View : HllView {};
+// Hack size 32 with wide hacks (nLong > 0): their rows' sums are read back
+// from lres (a separate type, so the kernels of matrices without wide hacks
+// carry no test for them).
+struct Hll32WView : HllView {};
 
 // Unrolled in-order accumulation over one row whose j-th entry sits at
 // vp[j*stride] / jp[j*stride] (32-bit offsets: every format keeps its
@@ -422,10 +427,15 @@ __device__ __forceinline__ double row_acc(const VT *__restrict__ vp, const int *
 }
 
 __device__ __forceinline__ double row_dot(const Hll32View &A, int s, const double *__restrict__ x) {
+  const int off = ld_ro(A.hkoffs + (s >> 5)) + (s & 31);
+  return row_acc<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base);
+}
+
+__device__ __forceinline__ double row_dot(const Hll32WView &A, int s, const double *__restrict__ x) {
   const int h0 = ld_ro(A.hkoffs + (s >> 5));
   // a row of a wide hack was summed (same order, same roundings) by the
   // long-row kernel launched just before with the same x
-  if (A.nLong && ((ld_ro(A.hkoffs + (s >> 5) + 1) - h0) >> 5) > PSBX_LONG_W) return __ldcg(A.lres + s);
+  if (((ld_ro(A.hkoffs + (s >> 5) + 1) - h0) >> 5) > A.longW) return __ldcg(A.lres + s);
   const int off = h0 + (s & 31);
   return row_acc<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base);
 }
@@ -458,6 +468,9 @@ __device__ __forceinline__ double row_abs_sum(const HllView &A, int s);
 __device__ __forceinline__ double row_abs_sum(const Hll32View &A, int s) {
   return row_abs_sum(static_cast<const HllView &>(A), s);
 }
+__device__ __forceinline__ double row_abs_sum(const Hll32WView &A, int s) {
+  return row_abs_sum(static_cast<const HllView &>(A), s);
+}
 __device__ __forceinline__ double row_abs_sum(const HllView &A, int s) {
   const int h = s / A.hksz, ii = s - h * A.hksz;
   const size_t off = (size_t)A.hkoffs[h] + ii;
@@ -478,6 +491,7 @@ __device__ __forceinline__ double row_abs_sum(const CsrView &A, int r) {
 
 __device__ __forceinline__ int out_row(const HllView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const Hll32View &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
+__device__ __forceinline__ int out_row(const Hll32WView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const HllViewF &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const EllView &, int r) { return r; }
 __device__ __forceinline__ int out_row(const CsrView &, int r) { return r; }
@@ -488,17 +502,22 @@ int psbx_hll_index_long(HllDevice *m);
 // Row sums of the wide hacks of a hack-32 matrix into lres, to be launched
 // before any row kernel that reads them with the same x; status (nullable)
 // makes it return at once when *status != 0.
-int psbx_long_rows32(const Hll32View &A, const double *x, const int *status, cudaStream_t st);
+int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cudaStream_t st);
 static inline Hll32View hll32_view(const HllView &v) {
   Hll32View w;
+  static_cast<HllView &>(w) = v;
+  return w;
+}
+static inline Hll32WView hll32w_view(const HllView &v) {
+  Hll32WView w;
   static_cast<HllView &>(w) = v;
   return w;
 }
 
 template <class View>
 static inline int psbx_long_rows(const View &, const double *, const int *, cudaStream_t) { return 0; }
-static inline int psbx_long_rows(const Hll32View &A, const double *x, const int *status, cudaStream_t st) {
-  return A.nLong ? psbx_long_rows32(A, x, status, st) : 0;
+static inline int psbx_long_rows(const Hll32WView &A, const double *x, const int *status, cudaStream_t st) {
+  return psbx_long_rows32(A, x, status, st);
 }
 EllView ell_view(const EllDevice *m);
 CsrView csr_view(const CsrDevice *m);

@@ -920,7 +920,7 @@ extern "C" int psbx_diag_prec_build(void *mat, int fmt, void *dinv) {
 // 1 when the matrix has wide hacks, whose rows a separate kernel sums before
 // each product (psbx_long_rows); 0 otherwise.
 template <class View> static inline int long_launch(const View &) { return 0; }
-static inline int long_launch(const Hll32View &A) { return A.nLong > 0 ? 1 : 0; }
+static inline int long_launch(const Hll32WView &) { return 1; }
 
 // Replays a captured batch of iterations until running(status) is false,
 // with 1, 2, 4, then 8 replays between two reads of the status word: a long
@@ -1266,8 +1266,11 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
   if (fmt == PSBX_FMT_HLL) {
     HllDevice *m = (HllDevice *)mat;
     if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
-    if (m->hackSize == 32)
-      return run_method(meth, hll32_view(hll_view(m)), dv, (const double *)B->v_, (double *)X->v_, n, opt);
+    if (m->hackSize == 32) {
+      const HllView v = hll_view(m);
+      if (v.nLong > 0) return run_method(meth, hll32w_view(v), dv, (const double *)B->v_, (double *)X->v_, n, opt);
+      return run_method(meth, hll32_view(v), dv, (const double *)B->v_, (double *)X->v_, n, opt);
+    }
     return run_method(meth, hll_view(m), dv, (const double *)B->v_, (double *)X->v_, n, opt);
   }
   if (fmt == PSBX_FMT_ELL)

@@ -45,11 +45,12 @@ HllView hll_view(const HllDevice *m) {
   v.longHacks = wide ? m->longHacks : nullptr;
   v.lres = wide ? m->lres : nullptr;
   v.nLong = wide ? m->nLong : 0;
+  v.longW = m->longW > 0 ? m->longW : PSBX_LONG_W;
   return v;
 }
 
 // --------------------------------------------------------------- wide hacks
-// A hack whose width exceeds PSBX_LONG_W would hold its warp for thousands
+// A hack whose width exceeds longW would hold its warp for thousands
 // of dependent steps (the tail of a row-sorted power-law matrix).  One block
 // per such hack: in chunks of LONG_CH entries per row, all 256 threads load
 // the chunk's values and indices (entry j of the 32 rows is one contiguous
@@ -57,7 +58,7 @@ HllView hll_view(const HllDevice *m) {
 // row r's products in entry order from 0 -- the same roundings as the
 // thread-per-row sum, so results are unchanged bit for bit.
 #define LONG_CH 128
-__global__ void __launch_bounds__(256) k_hll_long(Hll32View A, const double *__restrict__ x,
+__global__ void __launch_bounds__(256) k_hll_long(Hll32WView A, const double *__restrict__ x,
                                                   double *__restrict__ lres, const int *status) {
   if (status && *((volatile const int *)status) != 0) return;
   __shared__ double prod[LONG_CH * 32];
@@ -98,14 +99,14 @@ __global__ void __launch_bounds__(256) k_hll_long(Hll32View A, const double *__r
   if (threadIdx.x < 32 && s < A.rows) lres[s] = acc;
 }
 
-int psbx_long_rows32(const Hll32View &A, const double *x, const int *status, cudaStream_t st) {
+int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cudaStream_t st) {
   if (A.nLong <= 0) return SPGPU_SUCCESS;
   k_hll_long<<<A.nLong, 256, 0, st>>>(A, x, const_cast<double *>(A.lres), status);
   PSBX_LAUNCH_CK("k_hll_long");
   return SPGPU_SUCCESS;
 }
 
-// Lists the hacks wider than PSBX_LONG_W (hack size 32) from the offsets and
+// Lists the hacks wider than longW (hack size 32) from the offsets and
 // allocates their row-sum buffer; called whenever an HLL object's arrays are
 // (re)written.
 int psbx_hll_index_long(HllDevice *m) {
@@ -114,7 +115,8 @@ int psbx_hll_index_long(HllDevice *m) {
   m->longHacks = nullptr;
   m->lres = nullptr;
   m->nLong = 0;
-  if (m->hackSize != 32 || m->rows <= 0 || !m->hackOffs) return SPGPU_SUCCESS;
+  if (m->hackSize != 32 || m->rows <= 0 || !m->hackOffs || m->longW < 0) return SPGPU_SUCCESS;
+  const int lw = m->longW > 0 ? m->longW : PSBX_LONG_W;
   const int nh = (m->rows + 31) / 32;
   PsbxCtx &c = psbx_ctx();
   std::vector<int> hk((size_t)nh + 1);
@@ -122,7 +124,7 @@ int psbx_hll_index_long(HllDevice *m) {
   PSBX_CK(cudaStreamSynchronize(c.stream));
   std::vector<int> wide;
   for (int h = 0; h < nh; h++)
-    if (((hk[h + 1] - hk[h]) >> 5) > PSBX_LONG_W) wide.push_back(h);
+    if (((hk[h + 1] - hk[h]) >> 5) > lw) wide.push_back(h);
   if (wide.empty()) return SPGPU_SUCCESS;
   PSBX_CK(cudaMalloc(&m->longHacks, sizeof(int) * wide.size()));
   PSBX_CK(cudaMalloc(&m->lres, sizeof(double) * (size_t)m->rows));
@@ -196,7 +198,11 @@ int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, doub
                          cudaStream_t st) {
   if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
   if (alpha == 0.0 && m->perm == nullptr) return psbx_launch_scale(m->rows, beta, y, st);
-  if (m->hackSize == 32) return launch_rows(hll32_view(hll_view(m)), alpha, x, beta, y, st);
+  if (m->hackSize == 32) {
+    const HllView v = hll_view(m);
+    if (v.nLong > 0) return launch_rows(hll32w_view(v), alpha, x, beta, y, st);
+    return launch_rows(hll32_view(v), alpha, x, beta, y, st);
+  }
   return launch_rows(hll_view(m), alpha, x, beta, y, st);
 }
 

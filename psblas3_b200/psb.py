@@ -166,6 +166,20 @@ class HllMat:
               "psbx_hll_from_csr_device")
         return cls(h, rows)
 
+    @classmethod
+    def autotune_from_csr_device(cls, rows, cols, nnz, d_irp, d_ja, d_val, d_perm=None):
+        """Device CSR (raw device pointers, 1-based) -> the HLL layout with the
+        fastest SpMV among hack sizes 32/64/128 and wide-hack thresholds;
+        returns (HllMat, {"hksz", "wide_w", "ms"})."""
+        h = C.c_void_p()
+        hk, ww, ms = C.c_int(0), C.c_int(0), C.c_double(0.0)
+        check(lib.psbx_hll_autotune_from_csr_device(C.byref(h), rows, cols, nnz, C.c_void_p(d_irp),
+                                                    C.c_void_p(d_ja), C.c_void_p(d_val),
+                                                    None if d_perm is None else C.c_void_p(d_perm),
+                                                    C.byref(hk), C.byref(ww), C.byref(ms)),
+              "psbx_hll_autotune_from_csr_device")
+        return cls(h, rows), {"hksz": hk.value, "wide_w": ww.value, "ms": ms.value}
+
     def params(self):
         v = [C.c_int() for _ in range(7)]
         check(lib.getHllDeviceParams(self.h, *[C.byref(t) for t in v]), "getHllDeviceParams")

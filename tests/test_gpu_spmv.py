@@ -386,3 +386,21 @@ def test_hll_wide_hacks_bitexact(psb, alpha, beta):
     X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
     P.spmv(alpha, X, beta, Y)
     assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, alpha, x, beta, y0))
+
+
+def test_hll_autotune(psb):
+    """The autotuned layout (hack size, wide-hack threshold) gives the same
+    bits as the CPU csmv for a stencil and a skewed row-sorted matrix, and
+    its choice lies in the candidate set."""
+    import torch
+    for irp, ja, va in (gen.stencil27(40), gen.sort_rows_by_length(*gen.powerlaw(80000, kmax=4000, seed=2))[:3]):
+        n = len(irp) - 1
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        A, info = psb.HllMat.autotune_from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(),
+                                                     d[2].data_ptr())
+        assert info["hksz"] in (32, 64, 128) and info["ms"] > 0
+        assert info["wide_w"] in ((128, 256, 512, 1024, -1) if info["hksz"] == 32 else (0,))
+        x = np.random.default_rng(3).uniform(-1, 1, n)
+        X, Y = psb.DVect.bld(x), psb.DVect(n)
+        A.spmv(1.0, X, 0.0, Y)
+        assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, 1.0, x, 0.0, np.zeros(n))), info
