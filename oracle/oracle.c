@@ -854,3 +854,75 @@ int or_rgmres(int n, const int *irp, const int *ja, const double *val,
   free(V); free(w); free(w1); free(h); free(cs); free(sn); free(rs);
   return 0;
 }
+
+/* krylov/psb_dcgs.f90 (psb_dcgs_vect): conjugate gradient squared with the
+ * restart loop; init_conv once before it; rho == 0 or sigma == 0 go back to
+ * the restart (which recomputes r and rt = r). */
+int or_cgs(int n, const int *irp, const int *ja, const double *val,
+           const double *dinv, const double *b, double *x, double eps,
+           int itmax, int istop, int *iter, double *err, double *res_hist)
+{
+  double *q = (double *)calloc(n + 1, sizeof(double));
+  double *r = (double *)calloc(n + 1, sizeof(double));
+  double *rt = (double *)calloc(n + 1, sizeof(double));
+  double *p = (double *)calloc(n + 1, sizeof(double));
+  double *v = (double *)calloc(n + 1, sizeof(double));
+  double *uv = (double *)calloc(n + 1, sizeof(double));
+  double *z = (double *)calloc(n + 1, sizeof(double));
+  double *f = (double *)calloc(n + 1, sizeof(double));
+  double *s = (double *)calloc(n + 1, sizeof(double));
+  double *qt = (double *)calloc(n + 1, sizeof(double));
+  conv_t c;
+  int itx = 0, rc = 0;
+  double rho = 0.0, rho_old, alpha, beta, sigma;
+  if (init_conv(&c, istop, itmax, eps, n, irp, ja, val, b, x)) { rc = 1; goto done; }
+  for (;;) {
+    if (itx >= itmax) break;
+    int it = 0, conv = 0;
+    or_axpby(n, 1.0, b, 0.0, r);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    or_axpby(n, 1.0, r, 0.0, rt);
+    if (check_conv(&c, itx, n, x, r)) break;
+    if (res_hist) res_hist[itx] = end_err(&c);
+    rho = 0.0;
+    for (;;) {
+      it++;
+      itx++;
+      rho_old = rho;
+      rho = or_dot(n, rt, r);
+      if (rho == 0.0) break;
+      if (it == 1) {
+        or_axpby(n, 1.0, r, 0.0, uv);
+        or_axpby(n, 1.0, r, 0.0, p);
+      } else {
+        beta = rho / rho_old;
+        or_axpby(n, 1.0, r, 0.0, uv);
+        or_axpby(n, beta, q, 1.0, uv);
+        or_axpby(n, 1.0, q, beta, p);
+        or_axpby(n, 1.0, uv, beta, p);
+      }
+      prec_apply(n, dinv, p, f);
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, f, 0.0, v);
+      sigma = or_dot(n, rt, v);
+      if (sigma == 0.0) break;
+      alpha = rho / sigma;
+      or_axpby(n, 1.0, uv, 0.0, q);
+      or_axpby(n, -alpha, v, 1.0, q);
+      or_axpby(n, 1.0, uv, 0.0, s);
+      or_axpby(n, 1.0, q, 1.0, s);
+      prec_apply(n, dinv, s, z);
+      or_axpby(n, alpha, z, 1.0, x);
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, z, 0.0, qt);
+      or_axpby(n, -alpha, qt, 1.0, r);
+      int stop = check_conv(&c, itx, n, x, r);
+      if (res_hist && itx <= itmax) res_hist[itx] = end_err(&c);
+      if (stop) { conv = 1; break; }
+    }
+    if (conv) break;
+  }
+  *iter = itx;
+  *err = end_err(&c);
+done:
+  free(q); free(r); free(rt); free(p); free(v); free(uv); free(z); free(f); free(s); free(qt);
+  return rc;
+}

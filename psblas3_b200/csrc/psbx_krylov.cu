@@ -1,8 +1,9 @@
-// psbx_krylov.cu -- device-resident CG and BiCGSTAB with the diagonal
-// preconditioner: the psb_krylov('CG'|'BICGSTAB') path of
-// krylov/psb_dkrylov.f90:179-210, krylov/psb_dcg.F90:218-295,
-// krylov/psb_dcgstab.f90:226-365, stop test krylov/psb_d_krylov_conv_mod.f90:
-// 205-356, prec apply prec/impl/psb_d_diagprec_impl.f90:116.
+// psbx_krylov.cu -- device-resident Krylov solvers with the diagonal
+// preconditioner: the psb_krylov('CG'|'FCG'|'CGS'|'BICGSTAB'|'RGMRES') path of
+// krylov/psb_dkrylov.f90:179-210, krylov/psb_dcg.F90:218-295, psb_dfcg.F90,
+// psb_dcgs.f90, krylov/psb_dcgstab.f90:226-365, psb_drgmres.f90, stop test
+// krylov/psb_d_krylov_conv_mod.f90:205-356, prec apply
+// prec/impl/psb_d_diagprec_impl.f90:116.
 //
 // The reference runs one kernel per BLAS-1 call and brings every dot and
 // norm back to the host (3 blocking copies per CG iteration, 5 per
@@ -850,6 +851,180 @@ __global__ void __launch_bounds__(KT) k_gm_xupd(KState *S, GmSmall G, int n, con
   }
 }
 
+// ---------------------------------------------------------------- CGS
+// krylov/psb_dcgs.f90: per iteration uv/p update and f = M^-1 p | SpMV v = A f
+// with (rt,v) | q, s, z = M^-1 s, x update | SpMV A z fused with the r
+// update, (rt,r), and the stop-test norms.
+
+// restart: r = b - A*x ; rt = r ; stop test at itx ; first rho = (rt,r)
+template <class View>
+__global__ void __launch_bounds__(KT) k_cgs_init(View A, KState *S, const double *__restrict__ b,
+                                                 const double *__restrict__ x, double *__restrict__ r,
+                                                 double *__restrict__ rt, double *__restrict__ part,
+                                                 unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[192];
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double ax = row_dot(A, s, x);
+    const int i = out_row(A, s);
+    const double ri = radd(rmul(-1.0, ax), b[i]);
+    r[i] = ri;
+    rt[i] = ri;
+    dd_add_prod(acc[0], ri, ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(ld_ro(x + i)));
+  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      const double rr = dd_value(o[0]);
+      if (S->istop == 3 && !S->r0set) {  // psb_init_conv runs once, before the restart loop
+        S->r0n2 = sqrt(rr);
+        S->r0set = 1;
+      }
+      if (check_conv(S, rr, m[0], m[1])) {
+        S->status = ST_DONE;
+      } else {
+        S->it = 1;
+        S->itx += 1;
+        S->rho_old = 0.0;
+        S->rho = rr;  // (rt,r) with rt == r
+        S->status = rr == 0.0 ? ST_BREAK : ST_RUN;
+      }
+      *ticket = 0;
+    }
+  }
+}
+
+// it == 1: uv = r, p = r ; else uv = beta q + r, p = q + beta p, p = uv + beta p ;
+// f = M^-1 p
+__global__ void __launch_bounds__(KT) k_cgs_p(KState *S, int n, const double *__restrict__ r,
+                                              const double *__restrict__ q, const double *__restrict__ dinv,
+                                              double *__restrict__ uv, double *__restrict__ p,
+                                              double *__restrict__ f) {
+  if (stopped(S)) return;
+  const bool first = S->it == 1;
+  const double beta = S->beta;
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    const double ri = r[i];
+    double ui, pi;
+    if (first) {
+      ui = ri;
+      pi = ri;
+    } else {
+      const double qi = q[i];
+      ui = radd(rmul(beta, qi), ri);
+      pi = radd(qi, rmul(beta, p[i]));
+      pi = radd(ui, rmul(beta, pi));
+    }
+    uv[i] = ui;
+    p[i] = pi;
+    f[i] = prec(dinv, i, pi);
+  }
+}
+
+// v = A*f ; sigma = (rt,v) ; alpha = rho/sigma
+template <class View>
+__global__ void __launch_bounds__(KT) k_cgs_spmv1(View A, KState *S, const double *__restrict__ f,
+                                                  const double *__restrict__ rt, double *__restrict__ v,
+                                                  double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                  int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double t = row_dot(A, s, f);
+    const int i = out_row(A, s);
+    v[i] = t;
+    dd_add_prod(acc[0], ld_ro(rt + i), t);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      const double sigma = dd_value(o[0]);
+      S->sigma = sigma;
+      if (sigma == 0.0) S->status = ST_BREAK;  // psb_dcgs.f90: breakdown s1
+      else S->alpha = S->rho / sigma;
+      *ticket = 0;
+    }
+  }
+}
+
+// q = -alpha v + uv ; s = q + uv ; z = M^-1 s ; x = alpha z + x
+__global__ void __launch_bounds__(KT) k_cgs_q(KState *S, int n, const double *__restrict__ uv,
+                                              const double *__restrict__ v, const double *__restrict__ dinv,
+                                              double *__restrict__ q, double *__restrict__ z,
+                                              double *__restrict__ x) {
+  if (stopped(S)) return;
+  const double alpha = S->alpha, malpha = -S->alpha;
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    const double ui = uv[i];
+    const double qi = radd(rmul(malpha, v[i]), ui);
+    const double zi = prec(dinv, i, radd(qi, ui));
+    q[i] = qi;
+    z[i] = zi;
+    x[i] = radd(rmul(alpha, zi), x[i]);
+  }
+}
+
+// r = -alpha (A z) + r ; stop test ; next rho = (rt,r), beta = rho/rho_old
+template <class View>
+__global__ void __launch_bounds__(KT) k_cgs_spmv2(View A, KState *S, const double *__restrict__ z,
+                                                  const double *__restrict__ rt, const double *__restrict__ x,
+                                                  double *__restrict__ r, double *__restrict__ part,
+                                                  unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[192];
+  if (stopped(S)) return;
+  const double malpha = -S->alpha;
+  const bool need_x = S->istop == 1;
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double t = row_dot(A, s, z);
+    const int i = out_row(A, s);
+    const double ri = radd(rmul(malpha, t), r[i]);
+    r[i] = ri;
+    dd_add_prod(acc[0], ri, ri);
+    dd_add_prod(acc[1], ld_ro(rt + i), ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    if (need_x) mx[1] = fmax(mx[1], fabs(x[i]));
+  }
+  block_sum_dd<2>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<2>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[2];
+    double m[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      if (check_conv(S, dd_value(o[0]), m[0], m[1])) {
+        S->status = ST_DONE;
+      } else {
+        S->it += 1;
+        S->itx += 1;
+        S->rho_old = S->rho;
+        S->rho = dd_value(o[1]);
+        if (S->rho == 0.0) S->status = ST_BREAK;  // psb_dcgs.f90: breakdown r
+        else S->beta = S->rho / S->rho_old;
+      }
+      *ticket = 0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- prec build
 // psb_d_diag_precbld (prec/impl/psb_d_diagprec_impl.f90:229-292) with the
 // diagonal of psb_d_hll_get_diag (ext/impl/psb_d_hll_get_diag.f90:89-107):
@@ -1229,11 +1404,104 @@ static int solve_gmres(const View &A, const double *dinv, const double *b, doubl
   return rc;
 }
 
+// CGS driver: restart kernel on the host loop, then a graph of
+// KGRAPH_ITERS x (uv,p,f | SpMV + (rt,v) | q,z,x | SpMV + r, (rt,r), stop test).
+template <class View>
+static int solve_cgs(const View &A, const double *dinv, const double *b, double *x, int n, psbx_SolverOptions *opt) {
+  PsbxCtx &c = psbx_ctx();
+  cudaStream_t st = c.stream;
+  int grid = (n + KT - 1) / KT;
+  if (grid > c.sms * 8) grid = c.sms * 8;
+  if (grid < 1) grid = 1;
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  double *vec = nullptr, *part = nullptr;
+  KState *S = nullptr;
+  unsigned *ticket = nullptr;
+  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * 8 * nn, st));
+  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
+  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * 8 * nn, st));
+  KState *hS = (KState *)c.h_res;
+  KState init;
+  memset(&init, 0, sizeof(init));
+  init.eps = opt->eps;
+  init.itmax = opt->itmax;
+  init.istop = opt->istop;
+  init.status = ST_RUN;
+  PSBX_CK(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  double *r = vec, *rt = vec + nn, *p = vec + 2 * nn, *q = vec + 3 * nn, *uv = vec + 4 * nn, *f = vec + 5 * nn,
+         *v = vec + 6 * nn, *z = vec + 7 * nn;
+
+  k_kry_setup<<<grid, KT, 0, st>>>(n, b, S, part, ticket, grid);
+  psbx_count_launch();
+  if (opt->istop == 1) {
+    k_kry_normi<View><<<grid, KT, 0, st>>>(A, S, part, ticket, grid);
+    psbx_count_launch();
+  }
+  int rc = SPGPU_SUCCESS;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
+  if (!rc) {
+    for (int k = 0; k < KGRAPH_ITERS; k++) {
+      k_cgs_p<<<grid, KT, 0, st>>>(S, n, r, q, dinv, uv, p, f);
+      psbx_long_rows(A, f, &S->status, st);
+      k_cgs_spmv1<View><<<grid, KT, 0, st>>>(A, S, f, rt, v, part, ticket, grid);
+      k_cgs_q<<<grid, KT, 0, st>>>(S, n, uv, v, dinv, q, z, x);
+      psbx_long_rows(A, z, &S->status, st);
+      k_cgs_spmv2<View><<<grid, KT, 0, st>>>(A, S, z, rt, x, r, part, ticket, grid);
+    }
+    e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "EndCapture");
+  }
+  if (!rc) {
+    e = cudaGraphInstantiate(&gexec, graph, 0);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+  }
+  auto fetch = [&]() -> int {
+    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    return SPGPU_SUCCESS;
+  };
+  if (!rc) rc = fetch();
+  // restart loop of psb_dcgs.f90
+  while (!rc) {
+    if (hS->itx >= opt->itmax) break;
+    if ((rc = psbx_long_rows(A, x, nullptr, st))) break;
+    k_cgs_init<View><<<grid, KT, 0, st>>>(A, S, b, x, r, rt, part, ticket, grid);
+    psbx_count_launch(1 + long_launch(A));
+    if ((rc = fetch())) break;
+    if (hS->status == ST_DONE) break;
+    if (hS->status == ST_BREAK) continue;
+    rc = replay_until(gexec, st, (4 + 2 * long_launch(A)) * KGRAPH_ITERS, S, hS,
+                      [](const KState &k) { return k.status == ST_RUN; });
+    if (rc || hS->status == ST_DONE) break;
+    // ST_BREAK (rho or sigma == 0): back to the restart
+  }
+  if (!rc) {
+    opt->iter = hS->itx;
+    opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(S, st);
+  cudaFreeAsync(ticket, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (!rc && e2 != cudaSuccess) rc = psbx_cuda_status(e2, "solve_cgs");
+  return rc;
+}
+
 template <class View>
 static int run_method(int meth, const View &A, const double *dinv, const double *b, double *x, int n,
                       psbx_SolverOptions *opt) {
   if (meth == 2) return solve_fcg(A, dinv, b, x, n, opt);
   if (meth == 3) return solve_gmres(A, dinv, b, x, n, opt);
+  if (meth == 4) return solve_cgs(A, dinv, b, x, n, opt);
   return solve(A, meth == 1, dinv, b, x, n, opt);
 }
 
@@ -1242,12 +1510,13 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
   int rc = psbx_ensure_init();
   if (rc) return rc;
   if (!method || !mat || !b || !x || !opt) return SPGPU_UNSUPPORTED;
-  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES (psb_dkrylov.f90:179-210)
+  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES, 4 CGS (psb_dkrylov.f90:179-210)
   int meth;
   if (!strcasecmp(method, "CG")) meth = 0;
   else if (!strcasecmp(method, "BICGSTAB")) meth = 1;
   else if (!strcasecmp(method, "FCG")) meth = 2;
   else if (!strcasecmp(method, "RGMRES") || !strcasecmp(method, "GMRES")) meth = 3;
+  else if (!strcasecmp(method, "CGS")) meth = 4;
   else return SPGPU_UNSUPPORTED;  // other methods are outside this library
   if (opt->istop < 1 || opt->istop > 3) return SPGPU_UNSUPPORTED;  // psb_err_invalid_istop_
   // RGMRES: the reference accepts istop 1 and 2 (psb_drgmres.f90); istop 1
