@@ -140,7 +140,7 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
-        for name in ("or_cg", "or_bicgstab", "or_fcg", "or_cgs"):
+        for name in ("or_cg", "or_bicgstab", "or_fcg", "or_cgs", "or_bicg"):
             f = getattr(L, name)
             f.restype = I
             f.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I,
@@ -303,7 +303,7 @@ def diag_prec_build(diag):
 # ---------------------------------------------------------------- Krylov
 def krylov(method, irp, ja, val, b, x0=None, dinv=None, eps=1e-6, itmax=1000, istop=2,
            history=False, irst=10):
-    """psb_krylov('CG'|'FCG'|'CGS'|'BICGSTAB'|'RGMRES') restated; returns
+    """psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|'RGMRES') restated; returns
     (x, iter, err[, hist]).  irst is the GMRES restart length."""
     n = len(irp) - 1
     x = np.zeros(n) if x0 is None else _f64(x0).copy()
@@ -317,7 +317,8 @@ def krylov(method, irp, ja, val, b, x0=None, dinv=None, eps=1e-6, itmax=1000, is
         args.append(int(irst))
         f = lib().or_rgmres
     else:
-        f = {"CG": lib().or_cg, "BICGSTAB": lib().or_bicgstab, "FCG": lib().or_fcg, "CGS": lib().or_cgs}[m]
+        f = {"CG": lib().or_cg, "BICGSTAB": lib().or_bicgstab, "FCG": lib().or_fcg, "CGS": lib().or_cgs,
+             "BICG": lib().or_bicg}[m]
     rc = f(*args, C.byref(it), C.byref(err), None if hist is None else hist.ctypes.data_as(C.c_void_p))
     if rc != 0:
         raise ValueError(f"oracle krylov failed rc={rc}")

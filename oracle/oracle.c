@@ -926,3 +926,69 @@ done:
   free(q); free(r); free(rt); free(p); free(v); free(uv); free(z); free(f); free(s); free(qt);
   return rc;
 }
+
+/* krylov/psb_dbicg.f90 (psb_dbicg_vect): biconjugate gradient with the
+ * restart loop; the transposed products go through csmv 'T' (the diagonal
+ * preconditioner is its own transpose); rho == 0 or sigma == 0 go back to
+ * the restart. */
+int or_bicg(int n, const int *irp, const int *ja, const double *val,
+            const double *dinv, const double *b, double *x, double eps,
+            int itmax, int istop, int *iter, double *err, double *res_hist)
+{
+  double *r = (double *)calloc(n + 1, sizeof(double));
+  double *rt = (double *)calloc(n + 1, sizeof(double));
+  double *z = (double *)calloc(n + 1, sizeof(double));
+  double *zt = (double *)calloc(n + 1, sizeof(double));
+  double *p = (double *)calloc(n + 1, sizeof(double));
+  double *pt = (double *)calloc(n + 1, sizeof(double));
+  double *q = (double *)calloc(n + 1, sizeof(double));
+  double *qt = (double *)calloc(n + 1, sizeof(double));
+  conv_t c;
+  int itx = 0, rc = 0;
+  double rho = 0.0, rho_old, alpha, beta, sigma;
+  if (init_conv(&c, istop, itmax, eps, n, irp, ja, val, b, x)) { rc = 1; goto done; }
+  for (;;) {
+    if (itx >= itmax) break;
+    int it = 0, conv = 0;
+    or_axpby(n, 1.0, b, 0.0, r);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    or_axpby(n, 1.0, r, 0.0, rt);
+    rho = 0.0;
+    if (check_conv(&c, itx, n, x, r)) break;
+    if (res_hist) res_hist[itx] = end_err(&c);
+    for (;;) {
+      it++;
+      itx++;
+      prec_apply(n, dinv, r, z);
+      prec_apply(n, dinv, rt, zt);
+      rho_old = rho;
+      rho = or_dot(n, rt, z);
+      if (rho == 0.0) break;
+      if (it == 1) {
+        or_axpby(n, 1.0, z, 0.0, p);
+        or_axpby(n, 1.0, zt, 0.0, pt);
+      } else {
+        beta = rho / rho_old;
+        or_axpby(n, 1.0, z, beta, p);
+        or_axpby(n, 1.0, zt, beta, pt);
+      }
+      or_csr_csmv('N', n, n, irp, ja, val, 1.0, p, 0.0, q);
+      or_csr_csmv('T', n, n, irp, ja, val, 1.0, pt, 0.0, qt);
+      sigma = or_dot(n, pt, q);
+      if (sigma == 0.0) break;
+      alpha = rho / sigma;
+      or_axpby(n, alpha, p, 1.0, x);
+      or_axpby(n, -alpha, q, 1.0, r);
+      or_axpby(n, -alpha, qt, 1.0, rt);
+      int stop = check_conv(&c, itx, n, x, r);
+      if (res_hist && itx <= itmax) res_hist[itx] = end_err(&c);
+      if (stop) { conv = 1; break; }
+    }
+    if (conv) break;
+  }
+  *iter = itx;
+  *err = end_err(&c);
+done:
+  free(r); free(rt); free(z); free(zt); free(p); free(pt); free(q); free(qt);
+  return rc;
+}

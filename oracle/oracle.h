@@ -86,6 +86,9 @@ int or_rgmres(int n, const int *irp, const int *ja, const double *val,
 int or_cgs(int n, const int *irp, const int *ja, const double *val,
            const double *dinv, const double *b, double *x, double eps,
            int itmax, int istop, int *iter, double *err, double *res_hist);
+int or_bicg(int n, const int *irp, const int *ja, const double *val,
+            const double *dinv, const double *b, double *x, double eps,
+            int itmax, int istop, int *iter, double *err, double *res_hist);
 void or_drotg(double *a, double *b, double *c, double *s);
 
 #ifdef __cplusplus

@@ -1,9 +1,9 @@
 // psbx_krylov.cu -- device-resident Krylov solvers with the diagonal
-// preconditioner: the psb_krylov('CG'|'FCG'|'CGS'|'BICGSTAB'|'RGMRES') path of
-// krylov/psb_dkrylov.f90:179-210, krylov/psb_dcg.F90:218-295, psb_dfcg.F90,
-// psb_dcgs.f90, krylov/psb_dcgstab.f90:226-365, psb_drgmres.f90, stop test
-// krylov/psb_d_krylov_conv_mod.f90:205-356, prec apply
-// prec/impl/psb_d_diagprec_impl.f90:116.
+// preconditioner: the psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|'RGMRES')
+// path of krylov/psb_dkrylov.f90:179-210, krylov/psb_dcg.F90:218-295,
+// psb_dfcg.F90, psb_dcgs.f90, psb_dbicg.f90, krylov/psb_dcgstab.f90:226-365,
+// psb_drgmres.f90, stop test krylov/psb_d_krylov_conv_mod.f90:205-356, prec
+// apply prec/impl/psb_d_diagprec_impl.f90:116.
 //
 // The reference runs one kernel per BLAS-1 call and brings every dot and
 // norm back to the host (3 blocking copies per CG iteration, 5 per
@@ -1025,6 +1025,196 @@ __global__ void __launch_bounds__(KT) k_cgs_spmv2(View A, KState *S, const doubl
   }
 }
 
+// ---------------------------------------------------------------- BiCG
+// krylov/psb_dbicg.f90.  The transposed product A^T pt runs on a CSR copy of
+// A^T built once per solve (host counting sort, stable: the entries of each
+// column in ascending row order), so y_c = sum over rows i of (1*a_ic)*x_i
+// accumulates in the order of the reference's scatter loop (csmv 'T').
+
+// qt = A^T pt, one thread per column
+__global__ void __launch_bounds__(KT) k_spmv_t(KState *S, int n, const int *__restrict__ tirp,
+                                               const int *__restrict__ tja, const double *__restrict__ tval,
+                                               const double *__restrict__ x, double *__restrict__ y) {
+  if (stopped(S)) return;
+  for (int c = blockIdx.x * KT + threadIdx.x; c < n; c += gridDim.x * KT) {
+    double acc = 0.0;
+    for (int k = tirp[c]; k < tirp[c + 1]; k++) acc = radd(acc, rmul(ld_ro(tval + k), ld_ro(x + ld_ro(tja + k))));
+    y[c] = acc;
+  }
+}
+
+// restart: r = b - A*x ; rt = r ; stop test at itx
+template <class View>
+__global__ void __launch_bounds__(KT) k_bicg_init(View A, KState *S, const double *__restrict__ b,
+                                                  const double *__restrict__ x, double *__restrict__ r,
+                                                  double *__restrict__ rt, double *__restrict__ part,
+                                                  unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[192];
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double ax = row_dot(A, s, x);
+    const int i = out_row(A, s);
+    const double ri = radd(rmul(-1.0, ax), b[i]);
+    r[i] = ri;
+    rt[i] = ri;
+    dd_add_prod(acc[0], ri, ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(ld_ro(x + i)));
+  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      const double rr = dd_value(o[0]);
+      if (S->istop == 3 && !S->r0set) {  // psb_init_conv runs once, before the restart loop
+        S->r0n2 = sqrt(rr);
+        S->r0set = 1;
+      }
+      S->status = check_conv(S, rr, m[0], m[1]) ? ST_DONE : ST_RUN;
+      S->it = 0;
+      S->rho = 0.0;
+      *ticket = 0;
+    }
+  }
+}
+
+// iteration top after a restart: z = M^-1 r ; zt = M^-1 rt ; rho = (rt,z)
+__global__ void __launch_bounds__(KT) k_bicg_top(KState *S, int n, const double *__restrict__ r,
+                                                 const double *__restrict__ rt, const double *__restrict__ dinv,
+                                                 double *__restrict__ z, double *__restrict__ zt,
+                                                 double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                 int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    const double zi = prec(dinv, i, r[i]);
+    const double rti = rt[i];
+    z[i] = zi;
+    zt[i] = prec(dinv, i, rti);
+    dd_add_prod(acc[0], rti, zi);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      S->it += 1;
+      S->itx += 1;
+      S->rho_old = S->rho;
+      S->rho = dd_value(o[0]);
+      if (S->rho == 0.0) S->status = ST_BREAK;  // psb_dbicg.f90: breakdown r
+      else if (S->it > 1) S->beta = S->rho / S->rho_old;
+      *ticket = 0;
+    }
+  }
+}
+
+// p = z, pt = zt (it == 1) or p = z + beta p, pt = zt + beta pt
+__global__ void __launch_bounds__(KT) k_bicg_p(KState *S, int n, const double *__restrict__ z,
+                                               const double *__restrict__ zt, double *__restrict__ p,
+                                               double *__restrict__ pt) {
+  if (stopped(S)) return;
+  const bool first = S->it == 1;
+  const double beta = S->beta;
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    p[i] = first ? z[i] : radd(z[i], rmul(beta, p[i]));
+    pt[i] = first ? zt[i] : radd(zt[i], rmul(beta, pt[i]));
+  }
+}
+
+// q = A*p ; sigma = (pt,q) ; alpha = rho/sigma
+template <class View>
+__global__ void __launch_bounds__(KT) k_bicg_spmv(View A, KState *S, const double *__restrict__ p,
+                                                  const double *__restrict__ pt, double *__restrict__ q,
+                                                  double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                  int grid) {
+  __shared__ double sm[64];
+  if (stopped(S)) return;
+  dd_t acc[1] = {{0.0, 0.0}};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double t = row_dot(A, s, p);
+    const int i = out_row(A, s);
+    q[i] = t;
+    dd_add_prod(acc[0], ld_ro(pt + i), t);
+  }
+  block_sum_dd<1>(acc, sm);
+  publish_sums<1>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      const double sigma = dd_value(o[0]);
+      S->sigma = sigma;
+      if (sigma == 0.0) S->status = ST_BREAK;  // psb_dbicg.f90: breakdown s1
+      else S->alpha = S->rho / sigma;
+      *ticket = 0;
+    }
+  }
+}
+
+// x = alpha p + x ; r = -alpha q + r ; rt = -alpha qt + rt ; stop test ;
+// next top: z = M^-1 r, zt = M^-1 rt, rho = (rt,z)
+__global__ void __launch_bounds__(KT) k_bicg_update(KState *S, int n, const double *__restrict__ p,
+                                                    const double *__restrict__ q, const double *__restrict__ qt,
+                                                    const double *__restrict__ dinv, double *__restrict__ x,
+                                                    double *__restrict__ r, double *__restrict__ rt,
+                                                    double *__restrict__ z, double *__restrict__ zt,
+                                                    double *__restrict__ part, unsigned *__restrict__ ticket,
+                                                    int grid) {
+  __shared__ double sm[192];
+  if (stopped(S)) return;
+  const double alpha = S->alpha, malpha = -S->alpha;
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    const double xi = radd(rmul(alpha, p[i]), x[i]);
+    const double ri = radd(rmul(malpha, q[i]), r[i]);
+    const double rti = radd(rmul(malpha, qt[i]), rt[i]);
+    const double zi = prec(dinv, i, ri);
+    x[i] = xi;
+    r[i] = ri;
+    rt[i] = rti;
+    z[i] = zi;
+    zt[i] = prec(dinv, i, rti);
+    dd_add_prod(acc[0], ri, ri);
+    dd_add_prod(acc[1], rti, zi);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(xi));
+  }
+  block_sum_dd<2>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<2>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[2];
+    double m[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      if (check_conv(S, dd_value(o[0]), m[0], m[1])) {
+        S->status = ST_DONE;
+      } else {
+        S->it += 1;
+        S->itx += 1;
+        S->rho_old = S->rho;
+        S->rho = dd_value(o[1]);
+        if (S->rho == 0.0) S->status = ST_BREAK;
+        else S->beta = S->rho / S->rho_old;
+      }
+      *ticket = 0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- prec build
 // psb_d_diag_precbld (prec/impl/psb_d_diagprec_impl.f90:229-292) with the
 // diagonal of psb_d_hll_get_diag (ext/impl/psb_d_hll_get_diag.f90:89-107):
@@ -1496,6 +1686,203 @@ static int solve_cgs(const View &A, const double *dinv, const double *b, double 
   return rc;
 }
 
+// CSR of A^T (0-based), entries of each column in ascending row order, from
+// the matrix's own arrays (read back once per solve).
+static int build_transpose(void *mat, int fmt, int n, int **tirp, int **tja, double **tval) {
+  PsbxCtx &c = psbx_ctx();
+  std::vector<int> rowptr(n + 1, 0), cols;
+  std::vector<double> vals;
+  auto get = [&](void *dst, const void *src, size_t bytes) -> int {
+    if (!bytes) return SPGPU_SUCCESS;
+    PSBX_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+    return SPGPU_SUCCESS;
+  };
+  int rc = SPGPU_SUCCESS;
+  if (fmt == PSBX_FMT_HLL) {
+    HllDevice *m = (HllDevice *)mat;
+    const int hk = m->hackSize, nh = (m->rows + hk - 1) / hk;
+    std::vector<int> hko(nh + 1), irn(m->rows), ja(m->allocsize), perm;
+    std::vector<double> val(m->allocsize);
+    rc = get(hko.data(), m->hackOffs, sizeof(int) * (nh + 1));
+    if (!rc) rc = get(irn.data(), m->rS, sizeof(int) * m->rows);
+    if (!rc) rc = get(ja.data(), m->rP, sizeof(int) * (size_t)m->allocsize);
+    if (!rc) rc = get(val.data(), m->cM, sizeof(double) * (size_t)m->allocsize);
+    if (!rc && m->perm) {
+      perm.resize(m->rows);
+      rc = get(perm.data(), m->perm, sizeof(int) * m->rows);
+    }
+    if (!rc) PSBX_CK(cudaStreamSynchronize(c.stream));
+    std::vector<int> srow(n);  // storage row of each matrix row
+    for (int s = 0; s < m->rows; s++) srow[perm.empty() ? s : perm[s]] = s;
+    for (int i = 0; i < n; i++) {
+      const int s = srow[i], h = s / hk, l = s % hk;
+      for (int j = 0; j < irn[s]; j++) {
+        const size_t p = (size_t)hko[h] + (size_t)j * hk + l;
+        cols.push_back(ja[p] - m->baseIndex);
+        vals.push_back(val[p]);
+      }
+      rowptr[i + 1] = (int)cols.size();
+    }
+  } else if (fmt == PSBX_FMT_ELL) {
+    EllDevice *m = (EllDevice *)mat;
+    std::vector<int> irn(m->rows), ja((size_t)m->pitch * m->maxRowSize);
+    std::vector<double> val((size_t)m->pitch * m->maxRowSize);
+    rc = get(irn.data(), m->rS, sizeof(int) * m->rows);
+    if (!rc) rc = get(ja.data(), m->rP, sizeof(int) * ja.size());
+    if (!rc) rc = get(val.data(), m->cM, sizeof(double) * val.size());
+    if (!rc) PSBX_CK(cudaStreamSynchronize(c.stream));
+    for (int i = 0; i < n; i++) {
+      for (int j = 0; j < irn[i]; j++) {
+        const size_t p = (size_t)i + (size_t)j * m->pitch;
+        cols.push_back(ja[p] - m->baseIndex);
+        vals.push_back(val[p]);
+      }
+      rowptr[i + 1] = (int)cols.size();
+    }
+  } else {
+    CsrDevice *m = (CsrDevice *)((psbx_d_Cmat *)mat)->mat;
+    std::vector<int> irp(m->m + 1), ja(m->nz);
+    std::vector<double> val(m->nz);
+    rc = get(irp.data(), m->irp, sizeof(int) * (m->m + 1));
+    if (!rc) rc = get(ja.data(), m->ja, sizeof(int) * (size_t)m->nz);
+    if (!rc) rc = get(val.data(), m->val, sizeof(double) * (size_t)m->nz);
+    if (!rc) PSBX_CK(cudaStreamSynchronize(c.stream));
+    for (int i = 0; i < n; i++) {
+      for (int k = irp[i] - m->baseIndex; k < irp[i + 1] - m->baseIndex; k++) {
+        cols.push_back(ja[k] - m->baseIndex);
+        vals.push_back(val[k]);
+      }
+      rowptr[i + 1] = (int)cols.size();
+    }
+  }
+  if (rc) return rc;
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  // counting sort by column; rows are visited in ascending order, so each
+  // column's entries come out in ascending row order
+  const size_t nz = cols.size();
+  std::vector<int> tp(n + 1, 0), tj(nz > 0 ? nz : 1), next;
+  std::vector<double> tv(nz > 0 ? nz : 1);
+  for (size_t k = 0; k < nz; k++) {
+    if (cols[k] < 0 || cols[k] >= n) return SPGPU_UNSUPPORTED;  // BiCG needs a square matrix
+    tp[cols[k] + 1]++;
+  }
+  for (int c2 = 0; c2 < n; c2++) tp[c2 + 1] += tp[c2];
+  next.assign(tp.begin(), tp.end() - 1);
+  for (int i = 0; i < n; i++)
+    for (int k = rowptr[i]; k < rowptr[i + 1]; k++) {
+      const int pos = next[cols[k]]++;
+      tj[pos] = i;
+      tv[pos] = vals[k];
+    }
+  PSBX_CK(cudaMallocAsync(tirp, sizeof(int) * (n + 1), c.stream));
+  PSBX_CK(cudaMallocAsync(tja, sizeof(int) * tj.size(), c.stream));
+  PSBX_CK(cudaMallocAsync(tval, sizeof(double) * tv.size(), c.stream));
+  PSBX_CK(cudaMemcpyAsync(*tirp, tp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaMemcpyAsync(*tja, tj.data(), sizeof(int) * tj.size(), cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaMemcpyAsync(*tval, tv.data(), sizeof(double) * tv.size(), cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  return SPGPU_SUCCESS;
+}
+
+// BiCG driver: transpose once, restart kernels on the host loop, then a graph
+// of KGRAPH_ITERS x (p,pt | SpMV + (pt,q) | A^T pt | updates, stop test, top).
+template <class View>
+static int solve_bicg(const View &A, void *mat, int fmt, const double *dinv, const double *b, double *x, int n,
+                      psbx_SolverOptions *opt) {
+  PsbxCtx &c = psbx_ctx();
+  cudaStream_t st = c.stream;
+  int *tirp = nullptr, *tja = nullptr;
+  double *tval = nullptr;
+  int rc = build_transpose(mat, fmt, n, &tirp, &tja, &tval);
+  if (rc) return rc;
+  int grid = (n + KT - 1) / KT;
+  if (grid > c.sms * 8) grid = c.sms * 8;
+  if (grid < 1) grid = 1;
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  double *vec = nullptr, *part = nullptr;
+  KState *S = nullptr;
+  unsigned *ticket = nullptr;
+  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * 8 * nn, st));
+  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
+  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * 8 * nn, st));
+  KState *hS = (KState *)c.h_res;
+  KState init;
+  memset(&init, 0, sizeof(init));
+  init.eps = opt->eps;
+  init.itmax = opt->itmax;
+  init.istop = opt->istop;
+  init.status = ST_RUN;
+  PSBX_CK(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  double *r = vec, *rt = vec + nn, *z = vec + 2 * nn, *zt = vec + 3 * nn, *p = vec + 4 * nn, *pt = vec + 5 * nn,
+         *q = vec + 6 * nn, *qt = vec + 7 * nn;
+
+  k_kry_setup<<<grid, KT, 0, st>>>(n, b, S, part, ticket, grid);
+  psbx_count_launch();
+  if (opt->istop == 1) {
+    k_kry_normi<View><<<grid, KT, 0, st>>>(A, S, part, ticket, grid);
+    psbx_count_launch();
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
+  if (!rc) {
+    for (int k = 0; k < KGRAPH_ITERS; k++) {
+      k_bicg_p<<<grid, KT, 0, st>>>(S, n, z, zt, p, pt);
+      psbx_long_rows(A, p, &S->status, st);
+      k_bicg_spmv<View><<<grid, KT, 0, st>>>(A, S, p, pt, q, part, ticket, grid);
+      k_spmv_t<<<grid, KT, 0, st>>>(S, n, tirp, tja, tval, pt, qt);
+      k_bicg_update<<<grid, KT, 0, st>>>(S, n, p, q, qt, dinv, x, r, rt, z, zt, part, ticket, grid);
+    }
+    e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "EndCapture");
+  }
+  if (!rc) {
+    e = cudaGraphInstantiate(&gexec, graph, 0);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+  }
+  auto fetch = [&]() -> int {
+    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    return SPGPU_SUCCESS;
+  };
+  if (!rc) rc = fetch();
+  // restart loop of psb_dbicg.f90
+  while (!rc) {
+    if (hS->itx >= opt->itmax) break;
+    if ((rc = psbx_long_rows(A, x, nullptr, st))) break;
+    k_bicg_init<View><<<grid, KT, 0, st>>>(A, S, b, x, r, rt, part, ticket, grid);
+    k_bicg_top<<<grid, KT, 0, st>>>(S, n, r, rt, dinv, z, zt, part, ticket, grid);
+    psbx_count_launch(2 + long_launch(A));
+    if ((rc = fetch())) break;
+    if (hS->status == ST_DONE) break;
+    if (hS->status == ST_BREAK) continue;
+    rc = replay_until(gexec, st, (4 + long_launch(A)) * KGRAPH_ITERS, S, hS,
+                      [](const KState &k) { return k.status == ST_RUN; });
+    if (rc || hS->status == ST_DONE) break;
+    // ST_BREAK (rho or sigma == 0): back to the restart
+  }
+  if (!rc) {
+    opt->iter = hS->itx;
+    opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(S, st);
+  cudaFreeAsync(ticket, st);
+  cudaFreeAsync(tirp, st);
+  cudaFreeAsync(tja, st);
+  cudaFreeAsync(tval, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (!rc && e2 != cudaSuccess) rc = psbx_cuda_status(e2, "solve_bicg");
+  return rc;
+}
+
 template <class View>
 static int run_method(int meth, const View &A, const double *dinv, const double *b, double *x, int n,
                       psbx_SolverOptions *opt) {
@@ -1510,13 +1897,14 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
   int rc = psbx_ensure_init();
   if (rc) return rc;
   if (!method || !mat || !b || !x || !opt) return SPGPU_UNSUPPORTED;
-  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES, 4 CGS (psb_dkrylov.f90:179-210)
+  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES, 4 CGS, 5 BICG (psb_dkrylov.f90:179-210)
   int meth;
   if (!strcasecmp(method, "CG")) meth = 0;
   else if (!strcasecmp(method, "BICGSTAB")) meth = 1;
   else if (!strcasecmp(method, "FCG")) meth = 2;
   else if (!strcasecmp(method, "RGMRES") || !strcasecmp(method, "GMRES")) meth = 3;
   else if (!strcasecmp(method, "CGS")) meth = 4;
+  else if (!strcasecmp(method, "BICG")) meth = 5;
   else return SPGPU_UNSUPPORTED;  // other methods are outside this library
   if (opt->istop < 1 || opt->istop > 3) return SPGPU_UNSUPPORTED;  // psb_err_invalid_istop_
   // RGMRES: the reference accepts istop 1 and 2 (psb_drgmres.f90); istop 1
@@ -1531,6 +1919,22 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
     opt->iter = 0;
     opt->err = 0.0;
     return SPGPU_SUCCESS;
+  }
+  if (meth == 5) {  // BiCG also needs the matrix's arrays, for its transpose
+    const double *bp = (const double *)B->v_;
+    double *xp = (double *)X->v_;
+    if (fmt == PSBX_FMT_HLL) {
+      HllDevice *m = (HllDevice *)mat;
+      if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+      const HllView v = hll_view(m);
+      if (m->hackSize == 32 && v.nLong > 0) return solve_bicg(hll32w_view(v), mat, fmt, dv, bp, xp, n, opt);
+      if (m->hackSize == 32) return solve_bicg(hll32_view(v), mat, fmt, dv, bp, xp, n, opt);
+      return solve_bicg(v, mat, fmt, dv, bp, xp, n, opt);
+    }
+    if (fmt == PSBX_FMT_ELL) return solve_bicg(ell_view((EllDevice *)mat), mat, fmt, dv, bp, xp, n, opt);
+    if (fmt == PSBX_FMT_CSR)
+      return solve_bicg(csr_view((CsrDevice *)((psbx_d_Cmat *)mat)->mat), mat, fmt, dv, bp, xp, n, opt);
+    return SPGPU_UNSUPPORTED;
   }
   if (fmt == PSBX_FMT_HLL) {
     HllDevice *m = (HllDevice *)mat;

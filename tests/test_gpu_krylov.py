@@ -94,7 +94,7 @@ def test_cg_no_prec_and_itmax(psb):
 def test_zero_rhs_returns_at_once(psb):
     irp, ja, va = gen.poisson7(8)
     n = len(irp) - 1
-    for method in ("CG", "BICGSTAB", "FCG", "RGMRES", "CGS"):
+    for method in ("CG", "BICGSTAB", "FCG", "RGMRES", "CGS", "BICG"):
         (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, np.zeros(n))
         assert np.all(x == 0)
         assert it == ito
@@ -166,7 +166,7 @@ def test_itmax_fcg_and_rgmres(psb):
     assert abs(err - erro) <= 1e-6 * erro
 
 
-@pytest.mark.parametrize("method", ["CG", "FCG", "CGS", "BICGSTAB", "RGMRES"])
+@pytest.mark.parametrize("method", ["CG", "FCG", "CGS", "BICG", "BICGSTAB", "RGMRES"])
 def test_wide_hacks_in_solvers(psb, method):
     """Row-sorted SPD power-law matrix whose leading hacks are wider than 256
     (summed by a block each before every product): every method matches the
@@ -184,13 +184,15 @@ def test_wide_hacks_in_solvers(psb, method):
 
 @pytest.mark.parametrize("istop", [1, 2, 3])
 @pytest.mark.parametrize("fmt", ["HLL", "ELL", "CSR"])
-def test_cgs_c1(psb, istop, fmt):
-    """CGS (psb_dcgs.f90) on the nonsymmetric C1-type operator with DIAG:
+@pytest.mark.parametrize("method", ["CGS", "BICG"])
+def test_cgs_bicg_c1(psb, method, istop, fmt):
+    """CGS (psb_dcgs.f90) and BiCG (psb_dbicg.f90, A^T products on a
+    transposed copy) on the nonsymmetric C1-type operator with DIAG:
     iterations within +-2 of the oracle, tolerance reached, x close."""
     irp, ja, va = gen.pde3d(20, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
     n = len(irp) - 1
     b = O.csr_csmv(irp, ja, va, 1.0, np.ones(n), 0.0, np.zeros(n))
-    (x, it, err), (xo, ito, erro) = _solve_both(psb, "CGS", irp, ja, va, b, fmt=fmt, eps=1e-9, istop=istop)
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, b, fmt=fmt, eps=1e-9, istop=istop)
     assert abs(it - ito) <= 2, (it, ito)
     assert err <= 1e-9
     assert np.max(np.abs(x - xo)) <= 1e-6
