@@ -287,13 +287,28 @@ __device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k] = 0.0;
-  for (int j = lane; j < rr.n; j += 32) {
-    const int c = ld_stream(ja + rr.off + j * 32) - 1;
-    const double v = (double)ld_stream(val + rr.off + j * 32);
-    XT xv[K];
-    ld_row_ro<K>(x + (size_t)c * K, xv);
+  // a lane's entries lane, lane+32, ... in order, W of them per round with
+  // all their loads issued before the gathers
+  constexpr int W = K == 1 ? 8 : 2;
+  for (int j0 = lane; j0 < rr.n; j0 += 32 * W) {
+    int c[W];
+    double v[W];
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v, (double)xv[k]));
+    for (int u = 0; u < W; u++) {
+      const int j = j0 + 32 * u;
+      const bool ok = j < rr.n;
+      c[u] = ok ? ld_stream(ja + rr.off + j * 32) - 1 : 0;
+      v[u] = ok ? (double)ld_stream(val + rr.off + j * 32) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < W; u++) {
+      if (j0 + 32 * u < rr.n) {
+        XT xv[K];
+        ld_row_ro<K>(x + (size_t)c[u] * K, xv);
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v[u], (double)xv[k]));
+      }
+    }
   }
 #pragma unroll
   for (int k = 0; k < K; k++)
