@@ -249,11 +249,12 @@ int psbx_DefaultSolverOptions(psbx_SolverOptions *opt);
 #define PSBX_FMT_ELL 1
 #define PSBX_FMT_CSR 2
 
-/* Device-resident psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|'RGMRES')
- * (krylov/psb_dkrylov.f90:179-210 dispatch, psb_dcg.F90:218-295,
- * psb_dfcg.F90, psb_dcgs.f90, psb_dbicg.f90 -- its A^T products on a
- * transposed copy built at the start of the solve --, psb_dcgstab.f90:
- * 226-365, psb_drgmres.f90) with the diagonal
+/* Device-resident psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|
+ * 'BICGSTABL'|'RGMRES') (krylov/psb_dkrylov.f90:179-210 dispatch,
+ * psb_dcg.F90:218-295, psb_dfcg.F90, psb_dcgs.f90, psb_dbicg.f90 -- its A^T
+ * products on a transposed copy built at the start of the solve --,
+ * psb_dcgstab.f90:226-365, psb_dcgstabl.f90 with L = opt->irst,
+ * psb_drgmres.f90) with the diagonal
  * preconditioner (prec/impl/psb_d_diagprec_impl.f90:116).  RGMRES (also
  * 'GMRES') restarts every opt->irst steps and takes istop 2 only (the
  * reference also accepts 1); other method names return 1.

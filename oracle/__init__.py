@@ -145,9 +145,11 @@ def lib():
             f.restype = I
             f.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I,
                           C.POINTER(I), C.POINTER(D), C.c_void_p]
-        L.or_rgmres.restype = I
-        L.or_rgmres.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I, I,
-                                C.POINTER(I), C.POINTER(D), C.c_void_p]
+        for name in ("or_rgmres", "or_bicgstabl"):
+            f = getattr(L, name)
+            f.restype = I
+            f.argtypes = [I, _i32p, _i32p, _f64p, C.c_void_p, _f64p, _f64p, D, I, I, I,
+                          C.POINTER(I), C.POINTER(D), C.c_void_p]
         L.or_drotg.restype = None
         L.or_drotg.argtypes = [C.POINTER(D)] * 4
         _lib = L
@@ -303,7 +305,7 @@ def diag_prec_build(diag):
 # ---------------------------------------------------------------- Krylov
 def krylov(method, irp, ja, val, b, x0=None, dinv=None, eps=1e-6, itmax=1000, istop=2,
            history=False, irst=10):
-    """psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|'RGMRES') restated; returns
+    """psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|'BICGSTABL'|'RGMRES') restated; returns
     (x, iter, err[, hist]).  irst is the GMRES restart length."""
     n = len(irp) - 1
     x = np.zeros(n) if x0 is None else _f64(x0).copy()
@@ -313,9 +315,9 @@ def krylov(method, irp, ja, val, b, x0=None, dinv=None, eps=1e-6, itmax=1000, is
     m = method.upper()
     args = [n, _i32(irp), _i32(ja), _f64(val), None if d is None else d.ctypes.data_as(C.c_void_p),
             _f64(b), x, float(eps), int(itmax), int(istop)]
-    if m in ("RGMRES", "GMRES"):
+    if m in ("RGMRES", "GMRES", "BICGSTABL"):
         args.append(int(irst))
-        f = lib().or_rgmres
+        f = lib().or_bicgstabl if m == "BICGSTABL" else lib().or_rgmres
     else:
         f = {"CG": lib().or_cg, "BICGSTAB": lib().or_bicgstab, "FCG": lib().or_fcg, "CGS": lib().or_cgs,
              "BICG": lib().or_bicg}[m]

@@ -992,3 +992,115 @@ done:
   free(r); free(rt); free(z); free(zt); free(p); free(pt); free(q); free(qt);
   return rc;
 }
+
+/* krylov/psb_dcgstabl.f90 (psb_dcgstabl_vect): BiCGSTAB(L), nl = irst, left
+ * preconditioned (r and the new directions are preconditioned in place), the
+ * stop test on the preconditioned residual; breakdowns go back to the
+ * restart. */
+int or_bicgstabl(int n, const int *irp, const int *ja, const double *val,
+                 const double *dinv, const double *b, double *x, double eps,
+                 int itmax, int istop, int irst, int *iter, double *err,
+                 double *res_hist)
+{
+  if (irst <= 0) return 1;
+  const int nl = irst;
+  double *r = (double *)calloc(n + 1, sizeof(double));
+  double *rt0 = (double *)calloc(n + 1, sizeof(double));
+  double *uh = (double *)calloc((size_t)(nl + 1) * n + 1, sizeof(double));
+  double *rh = (double *)calloc((size_t)(nl + 1) * n + 1, sizeof(double));
+  double *tmp = (double *)calloc(n + 1, sizeof(double));
+  double *gamma = (double *)calloc(nl + 1, sizeof(double));
+  double *gamma1 = (double *)calloc(nl + 1, sizeof(double));
+  double *gamma2 = (double *)calloc(nl + 1, sizeof(double));
+  double *sigma = (double *)calloc(nl + 1, sizeof(double));
+  double *taum = (double *)calloc((size_t)(nl + 1) * (nl + 1), sizeof(double));
+#define UH(k) (uh + (size_t)(k) * n)
+#define RH(k) (rh + (size_t)(k) * n)
+#define TAU(i, j) taum[(i) + (size_t)(j) * (nl + 1)]
+  conv_t c;
+  int itx = 0, rc = 0;
+  double rho, rho_old, alpha, beta, omega;
+  if (init_conv(&c, istop, itmax, eps, n, irp, ja, val, b, x)) { rc = 1; goto done; }
+  for (;;) {
+    if (itx >= itmax) break;
+    int conv = 0;
+    or_axpby(n, 1.0, b, 0.0, r);
+    or_csr_csmv('N', n, n, irp, ja, val, -1.0, x, 1.0, r);
+    prec_apply(n, dinv, r, tmp);
+    memcpy(r, tmp, sizeof(double) * n);
+    or_axpby(n, 1.0, r, 0.0, rt0);
+    or_axpby(n, 1.0, r, 0.0, RH(0));
+    or_axpby(n, 0.0, r, 0.0, UH(0));
+    rho = 1.0;
+    alpha = 0.0;
+    omega = 1.0;
+    if (check_conv(&c, itx, n, x, r)) break;
+    if (res_hist) res_hist[itx] = end_err(&c);
+    for (;;) {
+      itx += nl;
+      rho = -omega * rho;
+      int brk = 0;
+      for (int j = 0; j < nl; j++) {
+        rho_old = rho;
+        rho = or_dot(n, RH(j), rt0);
+        if (rho == 0.0) { brk = 1; break; }
+        beta = alpha * rho / rho_old;
+        rho_old = rho;
+        for (int k = 0; k <= j; k++) or_axpby(n, 1.0, RH(k), -beta, UH(k));
+        or_csr_csmv('N', n, n, irp, ja, val, 1.0, UH(j), 0.0, UH(j + 1));
+        prec_apply(n, dinv, UH(j + 1), tmp);
+        memcpy(UH(j + 1), tmp, sizeof(double) * n);
+        gamma[j] = or_dot(n, UH(j + 1), rt0);
+        if (gamma[j] == 0.0) { brk = 1; break; }
+        alpha = rho / gamma[j];
+        for (int k = 0; k <= j; k++) or_axpby(n, -alpha, UH(k + 1), 1.0, RH(k));
+        or_axpby(n, alpha, UH(0), 1.0, x);
+        or_csr_csmv('N', n, n, irp, ja, val, 1.0, RH(j), 0.0, RH(j + 1));
+        prec_apply(n, dinv, RH(j + 1), tmp);
+        memcpy(RH(j + 1), tmp, sizeof(double) * n);
+      }
+      if (brk) break;
+      for (int j = 1; j <= nl; j++) {
+        for (int i = 1; i <= j - 1; i++) {
+          TAU(i, j) = or_dot(n, RH(i), RH(j));
+          TAU(i, j) = TAU(i, j) / sigma[i];
+          or_axpby(n, -TAU(i, j), RH(i), 1.0, RH(j));
+        }
+        sigma[j] = or_dot(n, RH(j), RH(j));
+        gamma1[j] = or_dot(n, RH(0), RH(j));
+        gamma1[j] = gamma1[j] / sigma[j];
+      }
+      gamma[nl] = gamma1[nl];
+      omega = gamma[nl];
+      for (int j = nl - 1; j >= 1; j--) {
+        gamma[j] = gamma1[j];
+        for (int i = j + 1; i <= nl; i++) gamma[j] = gamma[j] - TAU(j, i) * gamma[i];
+      }
+      for (int j = 1; j <= nl - 1; j++) {
+        gamma2[j] = gamma[j + 1];
+        for (int i = j + 1; i <= nl - 1; i++) gamma2[j] = gamma2[j] + TAU(j, i) * gamma[i + 1];
+      }
+      or_axpby(n, gamma[1], RH(0), 1.0, x);
+      or_axpby(n, -gamma1[nl], RH(nl), 1.0, RH(0));
+      or_axpby(n, -gamma[nl], UH(nl), 1.0, UH(0));
+      for (int j = 1; j <= nl - 1; j++) {
+        or_axpby(n, -gamma[j], UH(j), 1.0, UH(0));
+        or_axpby(n, gamma2[j], RH(j), 1.0, x);
+        or_axpby(n, -gamma1[j], RH(j), 1.0, RH(0));
+      }
+      int stop = check_conv(&c, itx, n, x, RH(0));
+      if (res_hist && itx <= itmax) res_hist[itx] = end_err(&c);
+      if (stop) { conv = 1; break; }
+    }
+    if (conv) break;
+  }
+  *iter = itx;
+  *err = end_err(&c);
+done:
+#undef UH
+#undef RH
+#undef TAU
+  free(r); free(rt0); free(uh); free(rh); free(tmp); free(gamma); free(gamma1); free(gamma2); free(sigma);
+  free(taum);
+  return rc;
+}

@@ -89,6 +89,10 @@ int or_cgs(int n, const int *irp, const int *ja, const double *val,
 int or_bicg(int n, const int *irp, const int *ja, const double *val,
             const double *dinv, const double *b, double *x, double eps,
             int itmax, int istop, int *iter, double *err, double *res_hist);
+int or_bicgstabl(int n, const int *irp, const int *ja, const double *val,
+                 const double *dinv, const double *b, double *x, double eps,
+                 int itmax, int istop, int irst, int *iter, double *err,
+                 double *res_hist);
 void or_drotg(double *a, double *b, double *c, double *s);
 
 #ifdef __cplusplus

@@ -1,9 +1,10 @@
 // psbx_krylov.cu -- device-resident Krylov solvers with the diagonal
-// preconditioner: the psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|'RGMRES')
-// path of krylov/psb_dkrylov.f90:179-210, krylov/psb_dcg.F90:218-295,
-// psb_dfcg.F90, psb_dcgs.f90, psb_dbicg.f90, krylov/psb_dcgstab.f90:226-365,
-// psb_drgmres.f90, stop test krylov/psb_d_krylov_conv_mod.f90:205-356, prec
-// apply prec/impl/psb_d_diagprec_impl.f90:116.
+// preconditioner: the psb_krylov('CG'|'FCG'|'CGS'|'BICG'|'BICGSTAB'|
+// 'BICGSTABL'|'RGMRES') path of krylov/psb_dkrylov.f90:179-210,
+// krylov/psb_dcg.F90:218-295, psb_dfcg.F90, psb_dcgs.f90, psb_dbicg.f90,
+// krylov/psb_dcgstab.f90:226-365, psb_dcgstabl.f90, psb_drgmres.f90, stop
+// test krylov/psb_d_krylov_conv_mod.f90:205-356, prec apply
+// prec/impl/psb_d_diagprec_impl.f90:116.
 //
 // The reference runs one kernel per BLAS-1 call and brings every dot and
 // norm back to the host (3 blocking copies per CG iteration, 5 per
@@ -1215,6 +1216,201 @@ __global__ void __launch_bounds__(KT) k_bicg_update(KState *S, int n, const doub
   }
 }
 
+// ---------------------------------------------------------------- BiCGSTAB(L)
+// krylov/psb_dcgstabl.f90 with nl = irst, kernel by kernel: every axpby,
+// dot and preconditioned product of the reference is one small kernel whose
+// scalars live in device memory (LState), and one outer iteration (nl BiCG
+// steps + the minimal-residual part) is one CUDA graph.
+struct LState {
+  double rho, rho_old, alpha, beta, omega;
+  double *gamma, *gamma1, *gamma2, *sigma, *taum;  // [nl+1] each, taum [(nl+1)^2]
+  int nl;
+};
+
+// y = a*x + b*y with the special cases of psi_daxpby (psi_d_serial_impl.F90:
+// alpha == 0 reads no x, beta == 0 reads no y); a = ca * (*pa) when pa is
+// given, else ca; b likewise
+__global__ void __launch_bounds__(KT) k_l_axpby(KState *S, int n, const double *pa, double ca,
+                                                const double *__restrict__ x, const double *pb, double cb,
+                                                double *__restrict__ y) {
+  if (stopped(S)) return;
+  const double a = pa ? ca * *pa : ca, b = pb ? cb * *pb : cb;
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    if (a == 0.0) {
+      if (b == 0.0) y[i] = 0.0;
+      else if (b != 1.0) y[i] = rmul(b, y[i]);
+    } else if (b == 0.0) {
+      y[i] = rmul(a, x[i]);
+    } else {
+      y[i] = radd(rmul(a, x[i]), rmul(b, y[i]));
+    }
+  }
+}
+
+// y = M^-1 (A x): psb_spmm(1,a,x,0,y) followed by prec%apply(y) in place
+template <class View>
+__global__ void __launch_bounds__(KT) k_l_spmv(View A, KState *S, const double *__restrict__ x,
+                                               const double *__restrict__ dinv, double *__restrict__ y) {
+  if (stopped(S)) return;
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double t = row_dot(A, s, x);
+    const int i = out_row(A, s);
+    y[i] = prec(dinv, i, t);
+  }
+}
+
+enum { LOP_RHO = 0, LOP_GAMMA = 1, LOP_TAU = 2, LOP_SIGMA = 3 };
+
+// dot products and the scalar step that follows each one in the reference:
+//   LOP_RHO    rho_old = rho; rho = (a,b); rho == 0 -> restart;
+//              beta = alpha*rho/rho_old; rho_old = rho
+//   LOP_GAMMA  gamma(j) = (a,b); == 0 -> restart; alpha = rho/gamma(j)
+//   LOP_TAU    taum(i,j) = (a,b) / sigma(i)
+//   LOP_SIGMA  sigma(j) = (a,a); gamma1(j) = (c,a) / sigma(j)   (c = rh(0))
+__global__ void __launch_bounds__(KT) k_l_dot(KState *S, LState *L, int op, int i, int j, int n,
+                                              const double *__restrict__ a, const double *__restrict__ b,
+                                              const double *__restrict__ c, double *__restrict__ part,
+                                              unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[128];
+  if (stopped(S)) return;
+  dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  for (int k = blockIdx.x * KT + threadIdx.x; k < n; k += gridDim.x * KT) {
+    const double ak = a[k];
+    dd_add_prod(acc[0], ak, op == LOP_SIGMA ? ak : b[k]);
+    if (op == LOP_SIGMA) dd_add_prod(acc[1], c[k], ak);
+  }
+  block_sum_dd<2>(acc, sm);
+  publish_sums<2>(part, grid, acc);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[2];
+    final_sum_dd<2>(part, grid, gridDim.x, o, sm);
+    if (threadIdx.x == 0) {
+      const double d = dd_value(o[0]);
+      const int ld = L->nl + 1;
+      if (op == LOP_RHO) {
+        L->rho_old = L->rho;
+        L->rho = d;
+        if (d == 0.0) {
+          S->status = ST_BREAK;
+        } else {
+          L->beta = L->alpha * L->rho / L->rho_old;
+          L->rho_old = L->rho;
+        }
+      } else if (op == LOP_GAMMA) {
+        L->gamma[j] = d;
+        if (d == 0.0) S->status = ST_BREAK;
+        else L->alpha = L->rho / d;
+      } else if (op == LOP_TAU) {
+        L->taum[i + (size_t)j * ld] = d / L->sigma[i];
+      } else {
+        L->sigma[j] = d;
+        L->gamma1[j] = dd_value(o[1]) / d;
+      }
+      *ticket = 0;
+    }
+  }
+}
+
+// top of an outer iteration: itx += nl ; rho = -omega*rho
+__global__ void k_l_top(KState *S, LState *L) {
+  if (threadIdx.x != 0 || stopped(S)) return;
+  S->itx += L->nl;
+  L->rho = -L->omega * L->rho;
+}
+
+// the minimal-residual recurrences of gamma, omega and gamma2
+__global__ void k_l_mr(KState *S, LState *L) {
+  if (threadIdx.x != 0 || stopped(S)) return;
+  const int nl = L->nl, ld = nl + 1;
+  double *g = L->gamma, *g1 = L->gamma1, *g2 = L->gamma2, *tau = L->taum;
+  g[nl] = g1[nl];
+  L->omega = g[nl];
+  for (int j = nl - 1; j >= 1; j--) {
+    g[j] = g1[j];
+    for (int i = j + 1; i <= nl; i++) g[j] = radd(g[j], -rmul(tau[j + (size_t)i * ld], g[i]));
+  }
+  for (int j = 1; j <= nl - 1; j++) {
+    g2[j] = g[j + 1];
+    for (int i = j + 1; i <= nl - 1; i++) g2[j] = radd(g2[j], rmul(tau[j + (size_t)i * ld], g[i + 1]));
+  }
+}
+
+// restart: r = M^-1 (b - A x) ; rt0 = rh(0) = r ; uh(0) = 0 ; rho = 1,
+// alpha = 0, omega = 1 ; stop test on r (no itx increment)
+template <class View>
+__global__ void __launch_bounds__(KT) k_l_init(View A, KState *S, LState *L, const double *__restrict__ b,
+                                               const double *__restrict__ x, const double *__restrict__ dinv,
+                                               double *__restrict__ rt0, double *__restrict__ rh0,
+                                               double *__restrict__ uh0, double *__restrict__ part,
+                                               unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[192];
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int s = blockIdx.x * KT + threadIdx.x; s < A.rows; s += gridDim.x * KT) {
+    const double ax = row_dot(A, s, x);
+    const int i = out_row(A, s);
+    const double ri = prec(dinv, i, radd(rmul(-1.0, ax), b[i]));
+    rt0[i] = ri;
+    rh0[i] = ri;
+    uh0[i] = 0.0;
+    dd_add_prod(acc[0], ri, ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(ld_ro(x + i)));
+  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      const double rr = dd_value(o[0]);
+      if (S->istop == 3 && !S->r0set) {  // psb_init_conv runs once, before the restart loop
+        S->r0n2 = sqrt(rr);
+        S->r0set = 1;
+      }
+      L->rho = 1.0;
+      L->alpha = 0.0;
+      L->omega = 1.0;
+      S->status = check_conv(S, rr, m[0], m[1]) ? ST_DONE : ST_RUN;
+      *ticket = 0;
+    }
+  }
+}
+
+// stop test on (x, rh(0)) at the end of an outer iteration
+__global__ void __launch_bounds__(KT) k_l_check(KState *S, int n, const double *__restrict__ x,
+                                                const double *__restrict__ r, double *__restrict__ part,
+                                                unsigned *__restrict__ ticket, int grid) {
+  __shared__ double sm[192];
+  if (stopped(S)) return;
+  dd_t acc[1] = {{0.0, 0.0}};
+  double mx[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * KT + threadIdx.x; i < n; i += gridDim.x * KT) {
+    const double ri = r[i];
+    dd_add_prod(acc[0], ri, ri);
+    mx[0] = fmax(mx[0], fabs(ri));
+    mx[1] = fmax(mx[1], fabs(x[i]));
+  }
+  block_sum_dd<1>(acc, sm);
+  block_max<2>(mx, sm + 128);
+  publish_sums<1>(part, grid, acc);
+  publish_max2(part, grid, mx);
+  if (psbx_last_block(ticket, gridDim.x)) {
+    dd_t o[1];
+    double m[2];
+    final_sum_dd<1>(part, grid, gridDim.x, o, sm);
+    final_max2(part, grid, gridDim.x, m, sm + 128);
+    if (threadIdx.x == 0) {
+      if (check_conv(S, dd_value(o[0]), m[0], m[1])) S->status = ST_DONE;
+      *ticket = 0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- prec build
 // psb_d_diag_precbld (prec/impl/psb_d_diagprec_impl.f90:229-292) with the
 // diagonal of psb_d_hll_get_diag (ext/impl/psb_d_hll_get_diag.f90:89-107):
@@ -1883,12 +2079,160 @@ static int solve_bicg(const View &A, void *mat, int fmt, const double *dinv, con
   return rc;
 }
 
+// BiCGSTAB(L) driver: the restart kernel on the host loop, then one graph
+// per outer iteration (nl BiCG steps, the minimal-residual part, the stop
+// test), replayed until the status changes.
+template <class View>
+static int solve_bicgstabl(const View &A, const double *dinv, const double *b, double *x, int n,
+                           psbx_SolverOptions *opt) {
+  PsbxCtx &c = psbx_ctx();
+  cudaStream_t st = c.stream;
+  const int nl = opt->irst, ld = nl + 1;
+  int grid = (n + KT - 1) / KT;
+  if (grid > c.sms * 8) grid = c.sms * 8;
+  if (grid < 1) grid = 1;
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  double *vec = nullptr, *part = nullptr, *small = nullptr;
+  KState *S = nullptr;
+  LState *L = nullptr;
+  unsigned *ticket = nullptr;
+  // rt0, uh(0..nl), rh(0..nl)
+  const size_t nv = 1 + 2 * (size_t)ld;
+  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * nv * nn, st));
+  PSBX_CK(cudaMallocAsync(&small, sizeof(double) * (4 * (size_t)ld + (size_t)ld * ld), st));
+  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
+  PSBX_CK(cudaMallocAsync(&L, sizeof(LState), st));
+  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
+  PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * nv * nn, st));
+  PSBX_CK(cudaMemsetAsync(small, 0, sizeof(double) * (4 * (size_t)ld + (size_t)ld * ld), st));
+  KState *hS = (KState *)c.h_res;
+  KState init;
+  memset(&init, 0, sizeof(init));
+  init.eps = opt->eps;
+  init.itmax = opt->itmax;
+  init.istop = opt->istop;
+  init.status = ST_RUN;
+  PSBX_CK(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, st));
+  LState hl;
+  memset(&hl, 0, sizeof(hl));
+  hl.gamma = small;
+  hl.gamma1 = small + ld;
+  hl.gamma2 = small + 2 * ld;
+  hl.sigma = small + 3 * ld;
+  hl.taum = small + 4 * ld;
+  hl.nl = nl;
+  PSBX_CK(cudaMemcpyAsync(L, &hl, sizeof(LState), cudaMemcpyHostToDevice, st));
+  double *rt0 = vec;
+  auto UH = [&](int k) { return vec + (1 + (size_t)k) * nn; };
+  auto RH = [&](int k) { return vec + (1 + (size_t)ld + k) * nn; };
+  const double *Lbeta = &L->beta, *Lalpha = &L->alpha;
+
+  k_kry_setup<<<grid, KT, 0, st>>>(n, b, S, part, ticket, grid);
+  psbx_count_launch();
+  if (opt->istop == 1) {
+    k_kry_normi<View><<<grid, KT, 0, st>>>(A, S, part, ticket, grid);
+    psbx_count_launch();
+  }
+  int rc = SPGPU_SUCCESS, per_graph = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
+  if (!rc) {
+    auto spmv = [&](const double *in, double *out) {
+      psbx_long_rows(A, in, &S->status, st);
+      k_l_spmv<View><<<grid, KT, 0, st>>>(A, S, in, dinv, out);
+      per_graph += 1 + long_launch(A);
+    };
+    auto axpby = [&](const double *pa, double ca, const double *xx, const double *pb, double cb, double *yy) {
+      k_l_axpby<<<grid, KT, 0, st>>>(S, n, pa, ca, xx, pb, cb, yy);
+      per_graph++;
+    };
+    auto dot = [&](int op, int i, int j, const double *a, const double *bb, const double *cc) {
+      k_l_dot<<<grid, KT, 0, st>>>(S, L, op, i, j, n, a, bb, cc, part, ticket, grid);
+      per_graph++;
+    };
+    k_l_top<<<1, 32, 0, st>>>(S, L);
+    per_graph++;
+    for (int j = 0; j < nl; j++) {
+      dot(LOP_RHO, 0, j, RH(j), rt0, nullptr);
+      for (int k = 0; k <= j; k++) axpby(nullptr, 1.0, RH(k), Lbeta, -1.0, UH(k));
+      spmv(UH(j), UH(j + 1));
+      dot(LOP_GAMMA, 0, j, UH(j + 1), rt0, nullptr);
+      for (int k = 0; k <= j; k++) axpby(Lalpha, -1.0, UH(k + 1), nullptr, 1.0, RH(k));
+      axpby(Lalpha, 1.0, UH(0), nullptr, 1.0, x);
+      spmv(RH(j), RH(j + 1));
+    }
+    for (int j = 1; j <= nl; j++) {
+      for (int i = 1; i <= j - 1; i++) {
+        dot(LOP_TAU, i, j, RH(i), RH(j), nullptr);
+        axpby(hl.taum + i + (size_t)j * ld, -1.0, RH(i), nullptr, 1.0, RH(j));
+      }
+      dot(LOP_SIGMA, 0, j, RH(j), nullptr, RH(0));
+    }
+    k_l_mr<<<1, 32, 0, st>>>(S, L);
+    per_graph++;
+    axpby(hl.gamma + 1, 1.0, RH(0), nullptr, 1.0, x);
+    axpby(hl.gamma1 + nl, -1.0, RH(nl), nullptr, 1.0, RH(0));
+    axpby(hl.gamma + nl, -1.0, UH(nl), nullptr, 1.0, UH(0));
+    for (int j = 1; j <= nl - 1; j++) {
+      axpby(hl.gamma + j, -1.0, UH(j), nullptr, 1.0, UH(0));
+      axpby(hl.gamma2 + j, 1.0, RH(j), nullptr, 1.0, x);
+      axpby(hl.gamma1 + j, -1.0, RH(j), nullptr, 1.0, RH(0));
+    }
+    k_l_check<<<grid, KT, 0, st>>>(S, n, x, RH(0), part, ticket, grid);
+    per_graph++;
+    e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "EndCapture");
+  }
+  if (!rc) {
+    e = cudaGraphInstantiate(&gexec, graph, 0);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+  }
+  auto fetch = [&]() -> int {
+    PSBX_CK(cudaMemcpyAsync(hS, S, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    return SPGPU_SUCCESS;
+  };
+  if (!rc) rc = fetch();
+  // restart loop of psb_dcgstabl.f90
+  while (!rc) {
+    if (hS->itx >= opt->itmax) break;
+    if ((rc = psbx_long_rows(A, x, nullptr, st))) break;
+    k_l_init<View><<<grid, KT, 0, st>>>(A, S, L, b, x, dinv, rt0, RH(0), UH(0), part, ticket, grid);
+    psbx_count_launch(1 + long_launch(A));
+    if ((rc = fetch())) break;
+    if (hS->status == ST_DONE) break;
+    rc = replay_until(gexec, st, per_graph, S, hS, [](const KState &k) { return k.status == ST_RUN; });
+    if (rc || hS->status == ST_DONE) break;
+    // ST_BREAK (rho or gamma(j) == 0): back to the restart
+  }
+  if (!rc) {
+    opt->iter = hS->itx;
+    opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(small, st);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(S, st);
+  cudaFreeAsync(L, st);
+  cudaFreeAsync(ticket, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (!rc && e2 != cudaSuccess) rc = psbx_cuda_status(e2, "solve_bicgstabl");
+  return rc;
+}
+
 template <class View>
 static int run_method(int meth, const View &A, const double *dinv, const double *b, double *x, int n,
                       psbx_SolverOptions *opt) {
   if (meth == 2) return solve_fcg(A, dinv, b, x, n, opt);
   if (meth == 3) return solve_gmres(A, dinv, b, x, n, opt);
   if (meth == 4) return solve_cgs(A, dinv, b, x, n, opt);
+  if (meth == 6) return solve_bicgstabl(A, dinv, b, x, n, opt);
   return solve(A, meth == 1, dinv, b, x, n, opt);
 }
 
@@ -1897,7 +2241,7 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
   int rc = psbx_ensure_init();
   if (rc) return rc;
   if (!method || !mat || !b || !x || !opt) return SPGPU_UNSUPPORTED;
-  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES, 4 CGS, 5 BICG (psb_dkrylov.f90:179-210)
+  // 0 CG, 1 BICGSTAB, 2 FCG, 3 RGMRES, 4 CGS, 5 BICG, 6 BICGSTABL (psb_dkrylov.f90:179-210)
   int meth;
   if (!strcasecmp(method, "CG")) meth = 0;
   else if (!strcasecmp(method, "BICGSTAB")) meth = 1;
@@ -1905,11 +2249,13 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
   else if (!strcasecmp(method, "RGMRES") || !strcasecmp(method, "GMRES")) meth = 3;
   else if (!strcasecmp(method, "CGS")) meth = 4;
   else if (!strcasecmp(method, "BICG")) meth = 5;
+  else if (!strcasecmp(method, "BICGSTABL")) meth = 6;
   else return SPGPU_UNSUPPORTED;  // other methods are outside this library
   if (opt->istop < 1 || opt->istop > 3) return SPGPU_UNSUPPORTED;  // psb_err_invalid_istop_
   // RGMRES: the reference accepts istop 1 and 2 (psb_drgmres.f90); istop 1
   // is not provided here, and irst must be positive (psb_err_invalid_irst_)
   if (meth == 3 && (opt->istop != 2 || opt->irst <= 0)) return SPGPU_UNSUPPORTED;
+  if (meth == 6 && opt->irst <= 0) return SPGPU_UNSUPPORTED;  // psb_err_invalid_irst_
   MultiVectDevice *B = (MultiVectDevice *)b, *X = (MultiVectDevice *)x, *D = (MultiVectDevice *)dinv;
   const int n = mat_rows(mat, fmt);
   if (n < 0 || B->size_ < n || X->size_ < n || (D && D->size_ < n)) return SPGPU_UNSUPPORTED;

@@ -94,7 +94,7 @@ def test_cg_no_prec_and_itmax(psb):
 def test_zero_rhs_returns_at_once(psb):
     irp, ja, va = gen.poisson7(8)
     n = len(irp) - 1
-    for method in ("CG", "BICGSTAB", "FCG", "RGMRES", "CGS", "BICG"):
+    for method in ("CG", "BICGSTAB", "FCG", "RGMRES", "CGS", "BICG", "BICGSTABL"):
         (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, ja, va, np.zeros(n))
         assert np.all(x == 0)
         assert it == ito
@@ -166,7 +166,7 @@ def test_itmax_fcg_and_rgmres(psb):
     assert abs(err - erro) <= 1e-6 * erro
 
 
-@pytest.mark.parametrize("method", ["CG", "FCG", "CGS", "BICG", "BICGSTAB", "RGMRES"])
+@pytest.mark.parametrize("method", ["CG", "FCG", "CGS", "BICG", "BICGSTAB", "BICGSTABL", "RGMRES"])
 def test_wide_hacks_in_solvers(psb, method):
     """Row-sorted SPD power-law matrix whose leading hacks are wider than 256
     (summed by a block each before every product): every method matches the
@@ -196,3 +196,19 @@ def test_cgs_bicg_c1(psb, method, istop, fmt):
     assert abs(it - ito) <= 2, (it, ito)
     assert err <= 1e-9
     assert np.max(np.abs(x - xo)) <= 1e-6
+
+
+@pytest.mark.parametrize("irst", [1, 2, 4])
+@pytest.mark.parametrize("istop", [1, 2])
+def test_bicgstabl_c1(psb, irst, istop):
+    """BiCGSTAB(L) (psb_dcgstabl.f90, L = irst, left preconditioned, stop test
+    on the preconditioned residual) on the C1-type operator: iterations
+    within +-2 of the oracle (they move in steps of L), tolerance reached,
+    x equal to the oracle's to 1e-8."""
+    irp, ja, va = gen.pde3d(20, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    b = O.csr_csmv(irp, ja, va, 1.0, np.ones(n), 0.0, np.zeros(n))
+    (x, it, err), (xo, ito, erro) = _solve_both(psb, "BICGSTABL", irp, ja, va, b, eps=1e-9, istop=istop, irst=irst)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-9
+    assert np.max(np.abs(x - xo)) <= 1e-8
