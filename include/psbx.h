@@ -339,6 +339,14 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
 int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, const double *d_dinv, double eps,
                    double inner_tol, int itmax, int *slot);
 int psbx_batch_step(void *eng, int replays, int *n_running);
+/* psbx_batch_step in two halves: launch enqueues the replays and the state
+ * read-back and returns at once (1 if a launch is already in flight); wait
+ * blocks until it is done.  Between them the host may read finished slots'
+ * solutions (their phase is done, so the running replays do not touch
+ * them), add requests and remove slots; adds and removes take effect at the
+ * next launch.  poll reports the state as of the last wait. */
+int psbx_batch_launch(void *eng, int replays);
+int psbx_batch_wait(void *eng, int *n_running);
 int psbx_batch_poll(void *eng, int slot, int *state, int *outer, int *iters, double *err);
 int psbx_batch_remove(void *eng, int slot);
 int psbx_batch_destroy(void *eng);

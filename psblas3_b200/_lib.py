@@ -97,6 +97,7 @@ _SIGS = {
     "psbx_batch_create": (I, [PP, I, I, I]),
     "psbx_batch_add": (I, [P, P, P, P, P, D, D, I, PI]),
     "psbx_batch_step": (I, [P, I, PI]),
+    "psbx_batch_launch": (I, [P, I]), "psbx_batch_wait": (I, [P, PI]),
     "psbx_batch_poll": (I, [P, I, PI, PI, PI, PD]),
     "psbx_batch_remove": (I, [P, I]),
     "psbx_batch_destroy": (I, [P]),

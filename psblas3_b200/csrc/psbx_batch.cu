@@ -93,6 +93,15 @@ struct Eng {
   cudaGraph_t graph = nullptr;
   BState *h_state_pinned = nullptr;
   BSol *h_sol_pinned = nullptr;
+  bool dirty = false;         // slots joined or left since the tile table was uploaded
+  cudaEvent_t done_ev = nullptr;  // end of the last launch's state readback
+  bool inflight = false;
+  // pinned staging of the tables (no wait for the copies: the next upload
+  // comes after a wait, which orders it after them)
+  BTile *h_tiles_pinned = nullptr;
+  int h_tiles_cap = 0;
+  BSys *h_sys_pinned = nullptr;
+  BCtl *h_ctl_pinned = nullptr;
 };
 
 // --------------------------------------------------------------- helpers
@@ -924,18 +933,29 @@ static int upload_tables(Eng *e, cudaStream_t st) {
     e->d_part = np_;
     e->max_tiles = cap;
   }
-  BCtl c;
+  if ((int)tiles.size() > e->h_tiles_cap) {
+    PSBX_CK(cudaStreamSynchronize(st));  // the old staging buffer may still be read
+    cudaFreeHost(e->h_tiles_pinned);
+    e->h_tiles_pinned = nullptr;
+    e->h_tiles_cap = 0;
+    const int cap = (int)tiles.size() * 2;
+    PSBX_CK(cudaHostAlloc(&e->h_tiles_pinned, sizeof(BTile) * cap, 0));
+    e->h_tiles_cap = cap;
+  }
+  BCtl &c = *e->h_ctl_pinned;
   memset(&c, 0, sizeof(c));
   c.ntiles = (int)tiles.size();
   c.cap = e->max_tiles;
   c.tiles = e->d_tiles;
   c.part = e->d_part;
   c.count = e->d_count;
-  if (!tiles.empty())
-    PSBX_CK(cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(BTile) * tiles.size(), cudaMemcpyHostToDevice, st));
-  PSBX_CK(cudaMemcpyAsync(e->d_sys, e->h_sys.data(), sizeof(BSys) * e->max_sys, cudaMemcpyHostToDevice, st));
-  PSBX_CK(cudaMemcpyAsync(e->d_ctl, &c, sizeof(BCtl), cudaMemcpyHostToDevice, st));
-  PSBX_CK(cudaStreamSynchronize(st));  // the host vectors above are reused
+  if (!tiles.empty()) {
+    memcpy(e->h_tiles_pinned, tiles.data(), sizeof(BTile) * tiles.size());
+    PSBX_CK(cudaMemcpyAsync(e->d_tiles, e->h_tiles_pinned, sizeof(BTile) * tiles.size(), cudaMemcpyHostToDevice, st));
+  }
+  memcpy(e->h_sys_pinned, e->h_sys.data(), sizeof(BSys) * e->max_sys);
+  PSBX_CK(cudaMemcpyAsync(e->d_sys, e->h_sys_pinned, sizeof(BSys) * e->max_sys, cudaMemcpyHostToDevice, st));
+  PSBX_CK(cudaMemcpyAsync(e->d_ctl, e->h_ctl_pinned, sizeof(BCtl), cudaMemcpyHostToDevice, st));
   return SPGPU_SUCCESS;
 }
 
@@ -968,6 +988,9 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   if (err == cudaSuccess) err = cudaMalloc(&e->d_count, sizeof(int) * 8);
   if (err == cudaSuccess) err = cudaMemsetAsync(e->d_count, 0, sizeof(int) * 8, c.stream);
   if (err == cudaSuccess) err = cudaMalloc(&e->d_part, sizeof(double) * 2 * MAXK * (size_t)e->max_tiles);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->done_ev, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sys_pinned, sizeof(BSys) * max_systems, 0);
+  if (err == cudaSuccess) err = cudaHostAlloc(&e->h_ctl_pinned, sizeof(BCtl), 0);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_state_pinned, sizeof(BState) * max_systems, 0);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sol_pinned, sizeof(BSol) * max_systems * nrhs, 0);
   if (err == cudaSuccess) err = cudaMemsetAsync(e->d_state, 0, sizeof(BState) * max_systems, c.stream);
@@ -1045,16 +1068,17 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   S.dinv = dv;
   S.rows = (int)n;
   S.sol0 = s * K;
-  {
+  if (m->leadLong < 0) {
     // leading run of rows longer than LONG_ROW (matrices whose rows are sorted
-    // by length put all their long rows there)
+    // by length put all their long rows there); kept on the matrix
     const int probe = n < 65536 ? (int)n : 65536;
     std::vector<int> irn(probe > 0 ? probe : 1);
     if (probe > 0) PSBX_CK(cudaMemcpy(irn.data(), m->rS, sizeof(int) * probe, cudaMemcpyDeviceToHost));
     int nl = 0;
     while (nl < probe && irn[nl] > LONG_ROW) nl++;
-    S.nlong = nl;
+    m->leadLong = nl;
   }
+  S.nlong = m->leadLong;
   kb_d2f_inv<<<psbx_grid_for(n, 256), 256, 0, c.stream>>>((int)n, d_dinv, dv);
   psbx_count_launch();
   std::vector<BSol> so(K);
@@ -1072,34 +1096,63 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   PSBX_CK(cudaMemcpyAsync(e->d_sol + (size_t)s * K, so.data(), sizeof(BSol) * K, cudaMemcpyHostToDevice, c.stream));
   kb_set_phase<<<1, 1, 0, c.stream>>>(e->d_state, e->d_count, s, PH_RESID);
   psbx_count_launch();
-  int rc = upload_tables(e, c.stream);
-  if (rc) return rc;
+  e->dirty = true;  // the tile table is rebuilt once, before the next step
+  // until the next step, poll reports the fresh state, not the slot's last occupant
+  memset(&e->h_state_pinned[s], 0, sizeof(BState));
+  e->h_state_pinned[s].phase = PH_RESID;
+  memcpy(e->h_sol_pinned + (size_t)s * K, so.data(), sizeof(BSol) * K);
   *slot = s;
   return SPGPU_SUCCESS;
 }
 
-// Runs `replays` replays of the captured batch (ITERS iterations each) and
-// returns how many slots are still running in *n_running.
-int psbx_batch_step(void *eng, int replays, int *n_running) {
+// Enqueues `replays` replays of the captured batch (ITERS iterations each)
+// and the read-back of every slot's state, and returns at once; the host can
+// prepare the next requests meanwhile.  psbx_batch_wait ends it.
+int psbx_batch_launch(void *eng, int replays) {
   Eng *e = (Eng *)eng;
-  if (!e) return SPGPU_UNSUPPORTED;
+  if (!e || e->inflight) return SPGPU_UNSUPPORTED;
   PsbxCtx &c = psbx_ctx();
   const int K = e->K;
+  if (e->dirty) {
+    int rc = upload_tables(e, c.stream);
+    if (rc) return rc;
+    e->dirty = false;
+  }
   for (int r = 0; r < replays; r++) {
     cudaError_t err = cudaGraphLaunch(e->gexec, c.stream);
-    if (err != cudaSuccess) return psbx_cuda_status(err, "psbx_batch_step");
+    if (err != cudaSuccess) return psbx_cuda_status(err, "psbx_batch_launch");
     psbx_count_launch(6 * ITERS);
   }
   PSBX_CK(cudaMemcpyAsync(e->h_state_pinned, e->d_state, sizeof(BState) * e->max_sys, cudaMemcpyDeviceToHost,
                           c.stream));
   PSBX_CK(cudaMemcpyAsync(e->h_sol_pinned, e->d_sol, sizeof(BSol) * e->max_sys * K, cudaMemcpyDeviceToHost,
                           c.stream));
-  PSBX_CK(cudaStreamSynchronize(c.stream));
+  PSBX_CK(cudaEventRecord(e->done_ev, c.stream));
+  e->inflight = true;
+  return SPGPU_SUCCESS;
+}
+
+// Waits for the last launch; *n_running = slots still running.
+int psbx_batch_wait(void *eng, int *n_running) {
+  Eng *e = (Eng *)eng;
+  if (!e) return SPGPU_UNSUPPORTED;
+  if (e->inflight) {
+    PSBX_CK(cudaEventSynchronize(e->done_ev));
+    e->inflight = false;
+  }
   int running = 0;
   for (int s = 0; s < e->max_sys; s++)
     if (e->used[s] && e->h_state_pinned[s].phase != PH_DONE) running++;
   if (n_running) *n_running = running;
   return SPGPU_SUCCESS;
+}
+
+// Runs `replays` replays of the captured batch (ITERS iterations each) and
+// returns how many slots are still running in *n_running.
+int psbx_batch_step(void *eng, int replays, int *n_running) {
+  int rc = psbx_batch_launch(eng, replays);
+  if (rc) return rc;
+  return psbx_batch_wait(eng, n_running);
 }
 
 // Status of a slot as of the last step: *state 0 running, 1 all rhs
@@ -1135,7 +1188,8 @@ int psbx_batch_remove(void *eng, int slot) {
   e->owned[slot] = nullptr;
   e->used[slot] = 0;
   memset(&e->h_sys[slot], 0, sizeof(BSys));
-  return upload_tables(e, c.stream);
+  e->dirty = true;  // its tiles leave the table before the next step (its phase is idle meanwhile)
+  return SPGPU_SUCCESS;
 }
 
 int psbx_batch_destroy(void *eng) {
@@ -1154,6 +1208,10 @@ int psbx_batch_destroy(void *eng) {
   cudaFree(e->d_ctl);
   cudaFree(e->d_count);
   cudaFree(e->d_part);
+  if (e->done_ev) cudaEventDestroy(e->done_ev);
+  cudaFreeHost(e->h_tiles_pinned);
+  cudaFreeHost(e->h_sys_pinned);
+  cudaFreeHost(e->h_ctl_pinned);
   cudaFreeHost(e->h_state_pinned);
   cudaFreeHost(e->h_sol_pinned);
   cudaStreamSynchronize(c.stream);

@@ -49,6 +49,7 @@ struct HllDevice {
   int nLong;
   double *lres;      // rows entries (storage order), allocated when nLong > 0
   int longW;         // 0: PSBX_LONG_W; < 0: never
+  int leadLong;      // batch engine: leading rows longer than 128 entries (-1 unknown)
 };
 
 // Default width above which a hack of 32 rows is summed by a whole block.

@@ -110,6 +110,7 @@ int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cu
 // allocates their row-sum buffer; called whenever an HLL object's arrays are
 // (re)written.
 int psbx_hll_index_long(HllDevice *m) {
+  m->leadLong = -1;  // the arrays changed: the batch engine's probe is redone
   cudaFree(m->longHacks);
   cudaFree(m->lres);
   m->longHacks = nullptr;

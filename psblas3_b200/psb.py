@@ -432,6 +432,16 @@ class BatchSolver:
         check(lib.psbx_batch_step(self.h, int(replays), C.byref(n)), "batch_step")
         return n.value
 
+    def launch(self, replays=1):
+        """Enqueue replays and the state read-back; returns at once."""
+        check(lib.psbx_batch_launch(self.h, int(replays)), "batch_launch")
+
+    def wait(self):
+        """Wait for the last launch; returns the number of running slots."""
+        n = C.c_int(0)
+        check(lib.psbx_batch_wait(self.h, C.byref(n)), "batch_wait")
+        return n.value
+
     def poll(self, slot):
         st, outer = C.c_int(0), C.c_int(0)
         its = (C.c_int * self.nrhs)()

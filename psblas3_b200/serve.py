@@ -55,7 +55,7 @@ def request_rhs(req, n):
     import torch
     g = torch.Generator(device="cuda")
     g.manual_seed(int(req.seed))
-    return torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 2.0 - 1.0
+    return torch.empty(n, dtype=torch.float64, device="cuda").uniform_(-1.0, 1.0, generator=g)
 
 
 class Request:
@@ -72,7 +72,7 @@ class Request:
 class Server:
     def __init__(self, pool, hbm_budget=150e9, max_slots=512, max_rows_total=200_000_000, inner_tol=1e-4,
                  itmax=200_000, replays_per_step=1, engine=None):
-        """engine: a psb.BatchSolver-like object (add/step/poll/remove/free);
+        """engine: a psb.BatchSolver-like object (add/launch/wait/poll/remove/free);
         by default a new 1-rhs batch engine with max_slots slots."""
         self.pool = pool
         self.budget = float(hbm_budget) - pool.device_bytes
@@ -86,13 +86,15 @@ class Server:
         self.rows_in_use = 0
         self.inner_tol, self.itmax = inner_tol, itmax
         self.replays = replays_per_step
+        self.inflight = False       # replays launched and not yet waited for
+        self.held = 0               # slots of finished requests not yet removed
 
     def submit(self, req):
         self.queue.append(req)
 
     def _admit(self, now):
         import torch
-        while self.queue and len(self.running) < self.max_slots:
+        while self.queue and len(self.running) + self.held < self.max_slots:
             req = self.queue[0]
             m = self.pool.mats[req.mat]
             need = m["n"] * BYTES_PER_ROW
@@ -108,16 +110,29 @@ class Server:
             self.in_use += need
             self.rows_in_use += m["n"]
 
-    def _reap(self, now):
+    def _collect(self):
+        """Requests whose solve ended, as of the last wait (removed from the
+        running set)."""
+        finished = []
         for slot in list(self.running):
             st, outer, its, err = self.eng.poll(slot)
             if st == 0:
                 continue
             req = self.running.pop(slot)
             req.state, req.outer, req.iters, req.err = st, outer, its[0], err[0]
+            finished.append(req)
+        return finished
+
+    def _retire(self, finished):
+        """Copy the finished solutions back to host arrays and free their slots
+        and memory (the slots' phase is done, so replays in flight do not
+        touch them)."""
+        for req in finished:
             req.x = req.dx.cpu().numpy()
+        now = time.perf_counter()
+        for req in finished:
             req.t_done = now
-            self.eng.remove(slot)
+            self.eng.remove(req.slot)
             m = self.pool.mats[req.mat]
             self.in_use -= m["n"] * BYTES_PER_ROW
             self.rows_in_use -= m["n"]
@@ -125,14 +140,29 @@ class Server:
             self.done.append(req)
 
     def step(self, now):
-        """Admit what fits, advance the running batch, retire finished ones."""
+        """One round: take the results of the replays in flight, admit what
+        fits, launch the next replays, and -- while the device runs them --
+        copy the finished solutions back and free their slots."""
+        finished = []
+        if self.inflight:
+            self.eng.wait()
+            self.inflight = False
+            finished = self._collect()
+        self.held = len(finished)  # their slots are freed only after the launch
         self._admit(now)
         if self.running:
-            self.eng.step(self.replays)
-            self._reap(time.perf_counter())
+            self.eng.launch(self.replays)
+            self.inflight = True
+        if finished:
+            self._retire(finished)
+        self.held = 0
+
+    @property
+    def busy(self):
+        return bool(self.queue or self.running or self.inflight)
 
     def drain(self, clock=time.perf_counter):
-        while self.queue or self.running:
+        while self.busy:
             self.step(clock())
 
     def close(self):
@@ -146,12 +176,12 @@ def run_stream(server, arrivals, clock=time.perf_counter):
     i = 0
     for r in arrivals:
         r.t_arrive = t0 + r.t_arrive
-    while i < len(arrivals) or server.queue or server.running:
+    while i < len(arrivals) or server.busy:
         now = clock()
         while i < len(arrivals) and arrivals[i].t_arrive <= now:
             server.submit(arrivals[i])
             i += 1
-        if not server.running and not server.queue and i < len(arrivals):
+        if not server.busy and i < len(arrivals):
             time.sleep(max(0.0, min(0.001, arrivals[i].t_arrive - now)))
             continue
         server.step(now)

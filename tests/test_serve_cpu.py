@@ -17,6 +17,8 @@ class FakeEngine:
 
     def add(self, A, db, dx, dinv, eps, inner_tol, itmax):
         s = min(set(range(len(self.slots) + 1)) - set(self.slots))
+        if getattr(self, "max_slots", None) is not None and len(self.slots) >= self.max_slots:
+            raise RuntimeError("no free slot")
         self.slots[s] = [0, A["n"] // 100, dx]
         self.log.append(("add", s, A["n"]))
         return s
@@ -27,6 +29,12 @@ class FakeEngine:
             if v[0] >= v[1]:
                 v[2].fill_(1.0)
         return sum(1 for v in self.slots.values() if v[0] < v[1])
+
+    def launch(self, replays=1):
+        self.pending = replays
+
+    def wait(self):
+        return self.step(self.pending)
 
     def poll(self, s):
         done, need, _ = self.slots[s]
@@ -47,8 +55,10 @@ class FakePool:
 
 def _server(sizes, budget_rows, max_slots=8, monkeypatch=None):
     monkeypatch.setattr(serve, "request_rhs", lambda req, n: torch.zeros(n, dtype=torch.float64))
+    eng = FakeEngine()
+    eng.max_slots = max_slots
     return serve.Server(FakePool(sizes), hbm_budget=budget_rows * serve.BYTES_PER_ROW, max_slots=max_slots,
-                        engine=FakeEngine())
+                        engine=eng)
 
 
 def test_fifo_admission_under_budget(monkeypatch):
@@ -111,3 +121,18 @@ def test_latency_stats():
     assert s["count"] == 100
     assert abs(s["p50_ms"] - 50.5) < 1e-9 and abs(s["p99_ms"] - 99.01) < 1e-9
     assert serve.latency_stats([]) == {}
+
+
+def test_finished_slots_count_until_retired(monkeypatch):
+    """With every slot taken, requests that finish in a round free their
+    slots only after the next launch: admission waits for them instead of
+    asking the engine for a slot it does not have."""
+    srv = _server([100] * 6, budget_rows=10**9, max_slots=2, monkeypatch=monkeypatch)
+    for i in range(6):
+        srv.submit(serve.Request(i, i, i, 1e-10, 0.0))
+    t = 0.0
+    while srv.busy:
+        srv.step(t)
+        assert len(srv.eng.slots) <= 2
+        t += 1.0
+    assert sorted(r.rid for r in srv.done) == list(range(6))
