@@ -102,6 +102,7 @@ struct Eng {
   int h_tiles_cap = 0;
   BSys *h_sys_pinned = nullptr;
   BCtl *h_ctl_pinned = nullptr;
+  BSol *h_sol_init = nullptr;  // pinned, per slot: the initial BSol of an add
 };
 
 // --------------------------------------------------------------- helpers
@@ -991,6 +992,7 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->done_ev, cudaEventDisableTiming);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sys_pinned, sizeof(BSys) * max_systems, 0);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_ctl_pinned, sizeof(BCtl), 0);
+  if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sol_init, sizeof(BSol) * max_systems * nrhs, 0);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_state_pinned, sizeof(BState) * max_systems, 0);
   if (err == cudaSuccess) err = cudaHostAlloc(&e->h_sol_pinned, sizeof(BSol) * max_systems * nrhs, 0);
   if (err == cudaSuccess) err = cudaMemsetAsync(e->d_state, 0, sizeof(BState) * max_systems, c.stream);
@@ -1093,7 +1095,10 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   e->h_sys[s] = S;
   e->used[s] = 1;
   e->owned[s] = buf;
-  PSBX_CK(cudaMemcpyAsync(e->d_sol + (size_t)s * K, so.data(), sizeof(BSol) * K, cudaMemcpyHostToDevice, c.stream));
+  // from pinned memory: a pageable copy would wait for the replays in flight
+  memcpy(e->h_sol_init + (size_t)s * K, so.data(), sizeof(BSol) * K);
+  PSBX_CK(cudaMemcpyAsync(e->d_sol + (size_t)s * K, e->h_sol_init + (size_t)s * K, sizeof(BSol) * K,
+                          cudaMemcpyHostToDevice, c.stream));
   kb_set_phase<<<1, 1, 0, c.stream>>>(e->d_state, e->d_count, s, PH_RESID);
   psbx_count_launch();
   e->dirty = true;  // the tile table is rebuilt once, before the next step
@@ -1212,6 +1217,7 @@ int psbx_batch_destroy(void *eng) {
   cudaFreeHost(e->h_tiles_pinned);
   cudaFreeHost(e->h_sys_pinned);
   cudaFreeHost(e->h_ctl_pinned);
+  cudaFreeHost(e->h_sol_init);
   cudaFreeHost(e->h_state_pinned);
   cudaFreeHost(e->h_sol_pinned);
   cudaStreamSynchronize(c.stream);

@@ -140,8 +140,9 @@ class Server:
             self.done.append(req)
 
     def step(self, now):
-        """One round: take the results of the replays in flight, admit what
-        fits, launch the next replays, and -- while the device runs them --
+        """One round: take the results of the replays in flight, launch the
+        next replays for the running requests, and -- while the device runs
+        them -- admit what fits (the new requests join at the next launch),
         copy the finished solutions back and free their slots."""
         finished = []
         if self.inflight:
@@ -149,8 +150,11 @@ class Server:
             self.inflight = False
             finished = self._collect()
         self.held = len(finished)  # their slots are freed only after the launch
-        self._admit(now)
         if self.running:
+            self.eng.launch(self.replays)
+            self.inflight = True
+        self._admit(now)
+        if not self.inflight and self.running:  # nothing was running: start at once
             self.eng.launch(self.replays)
             self.inflight = True
         if finished:
