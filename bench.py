@@ -593,7 +593,7 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
             "speedup_vs_fp64_one_at_a_time": (solves / tb) / (len(pairs) / t64)}
 
 
-def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0):
+def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0, replays_per_step=2):
     """C5: Poisson arrivals (rate per second, for `window` seconds) of solve
     requests drawn 50/50 from 3-D 7-point Poisson grids (side uniform in
     [10, 128]) and power-law unstructured SPD matrices (rows log-uniform in
@@ -630,7 +630,7 @@ def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0):
             break
         k = int(rng.integers(0, pool_each)) + (pool_each if rng.random() < 0.5 else 0)
         reqs.append(serve.Request(len(reqs), k, int(rng.integers(1 << 31)), 1e-10, t))
-    srv = serve.Server(pool, hbm_budget=150e9)
+    srv = serve.Server(pool, hbm_budget=150e9, replays_per_step=replays_per_step)
     l0 = psb.kernel_launches()
     wall = serve.run_stream(srv, reqs)
     launches = psb.kernel_launches() - l0
