@@ -122,13 +122,6 @@ template <int K> struct Occ {
   static constexpr int resid_blocks = K == 1 ? 4 : 2;
 };
 
-__device__ __forceinline__ void tile_range(int ntiles, int &t0, int &t1) {
-  // contiguous ranges of tiles per block (consecutive tiles of a system stay
-  // together); depends only on ntiles and the grid size
-  const long long per = ((long long)ntiles + gridDim.x - 1) / gridDim.x;
-  t0 = (int)min((long long)ntiles, per * blockIdx.x);
-  t1 = (int)min((long long)ntiles, per * (blockIdx.x + 1));
-}
 
 // A kernel whose phase no system is in returns after one load (instead of
 // walking the tile table); the finalisers move systems between phases and
@@ -437,11 +430,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys 
                                                                      BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
   if (phase_idle(ctl, PH_RESID)) return;
-  int t0, t1;
-  tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  for (int t = t0; t < t1; t++) {
+  const int ntiles = ctl->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_RESID) continue;
@@ -506,11 +498,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
   constexpr int RB = K == 1 ? 2 : 1;  // rows per thread whose loads are in flight together
   __shared__ double sm[32 * 2 * MAXK];
   if (phase_idle(ctl, PH_INIT)) return;
-  int t0, t1;
-  tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  for (int t = t0; t < t1; t++) {
+  const int ntiles = ctl->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_INIT) continue;
@@ -588,10 +579,9 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
                                                            const BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
   if (phase_idle(ctl, PH_INNER)) return;
-  int t0, t1;
-  tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
-  for (int t = t0; t < t1; t++) {
+  const int ntiles = ctl->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile T = tiles[t];
     if (state[T.sys].phase != PH_INNER) continue;
     const BSys &S = sys[T.sys];
@@ -649,11 +639,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *_
                                                               BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
   if (phase_idle(ctl, PH_INNER)) return;
-  int t0, t1;
-  tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  for (int t = t0; t < t1; t++) {
+  const int ntiles = ctl->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_INNER) continue;
@@ -704,11 +693,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
   constexpr int RB = K == 1 ? 4 : 1;
   __shared__ double sm[32 * 2 * MAXK];
   if (phase_idle(ctl, PH_INNER)) return;
-  int t0, t1;
-  tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
   double *part = ctl->part;
-  for (int t = t0; t < t1; t++) {
+  const int ntiles = ctl->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_INNER) continue;
@@ -806,10 +794,9 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__rest
                                                               const BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
   if (phase_idle(ctl, PH_XUPD)) return;
-  int t0, t1;
-  tile_range(ctl->ntiles, t0, t1);
   const BTile *__restrict__ tiles = ctl->tiles;
-  for (int t = t0; t < t1; t++) {
+  const int ntiles = ctl->ntiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile T = tiles[t];
     BState *st = state + T.sys;
     if (st->phase != PH_XUPD) continue;
