@@ -287,8 +287,9 @@ int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, int nnz,
 /* Autotuned device CSR -> HLL (the "autotuned hack size and threads per
  * row" of the GPU HLL SpMV; the reference fixes hksz = 32,
  * psb_d_cuda_cp_hlg_from_coo.F90:60): builds each candidate layout -- hack
- * size 32, 64 or 128 and, for hack size 32, the width above which a hack's
- * 32 rows are summed by a block of 256 threads (128, 256, 512, 1024 or
+ * size 32, 64 or 128 and, for hack size 32, the width above which a hack
+ * takes the wide path (its products formed by all blocks at once, then
+ * added in stored order by a warp per hack: 32, 64, 128, 256, 1024 or
  * never) -- times its SpMV on the library stream and keeps the fastest.
  * All candidates sum every row in stored order, so the products are the
  * same bits; *hksz, *wide_w (-1 never, 0 not applicable) and *ms (one SpMV)
@@ -298,6 +299,13 @@ int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int cols,
                                       const int *d_ja, const double *d_val,
                                       const int *d_perm, int *hksz,
                                       int *wide_w, double *ms);
+
+/* Sets the wide-hack threshold of a hack-32 HLL matrix built by this
+ * library (0: default -- 64 or four times the mean hack width, whichever is
+ * larger; < 0: never) and rebuilds its wide-hack lists.  Every threshold
+ * gives the same bits; only the time changes.  Returns SPGPU_UNSUPPORTED for
+ * another hack size unless wide_w is 0. */
+int psbx_hll_set_wide(void *deviceMat, int wide_w);
 
 /* Adds an FP32 copy of the values of an FP64 HLL handle (for the FP32 inner
  * iterations of the mixed-precision solver). */

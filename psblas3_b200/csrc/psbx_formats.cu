@@ -94,6 +94,9 @@ void freeHllDevice(void *deviceMat) {
   if (m->perm) cudaFree(m->perm);
   cudaFree(m->longHacks);
   cudaFree(m->lres);
+  cudaFree(m->wideBase);
+  cudaFree(m->wchunk);
+  cudaFree(m->wprod);
   free(m);
 }
 
@@ -902,8 +905,9 @@ int d_spmvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX, double beta,
 // Builds the HLL form of a device CSR matrix for each candidate layout and
 // keeps the one with the fastest SpMV (CUDA events on the library stream,
 // 2 warm-up and 5 timed products with x = 0): hack size 32, 64 or 128 and,
-// for hack size 32, the width above which a hack's rows are summed by a
-// whole block (threads per row 8 instead of 1): 128, 256, 512, 1024 or never.
+// for hack size 32, the width above which a hack takes the wide path
+// (products formed by all blocks at once, then added in order by a warp per
+// hack): 32, 64, 128, 256, 1024 or never.
 // Every candidate sums each row in stored order, so all give the same bits;
 // the choice changes time only.
 static int cst(cudaError_t e, const char *where) { return e == cudaSuccess ? 0 : psbx_cuda_status(e, where); }
@@ -943,12 +947,13 @@ extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int
   double best_ms = 0.0;
   int best_w = 0;
   static const int hks[] = {32, 64, 128};
-  static const int ws[] = {128, 256, 512, 1024, -1};
+  static const int ws[] = {32, 64, 128, 256, 1024, -1};
+  const int nws = (int)(sizeof(ws) / sizeof(ws[0]));
   for (int hi = 0; hi < 3 && !rc; hi++) {
     HllDevice *m = nullptr;
     rc = psbx_hll_from_csr_device((void **)&m, rows, cols, nnz, d_irp, d_ja, d_val, hks[hi], d_perm);
     if (rc) break;
-    const int nw = hks[hi] == 32 ? 5 : 1;
+    const int nw = hks[hi] == 32 ? nws : 1;
     int m_best_w = 0;
     double m_best = -1.0;
     for (int wi = 0; wi < nw && !rc; wi++) {
@@ -991,4 +996,17 @@ extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int
   if (wide_w) *wide_w = best->hackSize == 32 ? best_w : 0;
   if (ms) *ms = best_ms;
   return SPGPU_SUCCESS;
+}
+
+// Sets the wide-hack threshold of a hack-32 HLL matrix (0: default, < 0:
+// never) and rebuilds its wide-hack lists; results are the same bits for
+// every threshold.
+extern "C" int psbx_hll_set_wide(void *deviceMat, int wide_w) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m) return SPGPU_UNSUPPORTED;
+  if (m->hackSize != 32) return wide_w == 0 ? SPGPU_SUCCESS : SPGPU_UNSUPPORTED;
+  m->longW = wide_w;
+  return psbx_hll_index_long(m);
 }

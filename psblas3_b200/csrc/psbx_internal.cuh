@@ -42,18 +42,24 @@ struct HllDevice {
   float *cM32;       // optional FP32 copy of FP64 values (mixed precision)
   int *perm;         // optional storage-row -> matrix-row map (NULL: identity)
   int maxRowLen;     // longest stored row (-1: unknown)
-  // hacks wider than longW (hack size 32 only): their row sums are formed by
-  // a block per hack before each product (psbx_long_rows32) and read back
-  // from lres by the row kernels
+  // hacks wider than longW (hack size 32 only): their row sums are formed
+  // before each product (psbx_long_rows32: all products at once into wprod,
+  // then a warp per hack adds them in order) and read back from lres by the
+  // row kernels
   int *longHacks;    // hack ids, nLong of them
   int nLong;
   double *lres;      // rows entries (storage order), allocated when nLong > 0
-  int longW;         // 0: PSBX_LONG_W; < 0: never
+  int longW;         // 0: default (PSBX_LONG_W or 4x the mean hack width); < 0: never
+  int effW;          // the threshold the wide list was built with
   int leadLong;      // batch engine: leading rows longer than 128 entries (-1 unknown)
+  int *wideBase;     // nLong+1: offset of each wide hack's products in wprod
+  int *wchunk;       // 2*nWChunks: (wide hack index, first entry column) per product block
+  int nWChunks;
+  double *wprod;     // products of the wide hacks, laid out as their values
 };
 
-// Default width above which a hack of 32 rows is summed by a whole block.
-#define PSBX_LONG_W 256
+// Default width above which a hack of 32 rows takes the wide-hack path.
+#define PSBX_LONG_W 64
 
 struct EllDevice {
   void *cM;
@@ -357,6 +363,10 @@ struct HllView {
   const int *longHacks;  // hack size 32: hacks wider than longW
   const double *lres;    // their row sums, formed before the row kernel runs
   int nLong, longW;
+  const int *wideBase;   // wide hack i's products start at wprod + wideBase[i]
+  const int *wchunk;     // (wide hack index, first column) of each product block
+  double *wprod;
+  int nWChunks;
 };
 
 struct HllViewF {  // FP32 values, FP32 x
@@ -500,9 +510,9 @@ __device__ __forceinline__ int out_row(const CsrView &, int r) { return r; }
 HllView hll_view(const HllDevice *m);
 // Finds the wide hacks of a hack-32 matrix after its arrays are written.
 int psbx_hll_index_long(HllDevice *m);
-// Row sums of the wide hacks of a hack-32 matrix into lres, to be launched
-// before any row kernel that reads them with the same x; status (nullable)
-// makes it return at once when *status != 0.
+// Row sums of the wide hacks of a hack-32 matrix into lres (two launches), to
+// be launched before any row kernel that reads them with the same x; status
+// (nullable) makes the kernels return at once when *status != 0.
 int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cudaStream_t st);
 static inline Hll32View hll32_view(const HllView &v) {
   Hll32View w;

@@ -1478,10 +1478,10 @@ extern "C" int psbx_diag_prec_build(void *mat, int fmt, void *dinv) {
 // ---------------------------------------------------------------- driver
 #define KGRAPH_ITERS 8
 
-// 1 when the matrix has wide hacks, whose rows a separate kernel sums before
-// each product (psbx_long_rows); 0 otherwise.
+// 2 when the matrix has wide hacks, whose rows two kernels sum before each
+// product (psbx_long_rows); 0 otherwise.
 template <class View> static inline int long_launch(const View &) { return 0; }
-static inline int long_launch(const Hll32WView &) { return 1; }
+static inline int long_launch(const Hll32WView &) { return 2; }
 
 // Replays a captured batch of iterations until running(status) is false,
 // with 1, 2, 4, then 8 replays between two reads of the status word: a long

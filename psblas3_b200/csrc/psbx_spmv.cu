@@ -24,6 +24,7 @@
 // sequential sum only by rounding (checked against a tolerance).
 #include "psbx_internal.cuh"
 
+#include <algorithm>
 #include <vector>
 
 #define SPMV_T 256
@@ -45,93 +46,210 @@ HllView hll_view(const HllDevice *m) {
   v.longHacks = wide ? m->longHacks : nullptr;
   v.lres = wide ? m->lres : nullptr;
   v.nLong = wide ? m->nLong : 0;
-  v.longW = m->longW > 0 ? m->longW : PSBX_LONG_W;
+  v.longW = m->effW;  // the threshold the list was built with
+  v.wideBase = wide ? m->wideBase : nullptr;
+  v.wchunk = wide ? m->wchunk : nullptr;
+  v.wprod = wide ? m->wprod : nullptr;
+  v.nWChunks = wide ? m->nWChunks : 0;
   return v;
 }
 
 // --------------------------------------------------------------- wide hacks
-// A hack whose width exceeds longW would hold its warp for thousands
-// of dependent steps (the tail of a row-sorted power-law matrix).  One block
-// per such hack: in chunks of LONG_CH entries per row, all 256 threads load
-// the chunk's values and indices (entry j of the 32 rows is one contiguous
-// run) and form the products in shared memory, then lane r of warp 0 adds
-// row r's products in entry order from 0 -- the same roundings as the
-// thread-per-row sum, so results are unchanged bit for bit.
-#define LONG_CH 128
-__global__ void __launch_bounds__(256) k_hll_long(Hll32WView A, const double *__restrict__ x,
-                                                  double *__restrict__ lres, const int *status) {
+// A hack whose width exceeds longW would hold its warp for width/8 rounds of
+// two dependent memory latencies (the head of a row-sorted power-law matrix),
+// far longer than the rest of the product.  Its row sums are formed before
+// the row kernel in two launches:
+//  k_hll_wprod -- every product val*x(ja) of the wide hacks, WP_COLS entries
+//    of the hack's 32 rows per block, all blocks at once, stored in wprod in
+//    the values' layout (entry j of row r of wide hack i at wideBase[i]+32j+r);
+//  k_hll_wsum -- one warp per wide hack; lane r adds row r's products in
+//    entry order from 0, the same roundings as the thread-per-row sum, so
+//    results are unchanged bit for bit.  The products stream through a ring
+//    of WS_NBUF shared-memory buffers that cp.async fills WS_NBUF-1 chunks
+//    ahead, so only the additions are serial.
+#define WP_COLS 64
+#define WS_COLS 64
+#define WS_NBUF 6
+#define WS_WARPS 1
+#define WS_SMEM (WS_WARPS * WS_NBUF * WS_COLS * 32 * (int)sizeof(double))
+
+__global__ void __launch_bounds__(256) k_hll_wprod(Hll32WView A, const double *__restrict__ x, const int *status) {
   if (status && *((volatile const int *)status) != 0) return;
-  __shared__ double prod[LONG_CH * 32];
-  __shared__ int len[32];
-  const int h = A.longHacks[blockIdx.x];
+  const int i = A.wchunk[2 * blockIdx.x], c0 = A.wchunk[2 * blockIdx.x + 1];
+  const int h = A.longHacks[i];
   const int off = A.hkoffs[h];
-  const int width = (A.hkoffs[h + 1] - off) >> 5;
-  const int s = h * 32 + (threadIdx.x & 31);
-  if (threadIdx.x < 32) len[threadIdx.x] = s < A.rows ? A.irn[s] : 0;
-  __syncthreads();
+  const int r = threadIdx.x & 31;
+  const int s = h * 32 + r;
+  const int len = s < A.rows ? A.irn[s] : 0;
   const double *xb = x - A.base;
-  double acc = 0.0;
-  constexpr int PER = LONG_CH * 32 / 256;  // products per thread per chunk
-  for (int c0 = 0; c0 < width; c0 += LONG_CH) {
-    int c[PER];
-    double v[PER];
+  double *pb = A.wprod + A.wideBase[i];
+  constexpr int PER = WP_COLS * 32 / 256;  // entries per thread
+  int c[PER];
+  double v[PER];
 #pragma unroll
-    for (int u = 0; u < PER; u++) {
-      const int idx = threadIdx.x + u * 256;
-      const int j = c0 + (idx >> 5), r = idx & 31;
-      const bool ok = j < len[r];
-      const size_t p = (size_t)off + (size_t)j * 32 + r;
-      c[u] = ok ? ld_stream(A.ja + p) : A.base;
-      v[u] = ok ? ld_stream(A.val + p) : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < PER; u++) {
-      const int idx = threadIdx.x + u * 256;
-      if (c0 + (idx >> 5) < len[idx & 31]) prod[idx] = rmul(v[u], ld_ro(xb + c[u]));
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const int n = min(LONG_CH, len[threadIdx.x] - c0);
-      for (int k = 0; k < n; k++) acc = radd(acc, prod[k * 32 + threadIdx.x]);
-    }
-    __syncthreads();
+  for (int u = 0; u < PER; u++) {
+    const int j = c0 + (threadIdx.x >> 5) + 8 * u;
+    const bool ok = j < len;
+    const size_t p = (size_t)off + (size_t)j * 32 + r;
+    c[u] = ok ? ld_stream(A.ja + p) : A.base;
+    v[u] = ok ? ld_stream(A.val + p) : 0.0;
   }
-  if (threadIdx.x < 32 && s < A.rows) lres[s] = acc;
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int j = c0 + (threadIdx.x >> 5) + 8 * u;
+    if (j < len) pb[(size_t)j * 32 + r] = rmul(v[u], ld_ro(xb + c[u]));
+  }
+}
+
+// (no memory clobber: the ring is read only after the wait below, which has one)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(32 * WS_WARPS) k_hll_wsum(Hll32WView A, double *__restrict__ lres,
+                                                            const int *status) {
+  if (status && *((volatile const int *)status) != 0) return;
+  extern __shared__ __align__(16) double ring[];  // WS_WARPS rings of WS_NBUF chunks
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * WS_WARPS + w;
+  if (i >= A.nLong) return;  // whole warps only; the block has no barrier
+  const int h = A.longHacks[i];
+  const int width = (A.hkoffs[h + 1] - A.hkoffs[h]) >> 5;
+  const int s = h * 32 + lane;
+  const int len = s < A.rows ? A.irn[s] : 0;
+  const double *pb = A.wprod + A.wideBase[i];
+  double *buf = ring + (size_t)w * WS_NBUF * WS_COLS * 32;
+  const int nch = (width + WS_COLS - 1) / WS_COLS;
+  // chunk c = columns [c*WS_COLS, min(width, (c+1)*WS_COLS)): one contiguous
+  // run of 32 doubles per column, copied as 16-byte pieces (16 per column),
+  // piece k by lane k % 32; each chunk is one commit group
+  auto issue = [&](int c) {
+    if (c < nch) {
+      const double *src = pb + (size_t)c * WS_COLS * 32;
+      double *dst = buf + (c % WS_NBUF) * WS_COLS * 32;
+      const int npiece = min(WS_COLS, width - c * WS_COLS) * 16;
+      for (int k = lane; k < npiece; k += 32) cp_async16(dst + 2 * k, src + 2 * k);
+    }
+  };
+#pragma unroll
+  for (int c = 0; c < WS_NBUF - 1; c++) {
+    issue(c);
+    cp_async_commit();
+  }
+  double acc = 0.0;
+  for (int c = 0; c < nch; c++) {
+    cp_async_wait<WS_NBUF - 2>();  // chunk c has landed (this lane's pieces)
+    __syncwarp();                  // ... every lane's; and chunk c-1 is consumed
+    const double *b = buf + (c % WS_NBUF) * WS_COLS * 32 + lane;
+    const int n = min(WS_COLS, len - c * WS_COLS);
+    const int cn = c + WS_NBUF - 1;  // issued now, into chunk c-1's buffer
+    if (n == WS_COLS && (cn + 1) * WS_COLS <= width) {
+      // a whole chunk to add and a whole chunk to fetch: the copies are
+      // issued between the additions, in the cycles the add chain waits
+      const double *src = pb + (size_t)cn * WS_COLS * 32 + 2 * lane;
+      double *dst = buf + (cn % WS_NBUF) * WS_COLS * 32 + 2 * lane;
+      double t[WS_COLS];
+#pragma unroll
+      for (int u = 0; u < WS_COLS; u++) t[u] = b[u * 32];
+#pragma unroll
+      for (int u = 0; u < WS_COLS; u++) {
+        acc = radd(acc, t[u]);
+        if (u & 1) cp_async16(dst + 64 * (u >> 1), src + 64 * (u >> 1));
+      }
+    } else {
+      issue(cn);
+      int j = 0;
+      for (; j + 8 <= n; j += 8) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) t[u] = b[(j + u) * 32];
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc = radd(acc, t[u]);
+      }
+      for (; j < n; j++) acc = radd(acc, b[j * 32]);
+    }
+    cp_async_commit();
+  }
+  if (s < A.rows) lres[s] = acc;
 }
 
 int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cudaStream_t st) {
   if (A.nLong <= 0) return SPGPU_SUCCESS;
-  k_hll_long<<<A.nLong, 256, 0, st>>>(A, x, const_cast<double *>(A.lres), status);
-  PSBX_LAUNCH_CK("k_hll_long");
+  k_hll_wprod<<<A.nWChunks, 256, 0, st>>>(A, x, status);
+  PSBX_LAUNCH_CK("k_hll_wprod");
+  k_hll_wsum<<<(A.nLong + WS_WARPS - 1) / WS_WARPS, 32 * WS_WARPS, WS_SMEM, st>>>(A, const_cast<double *>(A.lres),
+                                                                                 status);
+  PSBX_LAUNCH_CK("k_hll_wsum");
   return SPGPU_SUCCESS;
 }
 
-// Lists the hacks wider than longW (hack size 32) from the offsets and
-// allocates their row-sum buffer; called whenever an HLL object's arrays are
-// (re)written.
+// Lists the hacks wider than the wide threshold (hack size 32) from the
+// offsets, with their product offsets and product blocks, and allocates the
+// product and row-sum buffers; called whenever an HLL object's arrays are
+// (re)written.  The default threshold is PSBX_LONG_W or four times the mean
+// hack width, whichever is larger: a matrix whose hacks are all about
+// equally wide keeps the thread-per-row sums (the extra product traffic
+// would cost more than the chains it saves).
 int psbx_hll_index_long(HllDevice *m) {
   m->leadLong = -1;  // the arrays changed: the batch engine's probe is redone
   cudaFree(m->longHacks);
   cudaFree(m->lres);
+  cudaFree(m->wideBase);
+  cudaFree(m->wchunk);
+  cudaFree(m->wprod);
   m->longHacks = nullptr;
   m->lres = nullptr;
+  m->wideBase = nullptr;
+  m->wchunk = nullptr;
+  m->wprod = nullptr;
   m->nLong = 0;
+  m->nWChunks = 0;
   if (m->hackSize != 32 || m->rows <= 0 || !m->hackOffs || m->longW < 0) return SPGPU_SUCCESS;
-  const int lw = m->longW > 0 ? m->longW : PSBX_LONG_W;
   const int nh = (m->rows + 31) / 32;
   PsbxCtx &c = psbx_ctx();
   std::vector<int> hk((size_t)nh + 1);
   PSBX_CK(cudaMemcpyAsync(hk.data(), m->hackOffs, sizeof(int) * ((size_t)nh + 1), cudaMemcpyDeviceToHost, c.stream));
   PSBX_CK(cudaStreamSynchronize(c.stream));
-  std::vector<int> wide;
+  int lw = m->longW;
+  if (lw == 0) {
+    const long long mean = ((long long)hk[nh] / 32 + nh - 1) / nh;
+    lw = (int)std::max<long long>(PSBX_LONG_W, 4 * mean);
+  }
+  m->effW = lw;
+  // widest first: their serial sums are the longest, so their warps start first
+  std::vector<int> list;
   for (int h = 0; h < nh; h++)
-    if (((hk[h + 1] - hk[h]) >> 5) > lw) wide.push_back(h);
+    if (((hk[h + 1] - hk[h]) >> 5) > lw) list.push_back(h);
+  std::stable_sort(list.begin(), list.end(), [&](int a, int b) { return hk[a + 1] - hk[a] > hk[b + 1] - hk[b]; });
+  std::vector<int> wide, base(1, 0), chunks;
+  for (int h : list) {
+    const int w = (hk[h + 1] - hk[h]) >> 5;
+    for (int c0 = 0; c0 < w; c0 += WP_COLS) {
+      chunks.push_back((int)wide.size());
+      chunks.push_back(c0);
+    }
+    wide.push_back(h);
+    base.push_back(base.back() + w * 32);
+  }
   if (wide.empty()) return SPGPU_SUCCESS;
   PSBX_CK(cudaMalloc(&m->longHacks, sizeof(int) * wide.size()));
   PSBX_CK(cudaMalloc(&m->lres, sizeof(double) * (size_t)m->rows));
+  PSBX_CK(cudaMalloc(&m->wideBase, sizeof(int) * base.size()));
+  PSBX_CK(cudaMalloc(&m->wchunk, sizeof(int) * chunks.size()));
+  PSBX_CK(cudaMalloc(&m->wprod, sizeof(double) * (size_t)base.back()));
   PSBX_CK(cudaMemcpyAsync(m->longHacks, wide.data(), sizeof(int) * wide.size(), cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaMemcpyAsync(m->wideBase, base.data(), sizeof(int) * base.size(), cudaMemcpyHostToDevice, c.stream));
+  PSBX_CK(cudaMemcpyAsync(m->wchunk, chunks.data(), sizeof(int) * chunks.size(), cudaMemcpyHostToDevice, c.stream));
   PSBX_CK(cudaStreamSynchronize(c.stream));
+  PSBX_CK(cudaFuncSetAttribute(k_hll_wsum, cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM));
   m->nLong = (int)wide.size();
+  m->nWChunks = (int)(chunks.size() / 2);
   return SPGPU_SUCCESS;
 }
 

@@ -42,7 +42,10 @@ def init(dev: int = 0) -> None:
 class DVect:
     """One (count=1) or several (count>1) FP64 device vectors."""
 
-    def __init__(self, n: int, count: int = 1, dtype=np.float64):
+    def __init__(self, n: int, count: int = 1, dtype=np.float64, zero: bool = True):
+        """zero: start from zeros (psb_geall + psb_geasb); the C entry point
+        FallocMultiVecDevice itself leaves the memory as cudaMalloc gives it,
+        as the reference's does."""
         self.n = int(n)
         self.count = int(count)
         self.dtype = np.dtype(dtype)
@@ -51,12 +54,15 @@ class DVect:
         check(lib.FallocMultiVecDevice(C.byref(h), self.count, self.n, et), "FallocMultiVecDevice")
         self.h = h
         self.pitch = lib.getMultiVecDevicePitch(self.h)
+        if zero:
+            self.zero()
 
     @classmethod
     def bld(cls, x):
         """psb_d_vect_cuda%bld(x): allocate and copy host data to the device."""
         x = np.asarray(x)
-        v = cls(x.shape[0], 1 if x.ndim == 1 else x.shape[1], np.float32 if x.dtype == np.float32 else np.float64)
+        v = cls(x.shape[0], 1 if x.ndim == 1 else x.shape[1], np.float32 if x.dtype == np.float32 else np.float64,
+                zero=False)
         v.set_vect(x)
         return v
 
@@ -90,7 +96,11 @@ class DVect:
         check(lib.setscalMultiVecDeviceDouble(float(val), int(first), int(last), 1, self.h), "setscal")
 
     def zero(self):
-        self.set_scal(0.0)
+        """Every element of every vector (padding included) to 0."""
+        if self.dtype == np.float64:
+            self.set_scal(0.0, 1, self.pitch * self.count)
+        else:
+            self.set_vect(np.zeros((self.n, self.count) if self.count > 1 else self.n, self.dtype))
 
     def scal(self, alpha):
         check(lib.scalMultiVecDeviceDouble(float(alpha), self.h), "scal")
@@ -179,6 +189,12 @@ class HllMat:
                                                     C.byref(hk), C.byref(ww), C.byref(ms)),
               "psbx_hll_autotune_from_csr_device")
         return cls(h, rows), {"hksz": hk.value, "wide_w": ww.value, "ms": ms.value}
+
+    def set_wide(self, wide_w):
+        """Wide-hack threshold (hack size 32): 0 default, < 0 never; the same
+        bits for every choice."""
+        check(lib.psbx_hll_set_wide(self.h, int(wide_w)), "psbx_hll_set_wide")
+        return self
 
     def params(self):
         v = [C.c_int() for _ in range(7)]

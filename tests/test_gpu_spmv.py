@@ -359,9 +359,10 @@ def test_distributed_parts_on_device(psb):
 @pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0), (2.5, -0.5)])
 def test_hll_wide_hacks_bitexact(psb, alpha, beta):
     """Row-sorted power-law matrix (rows up to 4,000 entries at the front):
-    hacks wider than 256 are summed by a block each, in entry order, so the
-    HLL SpMV stays bit-identical to the CPU csmv; host-written, device-built
-    and permuted (perm = the length order) layouts alike."""
+    the products of the wide hacks are formed by all blocks and each row's
+    products added in entry order by a warp per hack, so the HLL SpMV stays
+    bit-identical to the CPU csmv; host-written, device-built and permuted
+    (perm = the length order) layouts alike."""
     import torch
     irp, ja, va = gen.powerlaw(60000, kmax=4000, seed=21)
     sirp, sja, sva, order = gen.sort_rows_by_length(irp, ja, va)
@@ -399,8 +400,44 @@ def test_hll_autotune(psb):
         A, info = psb.HllMat.autotune_from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(),
                                                      d[2].data_ptr())
         assert info["hksz"] in (32, 64, 128) and info["ms"] > 0
-        assert info["wide_w"] in ((128, 256, 512, 1024, -1) if info["hksz"] == 32 else (0,))
+        assert info["wide_w"] in ((32, 64, 128, 256, 1024, -1) if info["hksz"] == 32 else (0,))
         x = np.random.default_rng(3).uniform(-1, 1, n)
         X, Y = psb.DVect.bld(x), psb.DVect(n)
         A.spmv(1.0, X, 0.0, Y)
         assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, 1.0, x, 0.0, np.zeros(n))), info
+
+
+@pytest.mark.parametrize("wide", [-1, 0, 1, 33, 64, 200])
+def test_hll_wide_threshold_same_bits(psb, wide):
+    """Every wide-hack threshold gives the CPU csmv's bits: 1 sends almost
+    every hack down the wide path (partial product blocks, partial ring
+    chunks, rows ending inside a chunk), -1 none; an unsorted power-law
+    matrix puts wide hacks between narrow ones."""
+    import torch
+    irp, ja, va = gen.powerlaw(20000, kmax=3000, seed=5)
+    n = len(irp) - 1
+    d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+    A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
+    A.set_wide(wide)
+    rng = np.random.default_rng(8)
+    x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+    A.spmv(-1.5, X, 0.5, Y)
+    assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, -1.5, x, 0.5, y0))
+    # and the CG over the same matrix made SPD (its products go the same way)
+    sirp, sja, sva = gen.powerlaw_spd(20000, kmax=3000, seed=6)
+    e = [torch.from_numpy(a).cuda() for a in (sirp, sja, sva)]
+    S = psb.HllMat.from_csr_device(n, n, len(sja), e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(), 32)
+    P = psb.DiagPrec("DIAG").build(S)
+    b = rng.uniform(-1, 1, n)
+    runs = []
+    for w in (-1, wide):
+        S.set_wide(w)
+        B, Xs = psb.DVect.bld(b), psb.DVect(n)
+        it, err = psb.psb_krylov("CG", S, P, B, Xs, eps=1e-10, itmax=1000)
+        runs.append((it, err, Xs.get_vect().copy()))
+    assert runs[1][0] == runs[0][0] and runs[1][1] == runs[0][1]
+    assert np.array_equal(runs[1][2], runs[0][2])  # same products, same reductions
+    assert runs[1][1] <= 1e-10
+    r = O.csr_csmv(sirp, sja, sva, -1.0, runs[1][2], 1.0, b)
+    assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b)

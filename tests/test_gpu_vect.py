@@ -152,3 +152,16 @@ def test_gather_scatter_halo_halves(psb):
         ref = v.copy()
         ref[idx - 1] = w if beta == 0.0 else beta * v[idx - 1] + w
         assert np.array_equal(V.get_vect(), ref)
+
+
+def test_new_vector_starts_at_zero(psb):
+    """DVect(n) is zero in every element of every vector even where its memory
+    held an earlier vector's data (an initial guess of psb_krylov)."""
+    for _ in range(3):
+        a = psb.DVect.bld(np.arange(1.0, 4097.0))
+        a.free()
+        z = psb.DVect(4096)
+        assert not np.any(z.get_vect())
+        z.free()
+    m = psb.DVect(1000, count=3)
+    assert not np.any(m.get_vect())
