@@ -18,8 +18,9 @@
 //
 // Layout: each system is an HLL-32 matrix (FP64 values, FP32 copy, shared
 // indices) with 1-based local columns, and K interleaved vectors
-// v[row*K + j].  Work is cut in tiles of up to TILE_ROWS rows of one system;
-// a block takes a contiguous range of tiles.  A tile's partial sums go to
+// v[row*K + j].  Work is cut in tiles of rows of one system (tile_plan);
+// block b takes tiles b, b + grid, b + 2 grid, ... so the blocks in flight
+// work on a window of consecutive tiles (whose gathered vectors share L2).  A tile's partial sums go to
 // part[tile]; the block that completes the last tile of a system (per-system
 // ticket) adds that system's partials in tile order -- fixed order, so the
 // result does not depend on scheduling -- and advances the system's phase.
@@ -34,7 +35,7 @@
 namespace {
 
 enum Phase { PH_IDLE = 0, PH_RESID = 1, PH_INIT = 2, PH_INNER = 3, PH_XUPD = 4, PH_DONE = 5 };
-enum { BT = 256, TILE_ROWS = 2048, ITERS = 8, MAXK = 8, LONG_ROW = 128 };
+enum { BT = 256, TILE_ROWS = 2048, TILE_NNZ = 16384, ITERS = 8, MAXK = 8, LONG_ROW = 64 };
 
 struct BSys {                 // read-only for the kernels
   const double *val64;
@@ -45,7 +46,6 @@ struct BSys {                 // read-only for the kernels
   float *r32, *z, *p, *q, *d;
   const float *dinv;
   int rows, sol0, tile0, ntiles;
-  int nlong;                  // leading rows handled warp-per-row (host use)
 };
 
 struct BState {               // written by the kernels
@@ -89,6 +89,7 @@ struct Eng {
   std::vector<BState> h_state;
   std::vector<int> used;      // slot in use
   std::vector<void *> owned;  // per slot: one allocation holding its vectors
+  std::vector<std::vector<int>> plan;  // per slot: its matrix's tile plan
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
   BState *h_state_pinned = nullptr;
@@ -877,6 +878,43 @@ static void capture_iters(Eng *e, cudaStream_t st) {
   }
 }
 
+// Tile plan of one matrix (rows relative to the matrix), built once from its
+// row lengths and kept on the matrix (the arrays' rewrite drops it): runs of
+// up to BT/32 consecutive rows longer than LONG_ROW become warp-per-row
+// tiles; the rows between them are cut into thread-per-row tiles of at most
+// TILE_ROWS rows and TILE_NNZ stored entries -- whole passes of the block
+// where the entry bound cuts -- so no thread carries a long serial chain
+// (the head of a row-sorted power-law matrix, a long row among short ones).
+// It depends on the matrix alone, so a system's tiles and the order of its
+// partial sums do not depend on the other systems in the engine.
+static int tile_plan(HllDevice *m) {
+  const int n = m->rows;
+  std::vector<int> irn(n > 0 ? n : 1);
+  if (n > 0) PSBX_CK(cudaMemcpy(irn.data(), m->rS, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+  std::vector<int> plan;
+  for (int r = 0; r < n;) {
+    int e = r;
+    if (irn[r] > LONG_ROW) {
+      while (e < n && e - r < BT / 32 && irn[e] > LONG_ROW) e++;
+      plan.insert(plan.end(), {r, e - r, 1});
+    } else {
+      long long ent = 0;
+      while (e < n && e - r < TILE_ROWS && irn[e] <= LONG_ROW && ent + irn[e] <= TILE_NNZ) ent += irn[e++];
+      const bool entry_cut = e < n && e - r < TILE_ROWS && irn[e] <= LONG_ROW;
+      if (entry_cut && e - r > BT) e = r + (e - r) / BT * BT;
+      plan.insert(plan.end(), {r, e - r, 0});
+    }
+    r = e;
+  }
+  int *t = (int *)malloc(sizeof(int) * (plan.empty() ? 1 : plan.size()));
+  if (!t) return SPGPU_OUTOFMEMORY;
+  if (!plan.empty()) memcpy(t, plan.data(), sizeof(int) * plan.size());
+  free(m->tplan);
+  m->tplan = t;
+  m->ntplan = (int)(plan.size() / 3);
+  return SPGPU_SUCCESS;
+}
+
 static int upload_tables(Eng *e, cudaStream_t st) {
   // rebuild the tile table from the slots in use
   std::vector<BTile> tiles;
@@ -884,21 +922,13 @@ static int upload_tables(Eng *e, cudaStream_t st) {
     if (!e->used[s]) continue;
     BSys &S = e->h_sys[s];
     S.tile0 = (int)tiles.size();
-    const int wide_rows = BT / 32;  // one warp per long row
-    for (int r = 0; r < S.nlong; r += wide_rows) {
+    const std::vector<int> &pl = e->plan[s];
+    for (size_t k = 0; k + 2 < pl.size(); k += 3) {
       BTile T;
       T.sys = s;
-      T.row0 = r;
-      T.nrows = S.nlong - r < wide_rows ? S.nlong - r : wide_rows;
-      T.kind = 1;
-      tiles.push_back(T);
-    }
-    for (int r = S.nlong; r < S.rows; r += TILE_ROWS) {
-      BTile T;
-      T.sys = s;
-      T.row0 = r;
-      T.nrows = S.rows - r < TILE_ROWS ? S.rows - r : TILE_ROWS;
-      T.kind = 0;
+      T.row0 = pl[k];
+      T.nrows = pl[k + 1];
+      T.kind = pl[k + 2];
       tiles.push_back(T);
     }
     S.ntiles = (int)tiles.size() - S.tile0;
@@ -965,6 +995,7 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   e->h_state.assign(max_systems, BState());
   e->used.assign(max_systems, 0);
   e->owned.assign(max_systems, nullptr);
+  e->plan.assign(max_systems, std::vector<int>());
   memset(e->h_sys.data(), 0, sizeof(BSys) * max_systems);
   memset(e->h_state.data(), 0, sizeof(BState) * max_systems);
   cudaError_t err = cudaSuccess;
@@ -1029,6 +1060,10 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
       break;
     }
   if (s < 0) return SPGPU_OUTOFMEMORY;  // no free slot
+  if (!m->tplan) {
+    int rc = tile_plan(m);
+    if (rc) return rc;
+  }
   PsbxCtx &c = psbx_ctx();
   const int K = e->K;
   const size_t n = (size_t)m->rows;
@@ -1057,17 +1092,7 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   S.dinv = dv;
   S.rows = (int)n;
   S.sol0 = s * K;
-  if (m->leadLong < 0) {
-    // leading run of rows longer than LONG_ROW (matrices whose rows are sorted
-    // by length put all their long rows there); kept on the matrix
-    const int probe = n < 65536 ? (int)n : 65536;
-    std::vector<int> irn(probe > 0 ? probe : 1);
-    if (probe > 0) PSBX_CK(cudaMemcpy(irn.data(), m->rS, sizeof(int) * probe, cudaMemcpyDeviceToHost));
-    int nl = 0;
-    while (nl < probe && irn[nl] > LONG_ROW) nl++;
-    m->leadLong = nl;
-  }
-  S.nlong = m->leadLong;
+  e->plan[s].assign(m->tplan, m->tplan + 3 * (size_t)m->ntplan);
   kb_d2f_inv<<<psbx_grid_for(n, 256), 256, 0, c.stream>>>((int)n, d_dinv, dv);
   psbx_count_launch();
   std::vector<BSol> so(K);

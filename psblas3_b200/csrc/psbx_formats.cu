@@ -65,7 +65,6 @@ int FallocHllDevice(void **deviceMat, unsigned hksize, unsigned rows, unsigned n
   m->elemType = (int)elementType;
   m->cols = (int)rows;
   m->maxRowLen = -1;
-  m->leadLong = -1;
   rc = dmalloc((void **)&m->rP, sizeof(int) * (size_t)allocsize);
   if (!rc) rc = dmalloc((void **)&m->rS, sizeof(int) * (size_t)rows);
   if (!rc) rc = dmalloc((void **)&m->diag, sizeof(int) * (size_t)rows);
@@ -97,6 +96,7 @@ void freeHllDevice(void *deviceMat) {
   cudaFree(m->wideBase);
   cudaFree(m->wchunk);
   cudaFree(m->wprod);
+  free(m->tplan);
   free(m);
 }
 

@@ -51,7 +51,8 @@ struct HllDevice {
   double *lres;      // rows entries (storage order), allocated when nLong > 0
   int longW;         // 0: default (PSBX_LONG_W or 4x the mean hack width); < 0: never
   int effW;          // the threshold the wide list was built with
-  int leadLong;      // batch engine: leading rows longer than 128 entries (-1 unknown)
+  int *tplan;        // batch engine tile plan (host memory, 3 ints per tile), built on first use
+  int ntplan;
   int *wideBase;     // nLong+1: offset of each wide hack's products in wprod
   int *wchunk;       // 2*nWChunks: (wide hack index, first entry column) per product block
   int nWChunks;

@@ -197,7 +197,9 @@ int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cu
 // equally wide keeps the thread-per-row sums (the extra product traffic
 // would cost more than the chains it saves).
 int psbx_hll_index_long(HllDevice *m) {
-  m->leadLong = -1;  // the arrays changed: the batch engine's probe is redone
+  free(m->tplan);  // the arrays changed: the batch engine's tile plan is redone
+  m->tplan = nullptr;
+  m->ntplan = 0;
   cudaFree(m->longHacks);
   cudaFree(m->lres);
   cudaFree(m->wideBase);
