@@ -380,52 +380,6 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
         T.free()
         return res
 
-    def c2b_powerlaw():
-        pi, pj, pv = gen.powerlaw(4_000_000, seed=0)
-        n2, nnz2 = len(pi) - 1, len(pj)
-        B2 = algorithmic_bytes(n2, nnz2)
-        x2 = np.random.default_rng(0).uniform(-1, 1, n2)
-        X2, Y2 = psb.DVect.bld(x2), psb.DVect(n2)
-        Cm = psb.CsrMat(n2, pi, pj, pv)
-        ms = _time_spmv(Cm, X2, Y2, steps, stream)
-        lens = np.diff(pi)
-        res = {"rows": n2, "nnz": nnz2, "max_row": int(lens.max()), "rows_over_2048": int((lens > 2048).sum()),
-               "csr": {"gb_s": B2 / ms / 1e6, "ms": ms}}
-        y_csr = Y2.get_vect()
-        Cm.free()
-        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
-        H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
-        del d_irp, d_ja, d_va
-        ms = _time_spmv(H, X2, Y2, max(3, steps // 5), stream)
-        res["hll_unsorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2}
-        yh = Y2.get_vect()
-        short = lens <= 2048
-        res["csr_equals_hll_on_short_rows"] = bool(np.array_equal(yh[short], y_csr[short]))
-        H.free()
-        # HLL holding the rows in decreasing-length order through a row
-        # permutation (y comes back in the original order): hacks of similar
-        # rows, the wide ones summed by a block each
-        order = np.argsort(-lens, kind="stable").astype(np.int32)
-        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
-        d_perm = torch.from_numpy(order).cuda()
-        H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32,
-                                       d_perm.data_ptr())
-        del d_irp, d_ja, d_va, d_perm
-        ms = _time_spmv(H, X2, Y2, steps, stream)
-        res["hll_row_sorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2,
-                                 "bitexact_vs_unsorted_hll": bool(np.array_equal(Y2.get_vect(), yh))}
-        H.free()
-        d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
-        d_perm = torch.from_numpy(order).cuda()
-        T, info = psb.HllMat.autotune_from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(),
-                                                      d_va.data_ptr(), d_perm.data_ptr())
-        del d_irp, d_ja, d_va, d_perm
-        ms = _time_spmv(T, X2, Y2, steps, stream)
-        res["hll_row_sorted_autotuned"] = dict(info, gb_s=B2 / ms / 1e6, ms=ms,
-                                               bitexact_vs_unsorted_hll=bool(np.array_equal(Y2.get_vect(), yh)))
-        T.free()
-        return res
-
     def c1_bicgstab():
         ci, cj, cv = gen.pde3d(40, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3)
         n1 = len(ci) - 1
@@ -457,7 +411,7 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
                 "cpu_iters": ito, "cpu_err": erro, "cpu_threads": os.cpu_count()}
 
     _part(out, "c2a_formats", c2a_formats)
-    _part(out, "c2b_powerlaw", c2b_powerlaw)
+    _part(out, "c2b_powerlaw", lambda: c2b_powerlaw(psb, gen, stream, steps))
     _part(out, "c1_bicgstab", c1_bicgstab)
     if not args.skip_c3:
         _part(out, "c3_cg", lambda: c3_cg(psb, gen))
@@ -591,6 +545,58 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
             "fp64_one_at_a_time_solves_per_s": len(pairs) / t64, "fp64_sample": len(pairs),
             "fp64_iters_median": float(np.median(it64)),
             "speedup_vs_fp64_one_at_a_time": (solves / tb) / (len(pairs) / t64)}
+
+
+def c2b_powerlaw(psb, gen, stream, steps=10):
+    """C2b: the power-law matrix (4M rows, alpha 2.1, rows up to 4,096
+    entries) in CSR, in HLL-32 as stored, and in HLL-32 with the rows held in
+    decreasing-length order through a row permutation (plain and autotuned);
+    HLL results compared bit for bit."""
+    import torch
+    pi, pj, pv = gen.powerlaw(4_000_000, seed=0)
+    n2, nnz2 = len(pi) - 1, len(pj)
+    B2 = algorithmic_bytes(n2, nnz2)
+    x2 = np.random.default_rng(0).uniform(-1, 1, n2)
+    X2, Y2 = psb.DVect.bld(x2), psb.DVect(n2)
+    Cm = psb.CsrMat(n2, pi, pj, pv)
+    ms = _time_spmv(Cm, X2, Y2, steps, stream)
+    lens = np.diff(pi)
+    res = {"rows": n2, "nnz": nnz2, "max_row": int(lens.max()), "rows_over_2048": int((lens > 2048).sum()),
+           "csr": {"gb_s": B2 / ms / 1e6, "ms": ms}}
+    y_csr = Y2.get_vect()
+    Cm.free()
+    d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
+    H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
+    del d_irp, d_ja, d_va
+    ms = _time_spmv(H, X2, Y2, max(3, steps // 5), stream)
+    res["hll_unsorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2}
+    yh = Y2.get_vect()
+    short = lens <= 2048
+    res["csr_equals_hll_on_short_rows"] = bool(np.array_equal(yh[short], y_csr[short]))
+    H.free()
+    # HLL holding the rows in decreasing-length order through a row
+    # permutation (y comes back in the original order): hacks of similar
+    # rows; the wide ones go through the wide-hack path
+    order = np.argsort(-lens, kind="stable").astype(np.int32)
+    d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
+    d_perm = torch.from_numpy(order).cuda()
+    H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32,
+                                   d_perm.data_ptr())
+    del d_irp, d_ja, d_va, d_perm
+    ms = _time_spmv(H, X2, Y2, steps, stream)
+    res["hll_row_sorted"] = {"gb_s": B2 / ms / 1e6, "ms": ms, "stored_over_nnz": H.params()["allocsize"] / nnz2,
+                             "bitexact_vs_unsorted_hll": bool(np.array_equal(Y2.get_vect(), yh))}
+    H.free()
+    d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
+    d_perm = torch.from_numpy(order).cuda()
+    T, info = psb.HllMat.autotune_from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(),
+                                                  d_va.data_ptr(), d_perm.data_ptr())
+    del d_irp, d_ja, d_va, d_perm
+    ms = _time_spmv(T, X2, Y2, steps, stream)
+    res["hll_row_sorted_autotuned"] = dict(info, gb_s=B2 / ms / 1e6, ms=ms,
+                                           bitexact_vs_unsorted_hll=bool(np.array_equal(Y2.get_vect(), yh)))
+    T.free()
+    return res
 
 
 def c5_serving(psb, gen, rate=2000.0, window=1.0, pool_each=8, seed=0, replays_per_step=2):
@@ -788,7 +794,7 @@ def main():
     ap.add_argument("--skip-c3", action="store_true", help="skip the 256^3 CG solves among the secondaries")
     ap.add_argument("--skip-c4", action="store_true", help="skip the batched 512-system solve")
     ap.add_argument("--skip-c5", action="store_true", help="skip the serving stream")
-    ap.add_argument("--only", choices=["c3", "c4", "c5"], default=None,
+    ap.add_argument("--only", choices=["c2b", "c3", "c4", "c5"], default=None,
                     help="run one secondary workload alone on one GPU and print its result (profiling runs)")
     args = ap.parse_args()
     if args.only:
@@ -800,14 +806,19 @@ def main():
 
 
 def run_only(name):
-    """One secondary workload by itself (C3 CG solves, C4 batched, C5
-    serving) on cuda:0; prints {"only": name, "result": {...}}."""
+    """One secondary workload by itself (C2b power-law SpMV, C3 CG solves,
+    C4 batched, C5 serving) on cuda:0; prints {"only": name, "result": {...}}."""
     import torch
     from psblas3_b200 import gen, psb
     psb.init(0)
     torch.cuda.set_device(0)
-    fn = {"c3": c3_cg, "c4": c4_batched, "c5": c5_serving}[name]
-    print(json.dumps({"only": name, "result": fn(psb, gen)}), flush=True)
+    if name == "c2b":
+        from psblas3_b200._lib import lib
+        stream = torch.cuda.ExternalStream(lib.psb_cudaGetStream(), device="cuda:0")
+        res = c2b_powerlaw(psb, gen, stream)
+    else:
+        res = {"c3": c3_cg, "c4": c4_batched, "c5": c5_serving}[name](psb, gen)
+    print(json.dumps({"only": name, "result": res}), flush=True)
 
 
 if __name__ == "__main__":
