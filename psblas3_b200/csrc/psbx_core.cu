@@ -66,6 +66,7 @@ int psbx_ensure_init() {
 static void ctx_destroy() {
   PsbxCtx &c = g_ctx;
   if (!c.init) return;
+  psbx_krylov_cache_clear();
   cudaStreamSynchronize(c.stream);
   cudaFree(c.d_part);
   cudaFree(c.d_ticket);

@@ -509,6 +509,9 @@ __device__ __forceinline__ int out_row(const EllView &, int r) { return r; }
 __device__ __forceinline__ int out_row(const CsrView &, int r) { return r; }
 
 HllView hll_view(const HllDevice *m);
+// Releases the iteration graphs (and workspaces) the Krylov driver keeps
+// between calls; called when the context is torn down.
+void psbx_krylov_cache_clear();
 // Finds the wide hacks of a hack-32 matrix after its arrays are written.
 int psbx_hll_index_long(HllDevice *m);
 // Row sums of the wide hacks of a hack-32 matrix into lres (two launches), to

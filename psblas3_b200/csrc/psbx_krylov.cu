@@ -1504,6 +1504,86 @@ static int replay_until(cudaGraphExec_t gexec, cudaStream_t st, int per_graph, K
   }
 }
 
+// Captured iteration graphs of the CG / BiCGSTAB driver, kept with their
+// workspaces.  A graph is a function of its kernels' arguments alone (matrix
+// view, vectors, workspace, sizes; the solver options live in the state
+// word, written at every call), so a later call whose arguments are the same
+// replays the kept graph instead of capturing and instantiating it again --
+// the repeated solves of a time-stepping loop.  The key holds every field of
+// the view and every pointer and size the captured kernels receive.  At most
+// KCACHE_N graphs, least recently used out; workspaces over KCACHE_MAX bytes
+// are not kept (their solves are long enough not to notice the capture).
+#define KCACHE_N 4
+#define KCACHE_MAX ((size_t)64 << 20)
+
+struct KCache {
+  std::vector<uint64_t> key;
+  cudaGraphExec_t gexec = nullptr;
+  double *vec = nullptr, *part = nullptr;
+  KState *S = nullptr;
+  unsigned *ticket = nullptr;
+  uint64_t used = 0;
+};
+static KCache g_kc[KCACHE_N];
+static uint64_t g_kc_clock = 0;
+
+static void key_hll(std::vector<uint64_t> &k, const HllView &v, uint64_t tag) {
+  k.insert(k.end(), {tag, (uint64_t)v.val, (uint64_t)v.ja, (uint64_t)v.irn, (uint64_t)v.hkoffs, (uint64_t)v.perm,
+                     (uint64_t)(uint32_t)v.rows, (uint64_t)(uint32_t)v.hksz, (uint64_t)(uint32_t)v.base,
+                     (uint64_t)v.longHacks, (uint64_t)v.lres, (uint64_t)(uint32_t)v.nLong,
+                     (uint64_t)(uint32_t)v.longW, (uint64_t)v.wideBase, (uint64_t)v.wchunk, (uint64_t)v.wprod,
+                     (uint64_t)(uint32_t)v.nWChunks});
+}
+static void key_view(std::vector<uint64_t> &k, const HllView &v) { key_hll(k, v, 0); }
+static void key_view(std::vector<uint64_t> &k, const Hll32View &v) { key_hll(k, v, 1); }
+static void key_view(std::vector<uint64_t> &k, const Hll32WView &v) { key_hll(k, v, 2); }
+static void key_view(std::vector<uint64_t> &k, const EllView &v) {
+  k.insert(k.end(), {3, (uint64_t)v.val, (uint64_t)v.ja, (uint64_t)v.irn, (uint64_t)(uint32_t)v.rows,
+                     (uint64_t)(uint32_t)v.pitch, (uint64_t)(uint32_t)v.base});
+}
+static void key_view(std::vector<uint64_t> &k, const CsrView &v) {
+  k.insert(k.end(), {4, (uint64_t)v.val, (uint64_t)v.ja, (uint64_t)v.irp, (uint64_t)(uint32_t)v.rows,
+                     (uint64_t)(uint32_t)v.base});
+}
+
+static void kc_release(KCache &e, cudaStream_t st) {
+  if (e.gexec) {
+    cudaStreamSynchronize(st);  // no replay of it in flight
+    cudaGraphExecDestroy(e.gexec);
+  }
+  cudaFreeAsync(e.vec, st);
+  cudaFreeAsync(e.part, st);
+  cudaFreeAsync(e.S, st);
+  cudaFreeAsync(e.ticket, st);
+  e = KCache();
+}
+
+void psbx_krylov_cache_clear() {
+  cudaStream_t st = psbx_ctx().stream;
+  for (KCache &e : g_kc)
+    if (!e.key.empty()) kc_release(e, st);
+  cudaStreamSynchronize(st);
+}
+
+static KCache *kc_find(const std::vector<uint64_t> &key) {
+  for (KCache &e : g_kc)
+    if (!e.key.empty() && e.key == key) {
+      e.used = ++g_kc_clock;
+      return &e;
+    }
+  return nullptr;
+}
+
+static KCache *kc_slot(cudaStream_t st) {  // a free entry, else the least recently used one, released
+  KCache *lru = &g_kc[0];
+  for (KCache &e : g_kc) {
+    if (e.key.empty()) return &e;
+    if (e.used < lru->used) lru = &e;
+  }
+  kc_release(*lru, st);
+  return lru;
+}
+
 template <class View>
 static int solve(const View &A, bool bicg, const double *dinv, const double *b, double *x, int n,
                  psbx_SolverOptions *opt) {
@@ -1517,12 +1597,30 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
   double *vec = nullptr, *part = nullptr;
   KState *S = nullptr;
   unsigned *ticket = nullptr;
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * (size_t)nvec * (size_t)(n > 0 ? n : 1), st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  cudaGraphExec_t gexec = nullptr;
+  const size_t vbytes = sizeof(double) * (size_t)nvec * (size_t)(n > 0 ? n : 1);
+  std::vector<uint64_t> key;
+  KCache *ce = nullptr;
+  if (vbytes <= KCACHE_MAX) {
+    key_view(key, A);
+    key.insert(key.end(), {(uint64_t)bicg, (uint64_t)dinv, (uint64_t)b, (uint64_t)x, (uint64_t)(uint32_t)n,
+                           (uint64_t)(uint32_t)grid});
+    ce = kc_find(key);
+  }
+  if (ce) {
+    vec = ce->vec;
+    part = ce->part;
+    S = ce->S;
+    ticket = ce->ticket;
+    gexec = ce->gexec;
+  } else {
+    PSBX_CK(cudaMallocAsync(&vec, vbytes, st));
+    PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+    PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
+    PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  }
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
-  PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * (size_t)nvec * (size_t)(n > 0 ? n : 1), st));
+  PSBX_CK(cudaMemsetAsync(vec, 0, vbytes, st));
 
   static_assert(sizeof(KState) <= 64 * sizeof(double), "KState fits the pinned staging area");
   KState *hS = (KState *)c.h_res;
@@ -1546,12 +1644,15 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     psbx_count_launch();
   }
 
-  // one captured batch of KGRAPH_ITERS iterations
+  // one captured batch of KGRAPH_ITERS iterations (kept from an earlier call
+  // with the same arguments, or captured now)
   cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
-  if (!rc) {
+  cudaError_t e = cudaSuccess;
+  if (!gexec) {
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) rc = psbx_cuda_status(e, "BeginCapture");
+  }
+  if (!rc && !gexec) {
     for (int k = 0; k < KGRAPH_ITERS; k++) {
       if (!bicg) {
         k_cg_p<<<grid, KT, 0, st>>>(S, n, v3, v0);
@@ -1570,10 +1671,20 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     }
     e = cudaStreamEndCapture(st, &graph);
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "EndCapture");
-  }
-  if (!rc) {
-    e = cudaGraphInstantiate(&gexec, graph, 0);
-    if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+    if (!rc) {
+      e = cudaGraphInstantiate(&gexec, graph, 0);
+      if (e != cudaSuccess) rc = psbx_cuda_status(e, "GraphInstantiate");
+    }
+    if (!rc && !key.empty()) {  // keep it, with the workspace it was captured on
+      ce = kc_slot(st);
+      ce->key = key;
+      ce->gexec = gexec;
+      ce->vec = vec;
+      ce->part = part;
+      ce->S = S;
+      ce->ticket = ticket;
+      ce->used = ++g_kc_clock;
+    }
   }
   const int per_graph = KGRAPH_ITERS * ((bicg ? 5 : 3) + (bicg ? 2 : 1) * long_launch(A));
 
@@ -1605,12 +1716,14 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     opt->iter = hS->itx;
     opt->err = hS->errden == 0.0 ? hS->errnum : hS->errnum / hS->errden;
   }
-  if (gexec) cudaGraphExecDestroy(gexec);
   if (graph) cudaGraphDestroy(graph);
-  cudaFreeAsync(vec, st);
-  cudaFreeAsync(part, st);
-  cudaFreeAsync(S, st);
-  cudaFreeAsync(ticket, st);
+  if (!ce) {  // not kept
+    if (gexec) cudaGraphExecDestroy(gexec);
+    cudaFreeAsync(vec, st);
+    cudaFreeAsync(part, st);
+    cudaFreeAsync(S, st);
+    cudaFreeAsync(ticket, st);
+  }
   cudaError_t e2 = cudaStreamSynchronize(st);
   if (!rc && e2 != cudaSuccess) rc = psbx_cuda_status(e2, "solve");
   return rc;

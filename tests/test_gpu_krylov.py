@@ -212,3 +212,39 @@ def test_bicgstabl_c1(psb, irst, istop):
     assert abs(it - ito) <= 2, (it, ito)
     assert err <= 1e-9
     assert np.max(np.abs(x - xo)) <= 1e-8
+
+
+@pytest.mark.parametrize("method", ["CG", "BICGSTAB"])
+def test_repeated_solves_replay_kept_graph(psb, method):
+    """Calls with the same matrix view and vectors replay the iteration graph
+    kept from the first call: the same iterations, error and bits; new values
+    in the same right-hand side vector solve the new system; a nonzero
+    initial guess is honoured; another vector is another graph."""
+    irp, ja, va = gen.pde3d(14, a=(1, 1, 1), b=(1 / np.sqrt(3),) * 3) if method == "BICGSTAB" else gen.poisson7(14)
+    n = len(irp) - 1
+    import torch
+    d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+    A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
+    P = psb.DiagPrec("DIAG").build(A)
+    rng = np.random.default_rng(11)
+    b1, b2, x0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    B, X = psb.DVect.bld(b1), psb.DVect(n)
+    runs = []
+    for _ in range(3):
+        X.zero()
+        it, err = psb.psb_krylov(method, A, P, B, X, eps=1e-10, itmax=2000)
+        runs.append((it, err, X.get_vect()))
+    for it, err, x in runs[1:]:
+        assert it == runs[0][0] and err == runs[0][1] and np.array_equal(x, runs[0][2])
+    B.set_vect(b2)
+    X.set_vect(x0)
+    it, err = psb.psb_krylov(method, A, P, B, X, eps=1e-10, itmax=2000)
+    assert err <= 1e-10
+    r = b2 - gen.csr_matvec(irp, ja, va, X.get_vect())
+    assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b2)
+    # a second solution vector: its own graph, same answer as the first one's
+    X2 = psb.DVect(n)
+    X.zero()
+    it_a, err_a = psb.psb_krylov(method, A, P, B, X, eps=1e-10, itmax=2000)
+    it_b, err_b = psb.psb_krylov(method, A, P, B, X2, eps=1e-10, itmax=2000)
+    assert (it_a, err_a) == (it_b, err_b) and np.array_equal(X.get_vect(), X2.get_vect())
