@@ -35,7 +35,7 @@
 namespace {
 
 enum Phase { PH_IDLE = 0, PH_RESID = 1, PH_INIT = 2, PH_INNER = 3, PH_XUPD = 4, PH_DONE = 5 };
-enum { BT = 256, TILE_ROWS = 2048, TILE_NNZ = 16384, ITERS = 8, MAXK = 8, LONG_ROW = 64 };
+enum { BT = 256, TILE_ROWS = 4096, TILE_NNZ = 32768, ITERS = 8, MAXK = 8, LONG_ROW = 64 };
 
 struct BSys {                 // read-only for the kernels
   const double *val64;
