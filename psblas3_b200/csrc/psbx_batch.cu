@@ -66,7 +66,7 @@ struct BSol {                 // one right-hand side
 };
 
 struct BTile {
-  int sys, row0, nrows, kind;  // kind 1: one warp per row (long rows)
+  int sys, row0, nrows, kind;  // kind 1: up to 8 long rows (tile_spmv)
 };
 
 struct BCtl {                 // read by every kernel at launch; lets the tile
@@ -282,9 +282,66 @@ __device__ __forceinline__ void row_multi(const VT *__restrict__ val, const int 
   }
 }
 
-// One HLL-32 row summed by a whole warp (rows longer than LONG_ROW): lane l
-// takes entries l, l+32, ...; a fixed shuffle tree combines them; the
-// result is valid in every lane.
+// The rows of a long-row tile (up to 8 consecutive rows longer than
+// LONG_ROW) summed by the whole block: thread t takes row t % 8 and its
+// entries t/8, t/8 + 32, ... in order, W per round with their loads issued
+// before the gathers, so one warp load reads entry j of 8 neighbouring rows
+// -- 32 contiguous bytes of the hack's column-major layout -- for 4 columns
+// (a warp on one row would touch a different 32-byte sector per lane).  The
+// 32 partial sums of a row are added in column-phase order; thread i < nrows
+// returns row i's sums.  Every thread of the block must call it.
+static_assert(BT / 32 == 8, "a long-row tile holds BT/32 = 8 rows");
+template <class VT, class XT, int K>
+__device__ __forceinline__ bool rows_by_block(const BSys &S, const BTile &T, const VT *__restrict__ val,
+                                              const XT *__restrict__ x, double (&out)[K]) {
+  __shared__ double red[K * BT];
+  const int i = threadIdx.x & 7, c0 = threadIdx.x >> 3;
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k] = 0.0;
+  if (i < T.nrows) {
+    const RowRef rr = row_ref(S.hkoffs, S.irn, T.row0 + i);
+    constexpr int W = K == 1 ? 8 : 2;
+    for (int j0 = c0; j0 < rr.n; j0 += 32 * W) {
+      int c[W];
+      double v[W];
+#pragma unroll
+      for (int u = 0; u < W; u++) {
+        const int j = j0 + 32 * u;
+        const bool ok = j < rr.n;
+        c[u] = ok ? ld_stream(S.ja + rr.off + j * 32) - 1 : 0;
+        v[u] = ok ? (double)ld_stream(val + rr.off + j * 32) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < W; u++) {
+        if (j0 + 32 * u < rr.n) {
+          XT xv[K];
+          ld_row_ro<K>(x + (size_t)c[u] * K, xv);
+#pragma unroll
+          for (int k = 0; k < K; k++) acc[k] = radd(acc[k], rmul(v[u], (double)xv[k]));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; k++) red[k * BT + threadIdx.x] = acc[k];
+  __syncthreads();
+  const bool mine = threadIdx.x < T.nrows;
+  if (mine) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double t = 0.0;
+      for (int c = 0; c < BT / 8; c++) t = radd(t, red[k * BT + c * 8 + threadIdx.x]);
+      out[k] = t;
+    }
+  }
+  __syncthreads();  // red is reused by the next tile
+  return mine;
+}
+
+// One long row summed by a whole warp (the 8-right-hand-side kernels, where
+// the block-wide sums below cost registers): lane l takes entries l, l+32,
+// ...; a fixed shuffle tree combines them; the result is valid in every lane.
 template <class VT, class XT, int K>
 __device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const int *__restrict__ ja, RowRef rr,
                                                const XT *__restrict__ x, double (&acc)[K]) {
@@ -322,17 +379,23 @@ __device__ __forceinline__ void row_multi_warp(const VT *__restrict__ val, const
 
 // Applies f(row, sums) to every row of a tile: thread-per-row tiles (kind 0)
 // walk rows threadIdx.x, +BT, ... with the next row's offset and length
-// loaded while the current row is summed; warp-per-row tiles (kind 1) call
-// f in lane 0 only.
+// loaded while the current row is summed; the rows of a long-row tile
+// (kind 1) are summed by the whole block and f is called by thread i for row
+// i (one right-hand side), or by a warp per row, f in lane 0 (8 of them).
 template <class VT, class XT, int K, class F>
 __device__ __forceinline__ void tile_spmv(const BSys &S, const BTile &T, const VT *__restrict__ val,
                                           const XT *__restrict__ x, F &&f) {
   if (T.kind == 1) {
-    for (int i = threadIdx.x >> 5; i < T.nrows; i += BT / 32) {
-      const int r = T.row0 + i;
+    if constexpr (K == 1) {
       double a[K];
-      row_multi_warp<VT, XT, K>(val, S.ja, row_ref(S.hkoffs, S.irn, r), x, a);
-      if ((threadIdx.x & 31) == 0) f(r, a);
+      if (rows_by_block<VT, XT, K>(S, T, val, x, a)) f(T.row0 + threadIdx.x, a);
+    } else {
+      for (int i = threadIdx.x >> 5; i < T.nrows; i += BT / 32) {
+        const int r = T.row0 + i;
+        double a[K];
+        row_multi_warp<VT, XT, K>(val, S.ja, row_ref(S.hkoffs, S.irn, r), x, a);
+        if ((threadIdx.x & 31) == 0) f(r, a);
+      }
     }
     return;
   }
@@ -880,7 +943,7 @@ static void capture_iters(Eng *e, cudaStream_t st) {
 
 // Tile plan of one matrix (rows relative to the matrix), built once from its
 // row lengths and kept on the matrix (the arrays' rewrite drops it): runs of
-// up to BT/32 consecutive rows longer than LONG_ROW become warp-per-row
+// up to BT/32 consecutive rows longer than LONG_ROW become long-row
 // tiles; the rows between them are cut into thread-per-row tiles of at most
 // TILE_ROWS rows and TILE_NNZ stored entries -- whole passes of the block
 // where the entry bound cuts -- so no thread carries a long serial chain

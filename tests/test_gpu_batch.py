@@ -119,7 +119,9 @@ def test_batched_converge_and_alone_equals_mix(psb, k):
 
 def test_eight_rhs_equal_single_rhs(psb):
     """Column j of an 8-rhs solve is bit-identical to the 1-rhs solve of
-    that right-hand side (same per-rhs operation order)."""
+    that right-hand side (same per-rhs operation order; rows longer than 64
+    entries, summed by the block for one right-hand side and by a warp for
+    eight, are the exception and absent here)."""
     systems = _aniso_set(11, 2, 8)
     r8 = _solve_set(psb, systems, 8)
     irp, ja, va, rhs = systems[1]
@@ -128,9 +130,9 @@ def test_eight_rhs_equal_single_rhs(psb):
 
 
 def test_powerlaw_long_rows_in_mix(psb):
-    """Row-sorted power-law systems put their rows longer than 128 entries
-    in warp-per-row tiles; they converge and stay bit-identical alone and in
-    a mix with stencil systems."""
+    """Row-sorted power-law systems put their rows longer than 64 entries
+    in long-row tiles (summed by the whole block); they converge and stay
+    bit-identical alone and in a mix with stencil systems."""
     rng = np.random.default_rng(3)
     systems = []
     for rows, seed in ((6000, 1), (2500, 2)):
