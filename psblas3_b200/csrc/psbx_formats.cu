@@ -272,7 +272,8 @@ extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int no
 // ------------------------------------------------ CSR (device) -> HLL build
 // Restates psi_d_convert_hll_from_coo.f90:31-122 / psi_d_xtr_ell_from_coo
 // on the device: irn from irp, hack widths = max irn in the hack, hkoffs by
-// an exclusive scan, then one block per hack fills the column-major slice.
+// an exclusive scan, then the column-major slices are filled (a warp per
+// hack for hack size 32, k_hll_fill32; k_hll_fill otherwise).
 // Padding is the CPU converter's: last stored column of the row (the hack's
 // first stored column for an empty row), value 0; rows past nr in the last
 // hack: column nr, value 0 (psi_d_convert_hll_from_coo.f90:94-96).

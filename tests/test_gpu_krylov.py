@@ -168,9 +168,10 @@ def test_itmax_fcg_and_rgmres(psb):
 
 @pytest.mark.parametrize("method", ["CG", "FCG", "CGS", "BICG", "BICGSTAB", "BICGSTABL", "RGMRES"])
 def test_wide_hacks_in_solvers(psb, method):
-    """Row-sorted SPD power-law matrix whose leading hacks are wider than 256
-    (summed by a block each before every product): every method matches the
-    oracle's iteration count within +-2 and reaches the tolerance."""
+    """Row-sorted SPD power-law matrix whose leading hacks take the wide-hack
+    path (products formed by all blocks, then each row added in order by a
+    warp per hack, before every product): every method matches the oracle's
+    iteration count within +-2 and reaches the tolerance."""
     irp, ja, va = gen.powerlaw_spd(40000, kmax=3000, seed=8)
     irp, ja, va, _ = gen.sort_rows_by_length(irp, ja, va)
     n = len(irp) - 1
