@@ -35,7 +35,13 @@
 namespace {
 
 enum Phase { PH_IDLE = 0, PH_RESID = 1, PH_INIT = 2, PH_INNER = 3, PH_XUPD = 4, PH_DONE = 5 };
-enum { BT = 256, TILE_ROWS = 4096, TILE_NNZ = 32768, ITERS = 8, MAXK = 8, LONG_ROW = 64 };
+enum { BT = 256, ITERS = 8, MAXK = 8, LONG_ROW = 64 };
+// Thread-per-row tile bounds (rows, stored entries): one right-hand side
+// runs fastest with 4096 / 32K (7-point 111^3: 17.8 ms per solve against
+// 19.7 with 2048 / 16K), eight with 2048 / 16K (their SpMV carries 8 sums
+// per row: 534 against 635 us per launch on C4).
+__host__ __device__ constexpr int tile_rows(int K) { return K == 1 ? 4096 : 2048; }
+__host__ __device__ constexpr int tile_nnz(int K) { return K == 1 ? 32768 : 16384; }
 
 struct BSys {                 // read-only for the kernels
   const double *val64;
@@ -945,13 +951,15 @@ static void capture_iters(Eng *e, cudaStream_t st) {
 // row lengths and kept on the matrix (the arrays' rewrite drops it): runs of
 // up to BT/32 consecutive rows longer than LONG_ROW become long-row
 // tiles; the rows between them are cut into thread-per-row tiles of at most
-// TILE_ROWS rows and TILE_NNZ stored entries -- whole passes of the block
+// tile_rows(K) rows and tile_nnz(K) stored entries -- whole passes of the block
 // where the entry bound cuts -- so no thread carries a long serial chain
 // (the head of a row-sorted power-law matrix, a long row among short ones).
 // It depends on the matrix alone, so a system's tiles and the order of its
-// partial sums do not depend on the other systems in the engine.
-static int tile_plan(HllDevice *m) {
+// partial sums do not depend on the other systems in the engine (the plan is
+// rebuilt when an engine with another K adds the matrix).
+static int tile_plan(HllDevice *m, int K) {
   const int n = m->rows;
+  const int trows = tile_rows(K), tnnz = tile_nnz(K);
   std::vector<int> irn(n > 0 ? n : 1);
   if (n > 0) PSBX_CK(cudaMemcpy(irn.data(), m->rS, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
   std::vector<int> plan;
@@ -962,8 +970,8 @@ static int tile_plan(HllDevice *m) {
       plan.insert(plan.end(), {r, e - r, 1});
     } else {
       long long ent = 0;
-      while (e < n && e - r < TILE_ROWS && irn[e] <= LONG_ROW && ent + irn[e] <= TILE_NNZ) ent += irn[e++];
-      const bool entry_cut = e < n && e - r < TILE_ROWS && irn[e] <= LONG_ROW;
+      while (e < n && e - r < trows && irn[e] <= LONG_ROW && ent + irn[e] <= tnnz) ent += irn[e++];
+      const bool entry_cut = e < n && e - r < trows && irn[e] <= LONG_ROW;
       if (entry_cut && e - r > BT) e = r + (e - r) / BT * BT;
       plan.insert(plan.end(), {r, e - r, 0});
     }
@@ -975,6 +983,7 @@ static int tile_plan(HllDevice *m) {
   free(m->tplan);
   m->tplan = t;
   m->ntplan = (int)(plan.size() / 3);
+  m->tplanK = K;
   return SPGPU_SUCCESS;
 }
 
@@ -1052,7 +1061,7 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   Eng *e = new Eng();
   e->K = nrhs;
   e->max_sys = max_systems;
-  e->max_tiles = max_rows_total / TILE_ROWS + max_systems + 1;
+  e->max_tiles = max_rows_total / tile_rows(e->K) + max_systems + 1;
   e->grid = c.sms * 8;
   e->h_sys.assign(max_systems, BSys());
   e->h_state.assign(max_systems, BState());
@@ -1123,8 +1132,8 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
       break;
     }
   if (s < 0) return SPGPU_OUTOFMEMORY;  // no free slot
-  if (!m->tplan) {
-    int rc = tile_plan(m);
+  if (!m->tplan || m->tplanK != e->K) {
+    int rc = tile_plan(m, e->K);
     if (rc) return rc;
   }
   PsbxCtx &c = psbx_ctx();

@@ -53,6 +53,7 @@ struct HllDevice {
   int effW;          // the threshold the wide list was built with
   int *tplan;        // batch engine tile plan (host memory, 3 ints per tile), built on first use
   int ntplan;
+  int tplanK;        // right-hand sides per row the plan was built for
   int *wideBase;     // nLong+1: offset of each wide hack's products in wprod
   int *wchunk;       // 2*nWChunks: (wide hack index, first entry column) per product block
   int nWChunks;
