@@ -372,11 +372,17 @@ int psbx_batch_destroy(void *eng);
  *           vectors of x and of y (ignored when count == 1)
  *   x, y    device pointers; stream: cudaStream_t (NULL: default stream)
  * The call is asynchronous on the stream and allocates nothing.  The first
- * call on each device looks up the scratch's device address, so make that
- * first call before any stream capture.  All calls share the one scratch
- * array: calls whose kernels overlap on the GPU (different streams, or
- * different host threads) race and give wrong results; order them.  Results
- * equal dotMultiVecDeviceDouble's (same kernel, same compensated sum). */
+ * call on each device looks up the scratch's device address and zeroes its
+ * counters (a synchronous cudaMemset), so make that first call before any
+ * stream capture.  Each later call leaves the counters at zero when its
+ * kernel ends.  gpuClose, cudaReset and psb_cudaDestroyHandle drop the
+ * looked-up addresses; a caller that resets the device itself
+ * (cudaDeviceReset) calls gpuClose before the next call here.  All calls
+ * share the one scratch array: calls whose kernels overlap on the GPU
+ * (different streams, or different host threads) race and give wrong
+ * results; order them.  Results are bit for bit those of
+ * dotMultiVecDeviceDouble on the same vectors (same kernel, same grid, same
+ * compensated sum). */
 int psbx_dot_noalloc(double *d_res, int n, int count, const double *x, const double *y, int pitch,
                      void *stream);
 

@@ -38,15 +38,25 @@ def build() -> str:
 
 
 _REF_GPU_PATH = os.path.join(_HERE, "_ref", "libspgpu_ref.so")
-_REF_SRC = "/root/reference/cuda/spgpu/kernels/hell_dspmv.cu"
+
+
+def ref_source_dir() -> str:
+    """Location of the psblas3 source tree: $PSBLAS_SRC, else the checkout
+    this build recipe was written against (/root/reference)."""
+    return os.environ.get("PSBLAS_SRC", "/root/reference")
 
 
 def build_ref() -> bool:
-    """Compile the reference's SPGPU HLL SpMV into oracle/_ref/ when the
-    psblas3 sources are present (they are not on every machine)."""
-    if not os.path.exists(_REF_SRC):
+    """Compile the reference's SPGPU kernels into oracle/_ref/ when the
+    psblas3 sources are present (they are not on every machine: without them
+    an existing oracle/_ref/ build is used, and the tests that need it skip)."""
+    src = ref_source_dir()
+    if not os.path.exists(os.path.join(src, "cuda", "spgpu", "kernels", "hell_dspmv.cu")):
+        if not os.path.exists(_REF_GPU_PATH):
+            print(f"oracle: psblas3 sources not found at {src} (set PSBLAS_SRC); "
+                  "oracle/_ref/ not built")
         return os.path.exists(_REF_GPU_PATH)
-    subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={src}"], check=True)
     return True
 
 

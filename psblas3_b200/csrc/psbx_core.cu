@@ -63,7 +63,10 @@ int psbx_ensure_init() {
   return ctx_create(dev);
 }
 
+void psbx_noalloc_forget(void);
+
 static void ctx_destroy() {
+  psbx_noalloc_forget();
   PsbxCtx &c = g_ctx;
   if (!c.init) return;
   psbx_krylov_cache_clear();

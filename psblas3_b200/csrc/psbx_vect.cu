@@ -551,7 +551,9 @@ void psbx_set_error(const char *msg);
 
 // Once per device, with that device current: the device addresses of the
 // scratch arrays (in host code their names are host-side stand-ins, not
-// device addresses) and the SM count for the grid size.
+// device addresses), the SM count for the grid size, and the tickets set to
+// zero.  After that every call leaves the tickets at zero itself: the last
+// block of each vector's reduction resets its ticket (k_reduce).
 static int noalloc_setup(int dev) {
   if (g_na_ready[dev]) return SPGPU_SUCCESS;
   cudaError_t e = cudaGetSymbolAddress((void **)&g_na_part[dev], psbx_noalloc_part);
@@ -560,8 +562,17 @@ static int noalloc_setup(int dev) {
   if (e != cudaSuccess) return psbx_cuda_status(e, "cudaGetSymbolAddress(psbx_noalloc_ticket)");
   e = cudaDeviceGetAttribute(&g_na_sms[dev], cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return psbx_cuda_status(e, "cudaDeviceGetAttribute");
+  e = cudaMemset(g_na_ticket[dev], 0, sizeof(unsigned) * PSBX_NOALLOC_MAX_VECS);
+  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaMemset(ticket)");
   g_na_ready[dev] = true;
   return SPGPU_SUCCESS;
+}
+
+// Called when the library context is released (gpuClose, cudaReset,
+// psb_cudaDestroyHandle): a context created afterwards may place the scratch
+// arrays elsewhere, so the next call looks their addresses up again.
+void psbx_noalloc_forget(void) {
+  for (int d = 0; d < PSBX_NOALLOC_MAX_DEVICES; d++) g_na_ready[d] = false;
 }
 
 extern "C" int psbx_dot_noalloc(double *d_res, int n, int count, const double *x, const double *y, int pitch,
@@ -584,9 +595,6 @@ extern "C" int psbx_dot_noalloc(double *d_res, int n, int count, const double *x
   int rc = noalloc_setup(dev);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  // the tickets must start at zero; the array keeps the previous call's state
-  e = cudaMemsetAsync(g_na_ticket[dev], 0, sizeof(unsigned) * PSBX_NOALLOC_MAX_VECS, st);
-  if (e != cudaSuccess) return psbx_cuda_status(e, "cudaMemsetAsync(ticket)");
   long long blocks = ((long long)(n > 0 ? n : 1) + VT * 4 - 1) / (VT * 4);
   long long cap = (long long)g_na_sms[dev] * 4;
   int g = (int)(blocks < cap ? blocks : cap);

@@ -3,7 +3,10 @@
 Reads, as text, the reference test sources and writes JSON fixtures next to
 this script.  Run it where the psblas3 source tree is available:
 
-    python tests/golden/make_kats.py /root/reference
+    python tests/golden/make_kats.py [PSBLAS_SOURCE_DIR]
+
+The directory comes from the argument, else $PSBLAS_SRC, else
+/root/reference; the script stops with a message when it is not there.
 
 Fixtures written:
   usmv_kats.json   every ``d_usmv_*`` case of test/torture/psb_d_mvsv_tester.f90
@@ -102,4 +105,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PSBLAS_SRC", "/root/reference")
+    if not os.path.isfile(os.path.join(src, "test/torture/psb_d_mvsv_tester.f90")):
+        sys.exit(f"make_kats: psblas3 sources not found at {src} (pass the directory or set PSBLAS_SRC)")
+    main(src)
