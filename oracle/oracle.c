@@ -327,6 +327,8 @@ int or_hll_get_diag(int nr, int hksz, const int *irn, const int *hkoffs,
 
 /* ------------------------------------------------------------------------ */
 /* Dense vector kernels.                                                     */
+/* Element-wise loops run over threads for long vectors: each entry is      */
+/* computed alone, so the results do not depend on the thread count.        */
 /* axpby: base/serial/psi_d_serial_impl.F90:593-745 (psi_daxpbyv).  The      */
 /* special cases there (alpha, beta in {0, +1, -1}) equal the generic form   */
 /* bit for bit for finite data; what they change is which operand is read:   */
@@ -335,11 +337,21 @@ int or_hll_get_diag(int nr, int hksz, const int *irn, const int *hkoffs,
 void or_axpby(int n, double alpha, const double *x, double beta, double *y)
 {
   if (alpha == 0.0) {
-    if (beta == 0.0) { for (int i = 0; i < n; i++) y[i] = 0.0; }
-    else if (beta != 1.0) { for (int i = 0; i < n; i++) y[i] = beta * y[i]; }
+    if (beta == 0.0) {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
+      for (int i = 0; i < n; i++) y[i] = 0.0;
+    } else if (beta != 1.0) {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
+      for (int i = 0; i < n; i++) y[i] = beta * y[i];
+    }
     return;
   }
-  if (beta == 0.0) { for (int i = 0; i < n; i++) y[i] = alpha * x[i]; return; }
+  if (beta == 0.0) {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
+    for (int i = 0; i < n; i++) y[i] = alpha * x[i];
+    return;
+  }
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
   for (int i = 0; i < n; i++) y[i] = alpha * x[i] + beta * y[i];
 }
 
@@ -347,6 +359,7 @@ void or_axpby(int n, double alpha, const double *x, double beta, double *y)
 void or_axpbyz(int n, double alpha, const double *x, double beta,
                const double *y, double *z)
 {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
   for (int i = 0; i < n; i++) {
     double a = (alpha == 0.0) ? 0.0 : alpha * x[i];
     z[i] = (beta == 0.0) ? a : (alpha == 0.0 ? beta * y[i] : a + beta * y[i]);
@@ -424,6 +437,7 @@ double or_nrm2(int n, const double *x) { return sqrt(or_dot(n, x, x)); }
 double or_amax(int n, const double *x)
 {
   double m = 0.0;
+#pragma omp parallel for schedule(static) num_threads(g_threads) reduction(max : m) if (n > 65536)
   for (int i = 0; i < n; i++) { double a = fabs(x[i]); if (a > m) m = a; }
   return m;
 }
@@ -441,6 +455,7 @@ double or_asum(int n, const double *x)
 void or_mlt(int n, double alpha, const double *d, const double *x,
             double beta, double *z)
 {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
   for (int i = 0; i < n; i++) {
     double t = alpha * (d[i] * x[i]);
     z[i] = (beta == 0.0) ? t : t + beta * z[i];
@@ -462,6 +477,7 @@ void or_upd_xyz(int n, double alpha, double beta, double gamma, double delta,
 void or_xyzw(int n, double a, double b, double c, double d, double e,
              double f, const double *x, double *y, double *z, double *w)
 {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (n > 65536)
   for (int i = 0; i < n; i++) {
     y[i] = a * x[i] + b * y[i];
     z[i] = c * y[i] + d * z[i];
