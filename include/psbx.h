@@ -94,6 +94,45 @@ int  readMultiVecDeviceDouble(void *deviceVec, double *hostVec);
 int  readMultiVecDeviceDoubleR2(void *deviceVec, double *hostVec, int ld);
 int  writeMultiVecDeviceFloat(void *deviceVec, float *hostVec);
 int  readMultiVecDeviceFloat(void *deviceVec, float *hostVec);
+/* cuda/psb_base_vectordev_mod.F90 (unregisterMapped), vectordev.c:145 */
+int  unregisterMapped(void *buf);
+/* cuda/psb_d_vectordev_mod.F90:85-160 / cuda_util.c:601-665: plain device
+ * buffers (raw pointers) for the gather/scatter buffers of the vector types:
+ * allocate n (or m*n) entries; write/read n entries, from the
+ * IndexBase-based entry first, or m*n entries; free.  registerMapped pins a
+ * host buffer of n entries and returns its device alias (cuda_util.c:104). */
+int  allocateDouble(void **d, int n);
+int  allocateMultiDouble(void **d, int m, int n);
+int  writeDouble(void *d, double *h, int n);
+int  readDouble(void *d, double *h, int n);
+int  writeDoubleFirst(int first, void *d, double *h, int n, int IndexBase);
+int  readDoubleFirst(int first, void *d, double *h, int n, int IndexBase);
+int  writeMultiDouble(void *d, double *h, int m, int n);
+int  readMultiDouble(void *d, double *h, int m, int n);
+void freeDouble(void *d);
+int  registerMappedDouble(void *buf, void **d_p, int n, double dummy);
+/* the same for the FP32 (psb_s_vectordev_mod.F90) and integer
+ * (psb_i_vectordev_mod.F90) vector types */
+int  allocateFloat(void **d, int n);
+int  allocateMultiFloat(void **d, int m, int n);
+int  writeFloat(void *d, float *h, int n);
+int  readFloat(void *d, float *h, int n);
+int  writeFloatFirst(int first, void *d, float *h, int n, int IndexBase);
+int  readFloatFirst(int first, void *d, float *h, int n, int IndexBase);
+int  writeMultiFloat(void *d, float *h, int m, int n);
+int  readMultiFloat(void *d, float *h, int m, int n);
+void freeFloat(void *d);
+int  registerMappedFloat(void *buf, void **d_p, int n, float dummy);
+int  allocateInt(void **d, int n);
+int  allocateMultiInt(void **d, int m, int n);
+int  writeInt(void *d, int *h, int n);
+int  readInt(void *d, int *h, int n);
+int  writeIntFirst(int first, void *d, int *h, int n, int IndexBase);
+int  readIntFirst(int first, void *d, int *h, int n, int IndexBase);
+int  writeMultiInt(void *d, int *h, int m, int n);
+int  readMultiInt(void *d, int *h, int m, int n);
+void freeInt(void *d);
+int  registerMappedInt(void *buf, void **d_p, int n, int dummy);
 /* dvectordev.c:101-112: x(first:last) = val (indexBase-relative) */
 int  setscalMultiVecDeviceDouble(double val, int first, int last,
                                  int indexBase, void *devVecX);
@@ -147,6 +186,79 @@ int  iscatMultiVecDeviceDoubleVecIdx(void *deviceVec, int vectorId, int n,
                                      int first, void *deviceIdx, int hfirst,
                                      void *host_values, int indexBase,
                                      double beta);
+/* dvectordev.c:98-125 (psb_d_vectordev_mod.F90:176-178): x(irl(i)) = val(i)
+ * (dupl 0, overwrite) or x(irl(i)) += val(i) (dupl 1); irl, val, x device
+ * multivectors, irl indexBase-based. */
+int  geinsMultiVecDeviceDouble(int n, void *devMultiVecIrl,
+                               void *devMultiVecVal, int dupl, int indexBase,
+                               void *devMultiVecX);
+
+/* ---- FP32 vectors: cuda/svectordev.h:40-80, psb_s_vectordev_mod.F90.
+ * Same layouts and meanings as the FP64 entries.  Element-wise operations
+ * round each FP32 multiply and add; dot and nrm2 accumulate the (exact) FP64
+ * products with the compensated sum and round to FP32 once; asum sums in
+ * FP64 and rounds once (the reference's SPGPU kernels accumulate in FP32). */
+int  writeMultiVecDeviceFloatR2(void *deviceVec, float *hostVec, int ld);
+int  readMultiVecDeviceFloatR2(void *deviceVec, float *hostVec, int ld);
+int  setscalMultiVecDeviceFloat(float val, int first, int last,
+                                int indexBase, void *devVecX);
+int  scalMultiVecDeviceFloat(float alpha, void *devVecA);
+int  nrm2MultiVecDeviceFloat(float *y_res, int n, void *devVecA);
+int  amaxMultiVecDeviceFloat(float *y_res, int n, void *devVecA);
+int  asumMultiVecDeviceFloat(float *y_res, int n, void *devVecA);
+int  dotMultiVecDeviceFloat(float *y_res, int n, void *devVecA, void *devVecB);
+int  axpbyMultiVecDeviceFloat(int n, float alpha, void *devVecX, float beta,
+                              void *devVecY);
+int  upd_xyzMultiVecDeviceFloat(int n, float alpha, float beta, float gamma,
+                                float delta, void *devVecX, void *devVecY,
+                                void *devVecZ);
+int  xyzwMultiVecDeviceFloat(int n, float a, float b, float c, float d,
+                             float e, float f, void *devVecX, void *devVecY,
+                             void *devVecZ, void *devVecW);
+int  axyMultiVecDeviceFloat(int n, float alpha, void *devVecA, void *devVecB);
+int  axybzMultiVecDeviceFloat(int n, float alpha, void *devVecA,
+                              void *devVecB, float beta, void *devVecZ);
+int  absMultiVecDeviceFloat2(int n, float alpha, void *devVecA, void *devVecB);
+int  absMultiVecDeviceFloat(int n, float alpha, void *devVecA);
+int  igathMultiVecDeviceFloat(void *deviceVec, int vectorId, int n, int first,
+                              void *indexes, int hfirst, void *host_values,
+                              int indexBase);
+int  igathMultiVecDeviceFloatVecIdx(void *deviceVec, int vectorId, int n,
+                                    int first, void *deviceIdx, int hfirst,
+                                    void *host_values, int indexBase);
+int  iscatMultiVecDeviceFloat(void *deviceVec, int vectorId, int n, int first,
+                              void *indexes, int hfirst, void *host_values,
+                              int indexBase, float beta);
+int  iscatMultiVecDeviceFloatVecIdx(void *deviceVec, int vectorId, int n,
+                                    int first, void *deviceIdx, int hfirst,
+                                    void *host_values, int indexBase,
+                                    float beta);
+int  geinsMultiVecDeviceFloat(int n, void *devMultiVecIrl,
+                              void *devMultiVecVal, int dupl, int indexBase,
+                              void *devMultiVecX);
+
+/* ---- integer vectors: cuda/ivectordev.c, psb_i_vectordev_mod.F90 (the
+ * index vectors of psb_i_vect_cuda). */
+int  writeMultiVecDeviceInt(void *deviceVec, int *hostVec);
+int  writeMultiVecDeviceIntR2(void *deviceVec, int *hostVec, int ld);
+int  readMultiVecDeviceInt(void *deviceVec, int *hostVec);
+int  readMultiVecDeviceIntR2(void *deviceVec, int *hostVec, int ld);
+int  setscalMultiVecDeviceInt(int val, int first, int last, int indexBase,
+                              void *devVecX);
+int  igathMultiVecDeviceInt(void *deviceVec, int vectorId, int n, int first,
+                            void *indexes, int hfirst, void *host_values,
+                            int indexBase);
+int  igathMultiVecDeviceIntVecIdx(void *deviceVec, int vectorId, int n,
+                                  int first, void *deviceIdx, int hfirst,
+                                  void *host_values, int indexBase);
+int  iscatMultiVecDeviceInt(void *deviceVec, int vectorId, int n, int first,
+                            void *indexes, int hfirst, void *host_values,
+                            int indexBase, int beta);
+int  iscatMultiVecDeviceIntVecIdx(void *deviceVec, int vectorId, int n,
+                                  int first, void *deviceIdx, int hfirst,
+                                  void *host_values, int indexBase, int beta);
+int  geinsMultiVecDeviceInt(int n, void *devMultiVecIrl, void *devMultiVecVal,
+                            int dupl, int indexBase, void *devMultiVecX);
 
 /* ======================================================================== */
 /* HLL (hacked ELLPACK): cuda/hlldev.h:96-153, cuda/hlldev_mod.F90:37-259    */
@@ -155,6 +267,15 @@ int  iscatMultiVecDeviceDoubleVecIdx(void *deviceVec, int vectorId, int n,
 /* hkoffs[k]; irn[i] = stored entries of row i; idiag[i] = 1-based position  */
 /* of the diagonal in row i (0 if none).                                     */
 /* ======================================================================== */
+/* cuda/hlldev.h:70-93 */
+typedef struct psbx_HllDeviceParams {
+  unsigned elementType, hackSize, rows, avgNzr, nzt, allocsize, firstIndex;
+} psbx_HllDeviceParams;
+/* cuda/hlldev.c:34-49 */
+psbx_HllDeviceParams bldHllDeviceParams(unsigned hksize, unsigned rows,
+                                        unsigned nzeros, unsigned allocsize,
+                                        unsigned elementType,
+                                        unsigned firstIndex);
 int  FallocHllDevice(void **deviceMat, unsigned hksize, unsigned rows,
                      unsigned nzeros, unsigned allocsize, unsigned elementType,
                      unsigned firstIndex);
@@ -177,9 +298,16 @@ int  readHllDeviceFloat(void *deviceMat, float *val, int *ja, int *hkoffs,
 int  psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int noffs,
                            int isz, int *irn, int *hoffs, int *idisp, int *ja,
                            double *val, void *deviceMat);
+int  psiCopyCooToHlgFloat(int nr, int nc, int nza, int hacksz, int noffs,
+                          int isz, int *irn, int *hoffs, int *idisp, int *ja,
+                          float *val, void *deviceMat);
 /* cuda/hlldev.c:185-207: y = alpha*A*x + beta*y (beta == 0: y not read) */
 int  spmvHllDeviceDouble(void *deviceMat, double alpha, void *deviceX,
                          double beta, void *deviceY);
+/* cuda/hlldev.c:160-183: the FP32 product.  Each row's products (exact in
+ * FP64) are added in FP64 in stored order and rounded to FP32 once; then
+ * y = alpha*sum + beta*y in FP32 (the reference's kernel accumulates in
+ * FP32). */
 int  spmvHllDeviceFloat(void *deviceMat, float alpha, void *deviceX,
                         float beta, void *deviceY);
 
@@ -188,6 +316,21 @@ int  spmvHllDeviceFloat(void *deviceMat, float alpha, void *deviceX,
 /* rounded up to 32 (cuda/spgpu/ell.c:33-37); host arrays are pitch x        */
 /* maxRowSize column-major (psb_d_cuda_elg_to_gpu.F90:60-90).                */
 /* ======================================================================== */
+/* cuda/elldev.h:75-97 */
+typedef struct psbx_EllDeviceParams {
+  unsigned elementType, pitch, rows, columns, maxRowSize, avgRowSize,
+      firstIndex;
+} psbx_EllDeviceParams;
+/* cuda/elldev.c:36-64.  pitch is the one FallocEllDevice allocates (rows
+ * rounded up to 32), so psb_d_cuda_elg_to_gpu.F90:65 finds it equal. */
+psbx_EllDeviceParams getEllDeviceParams(unsigned rows, unsigned maxRowSize,
+                                        unsigned nnzeros, unsigned columns,
+                                        unsigned elementType,
+                                        unsigned firstIndex);
+/* elldev_mod.F90:175-185 (no definition in the reference's C glue, no
+ * caller): no ELL timer is kept; getEllTimer returns 0. */
+void resetEllTimer(void);
+double getEllTimer(void);
 int  FallocEllDevice(void **deviceMat, unsigned rows, unsigned maxRowSize,
                      unsigned nnzeros, unsigned columns, unsigned elementType,
                      unsigned firstIndex);
@@ -205,6 +348,26 @@ int  psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ldv,
                            void *deviceMat);
 int  spmvEllDeviceDouble(void *deviceMat, double alpha, void *deviceX,
                          double beta, void *deviceY);
+/* FP32 ELL (elldev.c:172-192, 317-330; psiCopyCooToElgFloat); the product
+ * sums rows like spmvHllDeviceFloat. */
+int  writeEllDeviceFloat(void *deviceMat, float *val, int *ja, int ldj,
+                         int *irn, int *idiag);
+int  readEllDeviceFloat(void *deviceMat, float *val, int *ja, int ldj,
+                        int *irn, int *idiag);
+int  psiCopyCooToElgFloat(int nr, int nc, int nza, int hacksz, int ldv,
+                          int nzm, int *irn, int *idisp, int *ja, float *val,
+                          void *deviceMat);
+int  spmvEllDeviceFloat(void *deviceMat, float alpha, void *deviceX,
+                        float beta, void *deviceY);
+/* elldev.c:607-644 (ell_csput_base.cuh): for i < nnz, the stored entry of
+ * row ia[i] (1-based) in column ja[i] takes the value val[i] (a binary
+ * search over the row's ascending columns; absent entries are skipped).
+ * ia, ja: integer device multivectors; val: a device multivector of the
+ * matrix's type. */
+int  dev_csputEllDeviceDouble(void *deviceMat, int nnz, void *ia, void *ja,
+                              void *val);
+int  dev_csputEllDeviceFloat(void *deviceMat, int nnz, void *ia, void *ja,
+                             void *val);
 
 /* ======================================================================== */
 /* CSR (replaces the cuSPARSE-backed CSRG of cuda/d_cusparse_mod.F90:36-190; */
@@ -225,6 +388,22 @@ int d_CSRGDevice2Host(psbx_d_Cmat *Mat, int m, int n, int nz, int *irp,
 /* y = alpha*A*x + beta*y with x, y MultiVectDevice handles */
 int d_spmvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX,
                      double beta, void *deviceY);
+/* fcusparse_fct.h:132-220 (cusparseSpSV): y = alpha * T^{-1} x, T the
+ * triangle selected by d_CSRGDeviceSetMatFillMode (0 lower, 1 upper), with a
+ * unit diagonal when d_CSRGDeviceSetMatDiagType set 1 (the stored diagonal
+ * is then ignored); entries outside the triangle are ignored, a row without
+ * a stored diagonal (non-unit) is divided by 1.  Rows are solved in order
+ * with the sums of base/serial/impl/psb_d_csr_impl.F90:890-940, alpha
+ * applied after (:862-873).  beta is not used (as in cusparseSpSV).  Returns
+ * PSBX_TIMEOUT if a row's wait for its dependencies ran past its bound. */
+int d_spsvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX,
+                     double beta, void *deviceY);
+/* fcusparse_fct.h:465-471: 1 until the first d_spsvCSRGDevice call. */
+int d_CSRGIsNullSvBuffer(psbx_d_Cmat *Mat);
+/* base_cusparse_mod.F90:83-96 (fcusparse.c:44-70): no cuSPARSE handle is
+ * needed; Create initialises the library context, both return 0. */
+int FcusparseCreate(void);
+int FcusparseDestroy(void);
 
 /* ======================================================================== */
 /* Additions (no one-to-one counterpart in the reference glue)               */

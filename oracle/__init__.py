@@ -29,6 +29,7 @@ _lib = None
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 
 def build() -> str:
@@ -145,6 +146,9 @@ def lib():
             "or_upd_xyz": (None, [I, D, D, D, D, _f64p, _f64p, _f64p]),
             "or_xyzw": (None, [I, D, D, D, D, D, D, _f64p, _f64p, _f64p, _f64p]),
             "or_diag_prec_build": (None, [I, _f64p, _f64p]),
+            "or_hll_csmv_f32": (I, [I, I, I, _i32p, _i32p, _i32p, _f32p, C.c_float, _f32p, C.c_float, _f32p]),
+            "or_ell_csmv_f32": (I, [I, I, _i32p, _i32p, _f32p, C.c_float, _f32p, C.c_float, _f32p]),
+            "or_csr_trsv": (I, [I, _i32p, _i32p, _f64p, I, I, D, _f64p, _f64p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -252,6 +256,38 @@ def ell_csmv(e, nr, alpha, x, beta, y, trans="N", nc=None):
     return y
 
 
+def hll_csmv_f32(h, nr, alpha, x, beta, y, reference_fp32=False):
+    """FP32 HLL product (not transposed).  By default the library's
+    documented form (FP64 sums of exact products, rounded once); with
+    reference_fp32 the reference's FP32 accumulation (psb_s_hll_csmv)."""
+    y = np.ascontiguousarray(y, np.float32).copy()
+    lib().or_hll_csmv_f32(1 if reference_fp32 else 0, int(nr), int(h["hksz"]), _i32(h["irn"]), _i32(h["hkoffs"]),
+                          _i32(h["ja"]) if len(h["ja"]) else np.zeros(1, np.int32),
+                          np.ascontiguousarray(h["val"], np.float32) if len(h["val"]) else np.zeros(1, np.float32),
+                          float(alpha), np.ascontiguousarray(x, np.float32), float(beta), y)
+    return y
+
+
+def ell_csmv_f32(e, nr, alpha, x, beta, y):
+    """FP32 ELL product in the library's documented form (as hll_csmv_f32)."""
+    y = np.ascontiguousarray(y, np.float32).copy()
+    lib().or_ell_csmv_f32(int(nr), int(e["ldv"]), _i32(e["irn"]), _i32(e["ja"]),
+                          np.ascontiguousarray(e["val"], np.float32), float(alpha),
+                          np.ascontiguousarray(x, np.float32), float(beta), y)
+    return y
+
+
+def csr_trsv(irp, ja, val, lower, unit, alpha, x):
+    """psb_d_csr_cssv restated (not transposed, beta 0): y = alpha*T^{-1}x
+    with the CPU type's triangle storage (diagonal last in a lower row, first
+    in an upper row, absent when unit)."""
+    n = len(irp) - 1
+    y = np.zeros(n)
+    lib().or_csr_trsv(n, _i32(irp), _i32(ja), _f64(val), int(bool(lower)), int(bool(unit)), float(alpha),
+                      _f64(x), y)
+    return y
+
+
 def hll_get_diag(h, nr):
     d = np.zeros(nr, np.float64)
     lib().or_hll_get_diag(int(nr), int(h["hksz"]), h["irn"], h["hkoffs"],
@@ -304,6 +340,63 @@ def xyzw(a, b, c, d, e, f, x, y, z, w):
     y, z, w = _f64(y).copy(), _f64(z).copy(), _f64(w).copy()
     lib().or_xyzw(len(y), a, b, c, d, e, f, _f64(x), y, z, w)
     return y, z, w
+
+
+# FP32 vectors (the s type): the CPU loops of psi_s_serial_impl.F90 are the
+# FP64 ones with real(psb_spk_) -- every multiply and add rounded to FP32,
+# which numpy's float32 operations do one at a time.  The reductions restate
+# the library's documented form: dot and nrm2 are the compensated FP64 sums
+# of the (exact) FP64 products rounded to FP32 once, asum the FP64 sum
+# rounded once, amax exact.
+_F = np.float32
+
+
+def saxpby(alpha, x, beta, y):
+    x, y = np.asarray(x, _F), np.asarray(y, _F)
+    a, b = _F(alpha), _F(beta)
+    if a == 0:
+        return np.zeros_like(y) if b == 0 else (y.copy() if b == 1 else b * y)
+    return a * x if b == 0 else a * x + b * y
+
+
+def _axpby_el(a, x, b, y):
+    if a == 0:
+        return np.zeros_like(y) if b == 0 else b * y
+    return a * x if b == 0 else a * x + b * y
+
+
+def supd_xyz(alpha, beta, gamma, delta, x, y, z):
+    x, y, z = (np.asarray(v, _F) for v in (x, y, z))
+    yy = _axpby_el(_F(alpha), x, _F(beta), y)
+    return yy, _axpby_el(_F(gamma), yy, _F(delta), z)
+
+
+def sxyzw(a, b, c, d, e, f, x, y, z, w):
+    x, y, z, w = (np.asarray(v, _F) for v in (x, y, z, w))
+    yy = _F(a) * x + _F(b) * y
+    zz = _F(c) * yy + _F(d) * z
+    return yy, zz, _F(e) * zz + _F(f) * w
+
+
+def smlt(alpha, d, x, beta, z):
+    t = _F(alpha) * (np.asarray(d, _F) * np.asarray(x, _F))
+    return t if _F(beta) == 0 else t + _F(beta) * np.asarray(z, _F)
+
+
+def sdot(x, y):
+    return _F(dot(np.asarray(x, _F).astype(np.float64), np.asarray(y, _F).astype(np.float64)))
+
+
+def snrm2(x):
+    return _F(nrm2(np.asarray(x, _F).astype(np.float64)))
+
+
+def sasum(x):
+    return _F(asum(np.asarray(x, _F).astype(np.float64)))
+
+
+def samax(x):
+    return _F(np.max(np.abs(np.asarray(x, _F)))) if len(x) else _F(0)
 
 
 def diag_prec_build(diag):

@@ -287,6 +287,103 @@ int or_hll_csmv(char trans, int nr, int nc, int hksz, const int *irn,
   return 0;
 }
 
+/* FP32 HLL / ELL products y = alpha*A*x + beta*y (not transposed).
+ * mode 0 restates the library's documented form (include/psbx.h,
+ * spmvHllDeviceFloat): each product of two floats is formed exactly in
+ * FP64, the products are added in FP64 in stored order, the sum is rounded
+ * to FP32 once, then y = alpha*sum + beta*y in FP32 (beta == 0: y not read;
+ * alpha == 0: y = beta*y, 0 when beta == 0).
+ * mode 1 restates the reference's FP32 CPU product psb_s_hll_csmv
+ * (ext/impl/psb_s_hll_csmv.f90, the inner form of psb_d_hll_csmv.f90:345-360
+ * with real(psb_spk_)): acc = acc + val*x(ja) in FP32 -- the bar the
+ * library's FP32 product is compared with through the FP32 error bound. */
+static float f32_finish(float alpha, float acc, float beta, float y)
+{
+  float t = alpha * acc;
+  return beta == 0.0f ? t : t + beta * y;
+}
+
+int or_hll_csmv_f32(int mode, int nr, int hksz, const int *irn, const int *hkoffs,
+                    const int *hja, const float *hval, float alpha, const float *x,
+                    float beta, float *y)
+{
+  int nhk = (nr + hksz - 1) / hksz;
+  if (alpha == 0.0f) {
+    for (int i = 0; i < nr; i++) y[i] = beta == 0.0f ? 0.0f : beta * y[i];
+    return 0;
+  }
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+  for (int h = 0; h < nhk; h++) {
+    int i0 = h * hksz;
+    int ir = (hksz < nr - i0) ? hksz : nr - i0;
+    const int *hj = hja + hkoffs[h];
+    const float *hv = hval + hkoffs[h];
+    for (int ii = 0; ii < ir; ii++) {
+      float acc;
+      if (mode == 0) {
+        double a = 0.0;
+        for (int jj = 0; jj < irn[i0 + ii]; jj++)
+          a = a + (double)hv[(int64_t)jj * hksz + ii] * (double)x[hj[(int64_t)jj * hksz + ii] - 1];
+        acc = (float)a;
+      } else {
+        acc = 0.0f;
+        for (int jj = 0; jj < irn[i0 + ii]; jj++)
+          acc = acc + hv[(int64_t)jj * hksz + ii] * x[hj[(int64_t)jj * hksz + ii] - 1];
+      }
+      y[i0 + ii] = f32_finish(alpha, acc, beta, beta == 0.0f ? 0.0f : y[i0 + ii]);
+    }
+  }
+  return 0;
+}
+
+int or_ell_csmv_f32(int nr, int ldv, const int *irn, const int *eja, const float *eval,
+                    float alpha, const float *x, float beta, float *y)
+{
+  if (alpha == 0.0f) {
+    for (int i = 0; i < nr; i++) y[i] = beta == 0.0f ? 0.0f : beta * y[i];
+    return 0;
+  }
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+  for (int i = 0; i < nr; i++) {
+    double a = 0.0;
+    for (int j = 0; j < irn[i]; j++)
+      a = a + (double)eval[(int64_t)j * ldv + i] * (double)x[eja[(int64_t)j * ldv + i] - 1];
+    y[i] = f32_finish(alpha, (float)a, beta, beta == 0.0f ? 0.0f : y[i]);
+  }
+  return 0;
+}
+
+/* Triangular solve of psb_d_csr_cssv (base/serial/impl/psb_d_csr_impl.F90:
+ * 782-1041), not transposed, beta == 0: inner_csrsv (:890-940) then
+ * y = alpha*y (:862-873).  The storage is the CPU type's: a lower triangle
+ * keeps its diagonal as the last entry of each row and an upper one as the
+ * first, unless unit (no diagonal stored).  1-based irp/ja. */
+int or_csr_trsv(int n, const int *irp, const int *ja, const double *val, int lower,
+                int unit, double alpha, const double *x, double *y)
+{
+  if (lower) {
+    for (int i = 0; i < n; i++) {
+      double acc = 0.0;
+      int e = unit ? irp[i + 1] - 1 : irp[i + 1] - 2;
+      for (int j = irp[i]; j <= e; j++) acc = acc + val[j - 1] * y[ja[j - 1] - 1];
+      y[i] = unit ? x[i] - acc : (x[i] - acc) / val[irp[i + 1] - 2];
+    }
+  } else {
+    for (int i = n - 1; i >= 0; i--) {
+      double acc = 0.0;
+      int b = unit ? irp[i] : irp[i] + 1;
+      for (int j = b; j <= irp[i + 1] - 1; j++) acc = acc + val[j - 1] * y[ja[j - 1] - 1];
+      y[i] = unit ? x[i] - acc : (x[i] - acc) / val[irp[i] - 1];
+    }
+  }
+  if (alpha == -1.0) {
+    for (int i = 0; i < n; i++) y[i] = -y[i];
+  } else if (alpha != 1.0) {
+    for (int i = 0; i < n; i++) y[i] = alpha * y[i];
+  }
+  return 0;
+}
+
 int or_ell_csmv(char trans, int nr, int nc, int ldv, int nzm, const int *irn,
                 const int *eja, const double *eval, double alpha,
                 const double *x, double beta, double *y)

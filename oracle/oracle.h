@@ -47,6 +47,13 @@ int or_hll_csmv(char trans, int nr, int nc, int hksz, const int *irn,
 int or_ell_csmv(char trans, int nr, int nc, int ldv, int nzm, const int *irn,
                 const int *eja, const double *eval, double alpha,
                 const double *x, double beta, double *y);
+int or_hll_csmv_f32(int mode, int nr, int hksz, const int *irn, const int *hkoffs,
+                    const int *hja, const float *hval, float alpha, const float *x,
+                    float beta, float *y);
+int or_ell_csmv_f32(int nr, int ldv, const int *irn, const int *eja, const float *eval,
+                    float alpha, const float *x, float beta, float *y);
+int or_csr_trsv(int n, const int *irp, const int *ja, const double *val, int lower,
+                int unit, double alpha, const double *x, double *y);
 int or_hll_get_diag(int nr, int hksz, const int *irn, const int *hkoffs,
                     const double *hval, const int *idiag, double *d);
 

@@ -35,6 +35,19 @@ class Cmat(C.Structure):
 
 
 PC = C.POINTER(Cmat)
+PF = C.POINTER(C.c_float)
+
+
+class HllDeviceParams(C.Structure):
+    """psbx_HllDeviceParams == HllDeviceParams of cuda/hlldev.h:70-93."""
+    _fields_ = [(k, C.c_uint) for k in ("elementType", "hackSize", "rows", "avgNzr", "nzt", "allocsize",
+                                        "firstIndex")]
+
+
+class EllDeviceParams(C.Structure):
+    """psbx_EllDeviceParams == EllDeviceParams of cuda/elldev.h:75-97."""
+    _fields_ = [(k, C.c_uint) for k in ("elementType", "pitch", "rows", "columns", "maxRowSize", "avgRowSize",
+                                        "firstIndex")]
 
 _SIGS = {
     # environment
@@ -64,7 +77,36 @@ _SIGS = {
     "igathMultiVecDeviceDoubleVecIdx": (I, [P, I, I, I, P, I, P, I]),
     "iscatMultiVecDeviceDouble": (I, [P, I, I, I, P, I, P, I, D]),
     "iscatMultiVecDeviceDoubleVecIdx": (I, [P, I, I, I, P, I, P, I, D]),
+    "geinsMultiVecDeviceDouble": (I, [I, P, P, I, I, P]),
+    # plain device buffers and mapped host memory
+    "unregisterMapped": (I, [P]),
+    # FP32 vectors
+    "writeMultiVecDeviceFloatR2": (I, [P, P, I]), "readMultiVecDeviceFloatR2": (I, [P, P, I]),
+    "setscalMultiVecDeviceFloat": (I, [F, I, I, I, P]), "scalMultiVecDeviceFloat": (I, [F, P]),
+    "nrm2MultiVecDeviceFloat": (I, [PF, I, P]), "amaxMultiVecDeviceFloat": (I, [PF, I, P]),
+    "asumMultiVecDeviceFloat": (I, [PF, I, P]), "dotMultiVecDeviceFloat": (I, [PF, I, P, P]),
+    "axpbyMultiVecDeviceFloat": (I, [I, F, P, F, P]),
+    "upd_xyzMultiVecDeviceFloat": (I, [I, F, F, F, F, P, P, P]),
+    "xyzwMultiVecDeviceFloat": (I, [I, F, F, F, F, F, F, P, P, P, P]),
+    "axyMultiVecDeviceFloat": (I, [I, F, P, P]), "axybzMultiVecDeviceFloat": (I, [I, F, P, P, F, P]),
+    "absMultiVecDeviceFloat2": (I, [I, F, P, P]), "absMultiVecDeviceFloat": (I, [I, F, P]),
+    "igathMultiVecDeviceFloat": (I, [P, I, I, I, P, I, P, I]),
+    "igathMultiVecDeviceFloatVecIdx": (I, [P, I, I, I, P, I, P, I]),
+    "iscatMultiVecDeviceFloat": (I, [P, I, I, I, P, I, P, I, F]),
+    "iscatMultiVecDeviceFloatVecIdx": (I, [P, I, I, I, P, I, P, I, F]),
+    "geinsMultiVecDeviceFloat": (I, [I, P, P, I, I, P]),
+    # integer vectors
+    "writeMultiVecDeviceInt": (I, [P, P]), "writeMultiVecDeviceIntR2": (I, [P, P, I]),
+    "readMultiVecDeviceInt": (I, [P, P]), "readMultiVecDeviceIntR2": (I, [P, P, I]),
+    "setscalMultiVecDeviceInt": (I, [I, I, I, I, P]),
+    "igathMultiVecDeviceInt": (I, [P, I, I, I, P, I, P, I]),
+    "igathMultiVecDeviceIntVecIdx": (I, [P, I, I, I, P, I, P, I]),
+    "iscatMultiVecDeviceInt": (I, [P, I, I, I, P, I, P, I, I]),
+    "iscatMultiVecDeviceIntVecIdx": (I, [P, I, I, I, P, I, P, I, I]),
+    "geinsMultiVecDeviceInt": (I, [I, P, P, I, I, P]),
     # HLL
+    "bldHllDeviceParams": (HllDeviceParams, [U, U, U, U, U, U]),
+    "psiCopyCooToHlgFloat": (I, [I, I, I, I, I, I, P, P, P, P, P, P]),
     "FallocHllDevice": (I, [PP, U, U, U, U, U, U]), "freeHllDevice": (None, [P]),
     "getHllDeviceParams": (I, [P, PI, PI, PI, PI, PI, PI, PI]),
     "writeHllDeviceDouble": (I, [P, P, P, P, P, P]), "readHllDeviceDouble": (I, [P, P, P, P, P, P]),
@@ -77,6 +119,12 @@ _SIGS = {
     "writeEllDeviceDouble": (I, [P, P, P, I, P, P]), "readEllDeviceDouble": (I, [P, P, P, I, P, P]),
     "psiCopyCooToElgDouble": (I, [I, I, I, I, I, I, P, P, P, P, P]),
     "spmvEllDeviceDouble": (I, [P, D, P, D, P]),
+    "getEllDeviceParams": (EllDeviceParams, [U, U, U, U, U, U]),
+    "resetEllTimer": (None, []), "getEllTimer": (D, []),
+    "writeEllDeviceFloat": (I, [P, P, P, I, P, P]), "readEllDeviceFloat": (I, [P, P, P, I, P, P]),
+    "psiCopyCooToElgFloat": (I, [I, I, I, I, I, I, P, P, P, P, P]),
+    "spmvEllDeviceFloat": (I, [P, F, P, F, P]),
+    "dev_csputEllDeviceDouble": (I, [P, I, P, P, P]), "dev_csputEllDeviceFloat": (I, [P, I, P, P, P]),
     # CSR
     "d_CSRGDeviceAlloc": (I, [PC, I, I, I]), "d_CSRGDeviceFree": (I, [PC]),
     "d_CSRGDeviceGetParms": (I, [PC, PI, PI, PI]), "d_CSRGDeviceSetMatType": (I, [PC, I]),
@@ -84,6 +132,8 @@ _SIGS = {
     "d_CSRGDeviceSetMatIndexBase": (I, [PC, I]),
     "d_CSRGHost2Device": (I, [PC, I, I, I, P, P, P]), "d_CSRGDevice2Host": (I, [PC, I, I, I, P, P, P]),
     "d_spmvCSRGDevice": (I, [PC, D, P, D, P]),
+    "d_spsvCSRGDevice": (I, [PC, D, P, D, P]), "d_CSRGIsNullSvBuffer": (I, [PC]),
+    "FcusparseCreate": (I, []), "FcusparseDestroy": (I, []),
     # additions
     "psbx_DefaultSolverOptions": (I, [C.POINTER(SolverOptions)]),
     "psbx_dkrylov": (I, [CH, P, I, P, P, P, C.POINTER(SolverOptions)]),
@@ -103,6 +153,15 @@ _SIGS = {
     "psbx_batch_destroy": (I, [P]),
     "psbx_kernel_launches": (C.c_uint64, []), "psbx_last_error": (C.c_char_p, []),
 }
+
+for _t, _c in (("Int", C.c_int), ("Float", C.c_float), ("Double", C.c_double)):
+    _SIGS.update({
+        f"allocate{_t}": (I, [PP, I]), f"allocateMulti{_t}": (I, [PP, I, I]),
+        f"write{_t}": (I, [P, P, I]), f"read{_t}": (I, [P, P, I]),
+        f"write{_t}First": (I, [I, P, P, I, I]), f"read{_t}First": (I, [I, P, P, I, I]),
+        f"writeMulti{_t}": (I, [P, P, I, I]), f"readMulti{_t}": (I, [P, P, I, I]),
+        f"free{_t}": (None, [P]), f"registerMapped{_t}": (I, [P, PP, I, _c]),
+    })
 
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)

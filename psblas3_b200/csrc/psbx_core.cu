@@ -151,6 +151,88 @@ void psb_cudaSetStream(void *stream) {
   c.stream = stream ? (cudaStream_t)stream : c.defaultStream;
 }
 
+// ---------------------------------------------------------------------------
+// Plain device buffers: the "simple memory tools" of cuda/cuda_util.c:440-662
+// (allocateInt/Float/Double, write*/read* whole, from an indexBase-based
+// first entry, or m*n entries, free*), used by the Fortran vector types for
+// their gather/scatter buffers (psb_d_cuda_vect_mod.F90:155-549).  Raw
+// device pointers; copies run on the library stream and return when done.
+// ---------------------------------------------------------------------------
+static int buf_alloc(void **d, long long bytes) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  if (!d || bytes < 0) return SPGPU_UNSUPPORTED;
+  cudaError_t e = cudaMalloc(d, bytes > 0 ? (size_t)bytes : 16);
+  if (e != cudaSuccess) {
+    *d = nullptr;
+    return psbx_cuda_status(e, "allocate (device buffer)");
+  }
+  return SPGPU_SUCCESS;
+}
+
+static int buf_copy(void *dst, const void *src, long long bytes, cudaMemcpyKind kind) {
+  if (bytes <= 0) return SPGPU_SUCCESS;
+  if (!dst || !src) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  PSBX_CK(cudaMemcpyAsync(dst, src, (size_t)bytes, kind, c.stream));
+  PSBX_CK(cudaStreamSynchronize(c.stream));
+  return SPGPU_SUCCESS;
+}
+
+static void buf_free(void *d) {
+  if (!d) return;
+  if (g_ctx.init) cudaStreamSynchronize(g_ctx.stream);
+  cudaFree(d);
+}
+
+// cudaHostRegister with the mapped flag, then the device alias of the host
+// buffer (cuda_util.c:104-130).
+static int map_host(void *buf, void **dp, long long bytes) {
+  if (!buf || !dp || bytes <= 0) return SPGPU_UNSUPPORTED;
+  PSBX_CK(cudaHostRegister(buf, (size_t)bytes, cudaHostRegisterMapped));
+  PSBX_CK(cudaHostGetDevicePointer(dp, buf, 0));
+  return SPGPU_SUCCESS;
+}
+
+#define PSBX_BUFFER_TOOLS(NAME, T)                                                                    \
+  int allocate##NAME(void **d, int n) { return buf_alloc(d, (long long)n * sizeof(T)); }               \
+  int allocateMulti##NAME(void **d, int m, int n) { return buf_alloc(d, (long long)m * n * sizeof(T)); } \
+  int write##NAME(void *d, T *h, int n) {                                                               \
+    return buf_copy(d, h, (long long)n * sizeof(T), cudaMemcpyHostToDevice);                           \
+  }                                                                                                     \
+  int read##NAME(void *d, T *h, int n) { return buf_copy(h, d, (long long)n * sizeof(T), cudaMemcpyDeviceToHost); } \
+  int write##NAME##First(int first, void *d, T *h, int n, int IndexBase) {                              \
+    if (!d) return SPGPU_UNSUPPORTED;                                                                   \
+    return buf_copy((T *)d + (first - IndexBase), h, (long long)n * sizeof(T), cudaMemcpyHostToDevice); \
+  }                                                                                                     \
+  int read##NAME##First(int first, void *d, T *h, int n, int IndexBase) {                               \
+    if (!d) return SPGPU_UNSUPPORTED;                                                                   \
+    return buf_copy(h, (T *)d + (first - IndexBase), (long long)n * sizeof(T), cudaMemcpyDeviceToHost); \
+  }                                                                                                     \
+  int writeMulti##NAME(void *d, T *h, int m, int n) {                                                   \
+    return buf_copy(d, h, (long long)m * n * sizeof(T), cudaMemcpyHostToDevice);                       \
+  }                                                                                                     \
+  int readMulti##NAME(void *d, T *h, int m, int n) {                                                    \
+    return buf_copy(h, d, (long long)m * n * sizeof(T), cudaMemcpyDeviceToHost);                       \
+  }                                                                                                     \
+  void free##NAME(void *d) { buf_free(d); }                                                             \
+  int registerMapped##NAME(void *buf, void **d_p, int n, T dummy) {                                     \
+    (void)dummy;                                                                                        \
+    return map_host(buf, d_p, (long long)n * sizeof(T));                                               \
+  }
+
+PSBX_BUFFER_TOOLS(Int, int)
+PSBX_BUFFER_TOOLS(Float, float)
+PSBX_BUFFER_TOOLS(Double, double)
+#undef PSBX_BUFFER_TOOLS
+
+// cuda/vectordev.c:145-148
+int unregisterMapped(void *buf) {
+  if (!buf) return SPGPU_UNSUPPORTED;
+  PSBX_CK(cudaHostUnregister(buf));
+  return SPGPU_SUCCESS;
+}
+
 int psbx_DefaultSolverOptions(psbx_SolverOptions *opt) {
   // cbind/krylov/psb_base_krylov_cbind_mod.f90:13-26 defaults
   if (!opt) return SPGPU_UNSUPPORTED;

@@ -114,6 +114,20 @@ int getHllDeviceParams(void *deviceMat, int *hksize, int *rows, int *nzeros, int
   return SPGPU_SUCCESS;
 }
 
+// cuda/hlldev.c:34-49: the parameter block FallocHllDevice is built from.
+psbx_HllDeviceParams bldHllDeviceParams(unsigned hksize, unsigned rows, unsigned nzeros, unsigned allocsize,
+                                        unsigned elementType, unsigned firstIndex) {
+  psbx_HllDeviceParams p;
+  p.elementType = elementType;
+  p.hackSize = hksize;
+  p.rows = rows;
+  p.avgNzr = rows ? (nzeros + rows - 1) / rows : 0;
+  p.nzt = nzeros;
+  p.allocsize = allocsize;
+  p.firstIndex = firstIndex;
+  return p;
+}
+
 static int hll_copy(void *deviceMat, void *val, int *ja, int *hkoffs, int *irn, int *idiag, bool write, int type) {
   HllDevice *m = (HllDevice *)deviceMat;
   if (!m || m->elemType != type) return SPGPU_UNSUPPORTED;
@@ -227,19 +241,19 @@ __global__ void k_coo_to_hll(int nr, int hksz, int base, int nrpad, const int *_
   }
 }
 
-extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int noffs, int isz, int *irn, int *hoffs,
-                                     int *idisp, int *ja, double *val, void *deviceMat) {
+template <class T>
+static int coo_to_hll(int nr, int nza, int hacksz, int noffs, int isz, int *irn, int *hoffs, int *idisp, int *ja,
+                      T *val, void *deviceMat, int type) {
   HllDevice *m = (HllDevice *)deviceMat;
-  if (!m || m->elemType != SPGPU_TYPE_DOUBLE || m->rows != nr || m->hackSize != hacksz) return SPGPU_UNSUPPORTED;
+  if (!m || m->elemType != type || m->rows != nr || m->hackSize != hacksz) return SPGPU_UNSUPPORTED;
   if (noffs != m->hackOffsLength || isz > m->allocsize) return SPGPU_UNSUPPORTED;
-  (void)nc;
   PsbxCtx &c = psbx_ctx();
   int *dIdisp = nullptr, *dJa = nullptr;
-  double *dVal = nullptr;
+  T *dVal = nullptr;
   int rc = dmalloc((void **)&dIdisp, sizeof(int) * (size_t)(nr + 1));
   if (!rc) rc = dmalloc((void **)&dJa, sizeof(int) * (size_t)nza);
-  if (!rc) rc = dmalloc((void **)&dVal, sizeof(double) * (size_t)nza);
-  if (!rc) rc = h2d(dVal, val, sizeof(double) * (size_t)nza);
+  if (!rc) rc = dmalloc((void **)&dVal, sizeof(T) * (size_t)nza);
+  if (!rc) rc = h2d(dVal, val, sizeof(T) * (size_t)nza);
   if (!rc) rc = h2d(dJa, ja, sizeof(int) * (size_t)nza);
   if (!rc) rc = h2d(m->rS, irn, sizeof(int) * (size_t)nr);
   if (!rc) rc = h2d(m->hackOffs, hoffs, sizeof(int) * (size_t)(noffs + 1));
@@ -250,10 +264,9 @@ extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int no
     int jc = 1;
     if (nza > 0) jc = ja[(nr > 1 && idisp[1] < nza) ? idisp[1] : 0];
     const int nrpad = noffs * hacksz;
-    const int T = 256;
-    k_coo_to_hll<double><<<(nrpad + T - 1) / T, T, 0, c.stream>>>(nr, hacksz, m->baseIndex, nrpad, m->rS,
-                                                                  m->hackOffs, dIdisp, dJa, dVal, jc, m->diag,
-                                                                  m->rP, (double *)m->cM);
+    const int TB = 256;
+    k_coo_to_hll<T><<<(nrpad + TB - 1) / TB, TB, 0, c.stream>>>(nr, hacksz, m->baseIndex, nrpad, m->rS, m->hackOffs,
+                                                               dIdisp, dJa, dVal, jc, m->diag, m->rP, (T *)m->cM);
     psbx_count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "k_coo_to_hll");
@@ -262,11 +275,23 @@ extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int no
     m->maxRowLen = mx;
   }
   if (!rc) rc = sync_stream();
-  if (!rc) rc = psbx_hll_index_long(m);
+  if (!rc && type == SPGPU_TYPE_DOUBLE) rc = psbx_hll_index_long(m);
   cudaFree(dIdisp);
   cudaFree(dJa);
   cudaFree(dVal);
   return rc;
+}
+
+extern "C" int psiCopyCooToHlgDouble(int nr, int nc, int nza, int hacksz, int noffs, int isz, int *irn, int *hoffs,
+                                     int *idisp, int *ja, double *val, void *deviceMat) {
+  (void)nc;
+  return coo_to_hll<double>(nr, nza, hacksz, noffs, isz, irn, hoffs, idisp, ja, val, deviceMat, SPGPU_TYPE_DOUBLE);
+}
+
+extern "C" int psiCopyCooToHlgFloat(int nr, int nc, int nza, int hacksz, int noffs, int isz, int *irn, int *hoffs,
+                                    int *idisp, int *ja, float *val, void *deviceMat) {
+  (void)nc;
+  return coo_to_hll<float>(nr, nza, hacksz, noffs, isz, irn, hoffs, idisp, ja, val, deviceMat, SPGPU_TYPE_FLOAT);
 }
 
 // ------------------------------------------------ CSR (device) -> HLL build
@@ -662,19 +687,19 @@ void zeroEllDevice(void *deviceMat) {
 int getEllDevicePitch(void *deviceMat) { return ((EllDevice *)deviceMat)->pitch; }
 int getEllDeviceMaxRowSize(void *deviceMat) { return ((EllDevice *)deviceMat)->maxRowSize; }
 
-static int ell_copy(void *deviceMat, double *val, int *ja, int ldj, int *irn, int *idiag, bool write) {
+static int ell_copy(void *deviceMat, void *val, int *ja, int ldj, int *irn, int *idiag, bool write, int type) {
   EllDevice *m = (EllDevice *)deviceMat;
-  if (!m || m->dataType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  if (!m || m->dataType != type) return SPGPU_UNSUPPORTED;
   if (ldj != m->pitch) return SPGPU_UNSUPPORTED;  // host arrays must be pitch x maxRowSize
-  size_t as = (size_t)m->allocsize, nr = (size_t)m->rows;
+  size_t as = (size_t)m->allocsize, nr = (size_t)m->rows, es = vsize(type);
   int rc;
   if (write) {
-    rc = h2d(m->cM, val, as * 8);
+    rc = h2d(m->cM, val, as * es);
     if (!rc) rc = h2d(m->rP, ja, as * 4);
     if (!rc) rc = h2d(m->rS, irn, nr * 4);
     if (!rc) rc = h2d(m->diag, idiag, nr * 4);
   } else {
-    rc = d2h(val, m->cM, as * 8);
+    rc = d2h(val, m->cM, as * es);
     if (!rc) rc = d2h(ja, m->rP, as * 4);
     if (!rc) rc = d2h(irn, m->rS, nr * 4);
     if (!rc) rc = d2h(idiag, m->diag, nr * 4);
@@ -684,10 +709,53 @@ static int ell_copy(void *deviceMat, double *val, int *ja, int ldj, int *irn, in
 }
 
 int writeEllDeviceDouble(void *deviceMat, double *val, int *ja, int ldj, int *irn, int *idiag) {
-  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, true);
+  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, true, SPGPU_TYPE_DOUBLE);
 }
 int readEllDeviceDouble(void *deviceMat, double *val, int *ja, int ldj, int *irn, int *idiag) {
-  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, false);
+  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, false, SPGPU_TYPE_DOUBLE);
+}
+int writeEllDeviceFloat(void *deviceMat, float *val, int *ja, int ldj, int *irn, int *idiag) {
+  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, true, SPGPU_TYPE_FLOAT);
+}
+int readEllDeviceFloat(void *deviceMat, float *val, int *ja, int ldj, int *irn, int *idiag) {
+  return ell_copy(deviceMat, val, ja, ldj, irn, idiag, false, SPGPU_TYPE_FLOAT);
+}
+
+// cuda/elldev.c:36-64.  The pitch reported is the one FallocEllDevice uses
+// (rows rounded up to 32), so psb_d_cuda_elg_to_gpu's comparison of the two
+// (psb_d_cuda_elg_to_gpu.F90:65) holds and the object is not reallocated on
+// every upload.
+psbx_EllDeviceParams getEllDeviceParams(unsigned rows, unsigned maxRowSize, unsigned nnzeros, unsigned columns,
+                                        unsigned elementType, unsigned firstIndex) {
+  psbx_EllDeviceParams p;
+  p.elementType = elementType;
+  p.pitch = (unsigned)ell_pitch((int)rows);
+  p.rows = rows;
+  p.columns = columns;
+  p.maxRowSize = maxRowSize;
+  p.avgRowSize = rows ? (nnzeros + rows - 1) / rows : 0;
+  p.firstIndex = firstIndex;
+  return p;
+}
+
+// elldev_mod.F90:175-185 declares these; the reference's C glue defines
+// neither and no Fortran routine calls them.  They exist so the module
+// links: the library keeps no ELL timer, so the time is always 0.
+void resetEllTimer(void) {}
+double getEllTimer(void) { return 0.0; }
+
+int spmvEllDeviceFloat(void *deviceMat, float alpha, void *deviceX, float beta, void *deviceY) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  MultiVectDevice *x = (MultiVectDevice *)deviceX, *y = (MultiVectDevice *)deviceY;
+  if (!m || !x || !y || y->size_ < m->rows) return SPGPU_UNSUPPORTED;
+  if (x->elemType != SPGPU_TYPE_FLOAT || y->elemType != SPGPU_TYPE_FLOAT) return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  for (int v = 0; v < y->count_ && v < x->count_; v++) {
+    int rc = psbx_launch_ell_spmv_f32(m, alpha, (const float *)x->v_ + (size_t)v * x->pitch_, beta,
+                                      (float *)y->v_ + (size_t)v * y->pitch_, c.stream);
+    if (rc) return rc;
+  }
+  return SPGPU_SUCCESS;
 }
 
 int spmvEllDeviceDouble(void *deviceMat, double alpha, void *deviceX, double beta, void *deviceY) {
@@ -707,16 +775,17 @@ int spmvEllDeviceDouble(void *deviceMat, double alpha, void *deviceX, double bet
 
 // COO -> ELL scatter on the device (psi_cuda_CopyCooToElg.cuh): padding as
 // the CPU converter (last column of the row; first COO column if empty).
+template <class T>
 __global__ void k_coo_to_ell(int nr, int nzm, int pitch, int base, const int *__restrict__ rS,
                              const int *__restrict__ idisp, const int *__restrict__ cja,
-                             const double *__restrict__ cval, int *__restrict__ idiag, int *__restrict__ rP,
-                             double *__restrict__ cM) {
+                             const T *__restrict__ cval, int *__restrict__ idiag, int *__restrict__ rP,
+                             T *__restrict__ cM) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= pitch) return;
   if (i >= nr) {
     for (int k = 0; k < nzm; k++) {
       rP[(size_t)k * pitch + i] = 1;
-      cM[(size_t)k * pitch + i] = 0.0;
+      cM[(size_t)k * pitch + i] = T(0);
     }
     return;
   }
@@ -730,23 +799,22 @@ __global__ void k_coo_to_ell(int nr, int nzm, int pitch, int base, const int *__
   }
   for (int k = rsz; k < nzm; k++) {
     rP[(size_t)k * pitch + i] = c;
-    cM[(size_t)k * pitch + i] = 0.0;
+    cM[(size_t)k * pitch + i] = T(0);
   }
   idiag[i] = idval;
 }
 
-extern "C" int psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ldv, int nzm, int *irn, int *idisp,
-                                     int *ja, double *val, void *deviceMat) {
+template <class T>
+static int coo_to_ell(int nr, int nza, int nzm, int *irn, int *idisp, int *ja, T *val, void *deviceMat, int type) {
   EllDevice *m = (EllDevice *)deviceMat;
-  (void)nc; (void)hacksz; (void)ldv;
-  if (!m || m->dataType != SPGPU_TYPE_DOUBLE || m->rows != nr || nzm > m->maxRowSize) return SPGPU_UNSUPPORTED;
+  if (!m || m->dataType != type || m->rows != nr || nzm > m->maxRowSize) return SPGPU_UNSUPPORTED;
   PsbxCtx &c = psbx_ctx();
   int *dIdisp = nullptr, *dJa = nullptr;
-  double *dVal = nullptr;
+  T *dVal = nullptr;
   int rc = dmalloc((void **)&dIdisp, sizeof(int) * (size_t)(nr + 1));
   if (!rc) rc = dmalloc((void **)&dJa, sizeof(int) * (size_t)(nza > 0 ? nza : 1));
-  if (!rc) rc = dmalloc((void **)&dVal, sizeof(double) * (size_t)(nza > 0 ? nza : 1));
-  if (!rc) rc = h2d(dVal, val, sizeof(double) * (size_t)nza);
+  if (!rc) rc = dmalloc((void **)&dVal, sizeof(T) * (size_t)(nza > 0 ? nza : 1));
+  if (!rc) rc = h2d(dVal, val, sizeof(T) * (size_t)nza);
   if (!rc) rc = h2d(dJa, ja, sizeof(int) * (size_t)nza);
   if (!rc) rc = h2d(m->rS, irn, sizeof(int) * (size_t)nr);
   if (!rc) rc = h2d(dIdisp, idisp, sizeof(int) * (size_t)(nr + 1));
@@ -755,8 +823,8 @@ extern "C" int psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ld
     rc = h2d(dJa, &one, sizeof(int));
   }
   if (!rc && m->pitch > 0) {
-    k_coo_to_ell<<<(m->pitch + 255) / 256, 256, 0, c.stream>>>(nr, m->maxRowSize, m->pitch, m->baseIndex, m->rS,
-                                                               dIdisp, dJa, dVal, m->diag, m->rP, (double *)m->cM);
+    k_coo_to_ell<T><<<(m->pitch + 255) / 256, 256, 0, c.stream>>>(nr, m->maxRowSize, m->pitch, m->baseIndex, m->rS,
+                                                                  dIdisp, dJa, dVal, m->diag, m->rP, (T *)m->cM);
     psbx_count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = psbx_cuda_status(e, "k_coo_to_ell");
@@ -768,10 +836,77 @@ extern "C" int psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ld
   return rc;
 }
 
+extern "C" int psiCopyCooToElgDouble(int nr, int nc, int nza, int hacksz, int ldv, int nzm, int *irn, int *idisp,
+                                     int *ja, double *val, void *deviceMat) {
+  (void)nc; (void)hacksz; (void)ldv;
+  return coo_to_ell<double>(nr, nza, nzm, irn, idisp, ja, val, deviceMat, SPGPU_TYPE_DOUBLE);
+}
+
+extern "C" int psiCopyCooToElgFloat(int nr, int nc, int nza, int hacksz, int ldv, int nzm, int *irn, int *idisp,
+                                    int *ja, float *val, void *deviceMat) {
+  (void)nc; (void)hacksz; (void)ldv;
+  return coo_to_ell<float>(nr, nza, nzm, irn, idisp, ja, val, deviceMat, SPGPU_TYPE_FLOAT);
+}
+
+// dev_csputEllDevice{Double,Float} (cuda/elldev.c:607-644, kernel
+// ell_csput_base.cuh): overwrite the values of entries already present in
+// the pattern.  Entry i of the update names row ia[i] (1-based) and column
+// ja[i] (compared as stored); a binary search over the row's stored columns
+// (assumed ascending, as the converters leave them) finds the slot and its
+// value becomes val[i].  Entries whose column is not stored, or whose row is
+// outside the matrix, change nothing.  ia, ja, val are device multivectors.
+template <class T>
+__global__ void k_ell_csput(int nnz, int rows, int pitch, const int *__restrict__ rS, const int *__restrict__ rP,
+                            T *__restrict__ cM, const int *__restrict__ aI, const int *__restrict__ aJ,
+                            const T *__restrict__ aVal) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+    const int row = aI[i] - 1;
+    if (row < 0 || row >= rows) continue;
+    const int col = aJ[i];
+    int lo = 0, hi = rS[row] - 1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const int c = rP[(size_t)mid * pitch + row];
+      if (c == col) {
+        cM[(size_t)mid * pitch + row] = aVal[i];
+        break;
+      }
+      if (c < col) lo = mid + 1;
+      else hi = mid - 1;
+    }
+  }
+}
+
+template <class T>
+static int ell_csput(void *deviceMat, int nnz, void *ia, void *ja, void *val, int type) {
+  EllDevice *m = (EllDevice *)deviceMat;
+  MultiVectDevice *I = (MultiVectDevice *)ia, *J = (MultiVectDevice *)ja, *V = (MultiVectDevice *)val;
+  if (nnz <= 0) return SPGPU_SUCCESS;
+  if (!m || !I || !J || !V || m->dataType != type || V->elemType != type || I->elemType != SPGPU_TYPE_INT ||
+      J->elemType != SPGPU_TYPE_INT || nnz > I->size_ || nnz > J->size_ || nnz > V->size_)
+    return SPGPU_UNSUPPORTED;
+  PsbxCtx &c = psbx_ctx();
+  k_ell_csput<T><<<psbx_grid_for(nnz, 256), 256, 0, c.stream>>>(nnz, m->rows, m->pitch, m->rS, m->rP, (T *)m->cM,
+                                                                 (const int *)I->v_, (const int *)J->v_,
+                                                                 (const T *)V->v_);
+  PSBX_LAUNCH_CK("k_ell_csput");
+  return SPGPU_SUCCESS;
+}
+
+extern "C" int dev_csputEllDeviceDouble(void *deviceMat, int nnz, void *ia, void *ja, void *val) {
+  return ell_csput<double>(deviceMat, nnz, ia, ja, val, SPGPU_TYPE_DOUBLE);
+}
+extern "C" int dev_csputEllDeviceFloat(void *deviceMat, int nnz, void *ia, void *ja, void *val) {
+  return ell_csput<float>(deviceMat, nnz, ia, ja, val, SPGPU_TYPE_FLOAT);
+}
+
 // ============================================================== CSR objects
 static CsrDevice *CM(psbx_d_Cmat *M) { return M ? (CsrDevice *)M->mat : nullptr; }
 
 static void csr_free_arrays(CsrDevice *m) {
+  if (m->svFlag) cudaFree(m->svFlag);
+  if (m->svCtl) cudaFree(m->svCtl);
+  m->svFlag = nullptr; m->svCtl = nullptr; m->svGen = 0;
   cudaFree(m->val);
   cudaFree(m->irp);
   cudaFree(m->ja);
@@ -828,9 +963,26 @@ int d_CSRGDeviceGetParms(psbx_d_Cmat *Mat, int *nr, int *nc, int *nz) {
 
 // Matrix type / fill mode / diag type only matter for the triangular solve
 // (spsv), which is outside this library; accepted and ignored.
-int d_CSRGDeviceSetMatType(psbx_d_Cmat *Mat, int type) { (void)type; return CM(Mat) ? 0 : SPGPU_UNSUPPORTED; }
-int d_CSRGDeviceSetMatFillMode(psbx_d_Cmat *Mat, int type) { (void)type; return CM(Mat) ? 0 : SPGPU_UNSUPPORTED; }
-int d_CSRGDeviceSetMatDiagType(psbx_d_Cmat *Mat, int type) { (void)type; return CM(Mat) ? 0 : SPGPU_UNSUPPORTED; }
+// The descriptor settings of cuda/fcusparse_fct.h (cusparseSetMat*); the
+// fill mode and diagonal type select the triangle d_spsvCSRGDevice solves.
+int d_CSRGDeviceSetMatType(psbx_d_Cmat *Mat, int type) {
+  CsrDevice *m = CM(Mat);
+  if (!m || type < 0 || type > 3) return SPGPU_UNSUPPORTED;
+  m->matType = type;
+  return SPGPU_SUCCESS;
+}
+int d_CSRGDeviceSetMatFillMode(psbx_d_Cmat *Mat, int type) {
+  CsrDevice *m = CM(Mat);
+  if (!m || (type != 0 && type != 1)) return SPGPU_UNSUPPORTED;
+  m->fillMode = type;
+  return SPGPU_SUCCESS;
+}
+int d_CSRGDeviceSetMatDiagType(psbx_d_Cmat *Mat, int type) {
+  CsrDevice *m = CM(Mat);
+  if (!m || (type != 0 && type != 1)) return SPGPU_UNSUPPORTED;
+  m->diagType = type;
+  return SPGPU_SUCCESS;
+}
 int d_CSRGDeviceSetMatIndexBase(psbx_d_Cmat *Mat, int type) {
   CsrDevice *m = CM(Mat);
   if (!m || (type != 0 && type != 1)) return SPGPU_UNSUPPORTED;

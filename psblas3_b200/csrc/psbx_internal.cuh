@@ -95,6 +95,15 @@ struct CsrDevice {
   double *chunkPart; // one partial sum per chunk
   unsigned *chunkTicket;  // one counter per long row (kept at zero between calls)
   int nLong;
+  // triangular solve (d_spsvCSRGDevice): cuSPARSE descriptor settings kept
+  // as the Fortran side sets them, and the solve's state, allocated by the
+  // first solve
+  int matType;       // 0 general, 3 triangular (cusparse_matrix_type_*)
+  int fillMode;      // 0 lower, 1 upper (cusparse_fill_mode_*)
+  int diagType;      // 0 non-unit, 1 unit (cusparse_diag_type_*)
+  unsigned *svFlag;  // per row: generation of the solve that finished it
+  unsigned *svCtl;   // [0] row ticket, [1] timeout flag
+  unsigned svGen;    // generation of the last solve
 };
 
 // ---------------------------------------------------------------------------
@@ -120,6 +129,7 @@ struct PsbxCtx {
 PsbxCtx &psbx_ctx();             // lazily initialises on the current device
 int psbx_ensure_init();          // 0 or error code
 int psbx_cuda_status(cudaError_t e, const char *where);
+void psbx_set_error(const char *msg);  // message for psbx_last_error, also printed
 void psbx_count_launch(int n = 1);
 
 #define PSBX_CK(call)                                                        \
@@ -152,6 +162,11 @@ __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float rmulf(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float raddf(float a, float b) { return __fadd_rn(a, b); }
+// The same, overloaded, for kernels written once for double and float (an
+// argument pair of mixed types does not resolve, which keeps mixed-precision
+// arithmetic explicit).
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
 
 // Streaming (read-once) loads: evict-first in L1/L2 so gathered vectors stay.
 template <class T>
@@ -387,6 +402,13 @@ struct EllView {
   int rows, pitch, base;
 };
 
+struct EllViewF {  // FP32 values, FP32 x
+  const float *val;
+  const int *ja;
+  const int *irn;
+  int rows, pitch, base;
+};
+
 struct CsrView {
   const double *val;
   const int *ja;
@@ -471,6 +493,10 @@ __device__ __forceinline__ double row_dot(const EllView &A, int r, const double 
   return row_acc<double, double, 8, 0>(A.val + r, A.ja + r, A.pitch, ld_ro(A.irn + r), x - A.base);
 }
 
+__device__ __forceinline__ double row_dot(const EllViewF &A, int r, const float *__restrict__ x) {
+  return row_acc<float, float, 8, 0>(A.val + r, A.ja + r, A.pitch, ld_ro(A.irn + r), x - A.base);
+}
+
 __device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *__restrict__ x) {
   const int b = ld_ro(A.irp + r) - A.base, e = ld_ro(A.irp + r + 1) - A.base;
   return row_acc<double, double, 4, 1>(A.val + b, A.ja + b, 1, e - b, x - A.base);
@@ -507,6 +533,7 @@ __device__ __forceinline__ int out_row(const Hll32View &A, int s) { return A.per
 __device__ __forceinline__ int out_row(const Hll32WView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const HllViewF &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const EllView &, int r) { return r; }
+__device__ __forceinline__ int out_row(const EllViewF &, int r) { return r; }
 __device__ __forceinline__ int out_row(const CsrView &, int r) { return r; }
 
 HllView hll_view(const HllDevice *m);
@@ -542,6 +569,8 @@ CsrView csr_view(const CsrDevice *m);
 int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, double beta, double *y,
                          cudaStream_t st);
 int psbx_launch_hll_spmv_f32(const HllDevice *m, float alpha, const float *x, float beta, float *y,
+                             cudaStream_t st);
+int psbx_launch_ell_spmv_f32(const EllDevice *m, float alpha, const float *x, float beta, float *y,
                              cudaStream_t st);
 int psbx_launch_ell_spmv(const EllDevice *m, double alpha, const double *x, double beta, double *y,
                          cudaStream_t st);

@@ -365,6 +365,45 @@ int psbx_launch_hll_spmv_f32(const HllDevice *m, float alpha, const float *x, fl
   return SPGPU_SUCCESS;
 }
 
+// FP32 ELL (spgpuSellspmv, ell_spmv_base_template.cuh with float values):
+// the row sum is formed like the FP32 HLL one -- every product of two floats
+// is exact in FP64, the products are added in FP64 in stored order and the
+// sum is rounded to FP32 once -- then y = alpha*sum + beta*y in FP32.
+template <int MODE>
+__global__ void __launch_bounds__(SPMV_T) k_ell_spmv_f32(EllViewF A, float alpha, const float *__restrict__ x,
+                                                         float beta, float *__restrict__ y) {
+  const int r = blockIdx.x * SPMV_T + threadIdx.x;
+  if (r >= A.rows) return;
+  const float acc = (float)row_dot(A, r, x);
+  const float t = rmulf(alpha, acc);
+  y[r] = MODE == 1 ? t : raddf(t, rmulf(beta, y[r]));
+}
+
+int psbx_launch_ell_spmv_f32(const EllDevice *m, float alpha, const float *x, float beta, float *y,
+                             cudaStream_t st) {
+  if (m->dataType != SPGPU_TYPE_FLOAT) return SPGPU_UNSUPPORTED;
+  EllViewF A;
+  A.val = (const float *)m->cM;
+  A.ja = m->rP;
+  A.irn = m->rS;
+  A.rows = m->rows;
+  A.pitch = m->pitch;
+  A.base = m->baseIndex;
+  if (A.rows <= 0) return SPGPU_SUCCESS;
+  if (alpha == 0.0f) {
+    k_f32_scale<<<psbx_grid_for(A.rows, SPMV_T), SPMV_T, 0, st>>>(A.rows, beta, y);
+    PSBX_LAUNCH_CK("k_f32_scale");
+    return SPGPU_SUCCESS;
+  }
+  const int g = (A.rows + SPMV_T - 1) / SPMV_T;
+  if (beta == 0.0f)
+    k_ell_spmv_f32<1><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  else
+    k_ell_spmv_f32<0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  PSBX_LAUNCH_CK("k_ell_spmv_f32");
+  return SPGPU_SUCCESS;
+}
+
 // --------------------------------------------------------------- CSR stream
 // Block b holds rows rowBlocks[2b] .. rowBlocks[2b+1]-1; their entries (at
 // most CSR_TILE) are contiguous in val/ja.

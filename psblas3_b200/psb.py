@@ -39,8 +39,13 @@ def init(dev: int = 0) -> None:
 
 
 # ------------------------------------------------------------------ vectors
+_VT = {np.dtype(np.float64): ("Double", L.SPGPU_TYPE_DOUBLE), np.dtype(np.float32): ("Float", L.SPGPU_TYPE_FLOAT),
+       np.dtype(np.int32): ("Int", L.SPGPU_TYPE_INT)}
+
+
 class DVect:
-    """One (count=1) or several (count>1) FP64 device vectors."""
+    """One (count=1) or several (count>1) device vectors of FP64 (the d
+    type), FP32 (the s type) or int32 (the i type) entries."""
 
     def __init__(self, n: int, count: int = 1, dtype=np.float64, zero: bool = True):
         """zero: start from zeros (psb_geall + psb_geasb); the C entry point
@@ -49,7 +54,7 @@ class DVect:
         self.n = int(n)
         self.count = int(count)
         self.dtype = np.dtype(dtype)
-        et = L.SPGPU_TYPE_DOUBLE if self.dtype == np.float64 else L.SPGPU_TYPE_FLOAT
+        self.tname, et = _VT[self.dtype]
         h = C.c_void_p()
         check(lib.FallocMultiVecDevice(C.byref(h), self.count, self.n, et), "FallocMultiVecDevice")
         self.h = h
@@ -61,8 +66,8 @@ class DVect:
     def bld(cls, x):
         """psb_d_vect_cuda%bld(x): allocate and copy host data to the device."""
         x = np.asarray(x)
-        v = cls(x.shape[0], 1 if x.ndim == 1 else x.shape[1], np.float32 if x.dtype == np.float32 else np.float64,
-                zero=False)
+        dt = x.dtype if x.dtype in (np.float32, np.int32) else np.float64
+        v = cls(x.shape[0], 1 if x.ndim == 1 else x.shape[1], dt, zero=False)
         v.set_vect(x)
         return v
 
@@ -76,13 +81,11 @@ class DVect:
 
     def set_vect(self, x):
         buf = self._host(x)
-        f = lib.writeMultiVecDeviceDouble if self.dtype == np.float64 else lib.writeMultiVecDeviceFloat
-        check(f(self.h, _ptr(buf)), "writeMultiVecDevice")
+        check(getattr(lib, "writeMultiVecDevice" + self.tname)(self.h, _ptr(buf)), "writeMultiVecDevice")
 
     def get_vect(self):
         buf = np.zeros((self.count, self.pitch), self.dtype)
-        f = lib.readMultiVecDeviceDouble if self.dtype == np.float64 else lib.readMultiVecDeviceFloat
-        check(f(self.h, _ptr(buf)), "readMultiVecDevice")
+        check(getattr(lib, "readMultiVecDevice" + self.tname)(self.h, _ptr(buf)), "readMultiVecDevice")
         out = buf[:, : self.n]
         return out[0].copy() if self.count == 1 else out.T.copy()
 
@@ -93,17 +96,15 @@ class DVect:
 
     def set_scal(self, val, first=1, last=None):
         last = self.n if last is None else last
-        check(lib.setscalMultiVecDeviceDouble(float(val), int(first), int(last), 1, self.h), "setscal")
+        v = int(val) if self.dtype == np.int32 else float(val)
+        check(getattr(lib, "setscalMultiVecDevice" + self.tname)(v, int(first), int(last), 1, self.h), "setscal")
 
     def zero(self):
         """Every element of every vector (padding included) to 0."""
-        if self.dtype == np.float64:
-            self.set_scal(0.0, 1, self.pitch * self.count)
-        else:
-            self.set_vect(np.zeros((self.n, self.count) if self.count > 1 else self.n, self.dtype))
+        self.set_scal(0, 1, self.pitch * self.count)
 
     def scal(self, alpha):
-        check(lib.scalMultiVecDeviceDouble(float(alpha), self.h), "scal")
+        check(getattr(lib, "scalMultiVecDevice" + self.tname)(float(alpha), self.h), "scal")
 
     def free(self):
         if self.h:
