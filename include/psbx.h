@@ -448,6 +448,22 @@ int psbx_DefaultSolverOptions(psbx_SolverOptions *opt);
 int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv,
                  void *b, void *x, psbx_SolverOptions *opt);
 
+/* Mixed-precision psb_krylov('CG') for one system (krylov/psb_dcg.F90:218-295
+ * with the DIAG preconditioner; no single reference entry): the iterations
+ * run in FP32 -- the matrix's FP32 value copy (made here if absent), FP32
+ * vectors, dot products accumulated in FP64 -- and the residual
+ * r = b - A x, the solution x and the stop test ||r|| <= eps ||b|| (istop 2
+ * only) in FP64.  The FP32 recursive residual is replaced by the FP64 true
+ * residual whenever it has fallen by the factor delta (0 < delta < 1, e.g.
+ * 0.1) since the last replacement, keeping the search direction.
+ *   mat   FP64 HLL handle, hack size 32;  dinv  FP64 inverse diagonal or NULL
+ *   b, x  FP64 MultiVectDevice (x = x0 on entry, the solution on exit)
+ * opt->iter = inner iterations, opt->err = ||b - A x|| / ||b|| (FP64, true
+ * residual); *refreshes (nullable) = residual replacements.  Returns 0
+ * (converged or itmax) or an error code. */
+int psbx_dmixed_cg(void *mat, void *dinv, void *b, void *x,
+                   psbx_SolverOptions *opt, double delta, int *refreshes);
+
 /* psb_d_diag_precbld (prec/impl/psb_d_diagprec_impl.f90:229-292) on the
  * device: dinv(i) = 1/a_ii, 1 where a_ii == 0 (HLL uses idiag). */
 int psbx_diag_prec_build(void *mat, int fmt, void *dinv);

@@ -138,6 +138,7 @@ _SIGS = {
     "psbx_DefaultSolverOptions": (I, [C.POINTER(SolverOptions)]),
     "psbx_dkrylov": (I, [CH, P, I, P, P, P, C.POINTER(SolverOptions)]),
     "psbx_diag_prec_build": (I, [P, I, P]),
+    "psbx_dmixed_cg": (I, [P, P, P, P, C.POINTER(SolverOptions), D, PI]),
     "psbx_hll_from_csr_device": (I, [PP, I, I, I, P, P, P, I, P]),
     "psbx_hll_autotune_from_csr_device": (I, [PP, I, I, I, P, P, P, P, PI, PI, PD]),
     "psbx_hll_make_single": (I, [P]), "psbx_hll_set_wide": (I, [P, I]),

@@ -424,6 +424,11 @@ struct Hll32View : HllView {};
 // from lres (a separate type, so the kernels of matrices without wide hacks
 // carry no test for them).
 struct Hll32WView : HllView {};
+// Hack size 32, every row at most PSBX_SHORT_ROW entries (the 7-point
+// operators): a row's entries are read as one predicated group, so all of its
+// index and value loads are in flight at once instead of one after another.
+struct Hll32SView : HllView {};
+#define PSBX_SHORT_ROW 16
 
 // Unrolled in-order accumulation over one row whose j-th entry sits at
 // vp[j*stride] / jp[j*stride] (32-bit offsets: every format keeps its
@@ -459,6 +464,53 @@ __device__ __forceinline__ double row_acc(const VT *__restrict__ vp, const int *
     acc = radd(acc, rmul((double)v, (double)ld_ro(xb + c)));
   }
   return acc;
+}
+
+// row_acc with the tail as one predicated group of U: the loads of entries
+// past the row's end are not issued and their terms are not added, so the
+// sum (and its rounding) is the same as row_acc's.
+template <class VT, class XT, int U, int STRIDE>
+__device__ __forceinline__ double row_acc_p(const VT *__restrict__ vp, const int *__restrict__ jp, int stride, int n,
+                                            const XT *__restrict__ xb, int base) {
+  const int st = STRIDE > 0 ? STRIDE : stride;
+  double acc = 0.0;
+  int j = 0;
+  for (; j + U <= n; j += U) {
+    int c[U];
+    VT v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      c[u] = ld_stream(jp + (j + u) * st);
+      v[u] = ld_stream(vp + (j + u) * st);
+    }
+    XT xv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) xv[u] = ld_ro(xb + c[u]);
+#pragma unroll
+    for (int u = 0; u < U; u++) acc = radd(acc, rmul((double)v[u], (double)xv[u]));
+  }
+  if (j < n) {
+    int c[U];
+    VT v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool ok = j + u < n;
+      c[u] = ok ? ld_stream(jp + (j + u) * st) : base;
+      v[u] = ok ? ld_stream(vp + (j + u) * st) : VT(0);
+    }
+    XT xv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) xv[u] = j + u < n ? ld_ro(xb + c[u]) : XT(0);
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (j + u < n) acc = radd(acc, rmul((double)v[u], (double)xv[u]));
+  }
+  return acc;
+}
+
+__device__ __forceinline__ double row_dot(const Hll32SView &A, int s, const double *__restrict__ x) {
+  const int off = ld_ro(A.hkoffs + (s >> 5)) + (s & 31);
+  return row_acc_p<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base, A.base);
 }
 
 __device__ __forceinline__ double row_dot(const Hll32View &A, int s, const double *__restrict__ x) {
@@ -507,6 +559,9 @@ __device__ __forceinline__ double row_abs_sum(const HllView &A, int s);
 __device__ __forceinline__ double row_abs_sum(const Hll32View &A, int s) {
   return row_abs_sum(static_cast<const HllView &>(A), s);
 }
+__device__ __forceinline__ double row_abs_sum(const Hll32SView &A, int s) {
+  return row_abs_sum(static_cast<const HllView &>(A), s);
+}
 __device__ __forceinline__ double row_abs_sum(const Hll32WView &A, int s) {
   return row_abs_sum(static_cast<const HllView &>(A), s);
 }
@@ -531,6 +586,7 @@ __device__ __forceinline__ double row_abs_sum(const CsrView &A, int r) {
 __device__ __forceinline__ int out_row(const HllView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const Hll32View &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const Hll32WView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
+__device__ __forceinline__ int out_row(const Hll32SView &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const HllViewF &A, int s) { return A.perm ? ld_ro(A.perm + s) : s; }
 __device__ __forceinline__ int out_row(const EllView &, int r) { return r; }
 __device__ __forceinline__ int out_row(const EllViewF &, int r) { return r; }
@@ -555,6 +611,16 @@ static inline Hll32WView hll32w_view(const HllView &v) {
   Hll32WView w;
   static_cast<HllView &>(w) = v;
   return w;
+}
+static inline Hll32SView hll32s_view(const HllView &v) {
+  Hll32SView w;
+  static_cast<HllView &>(w) = v;
+  return w;
+}
+// A hack-32 matrix with no wide hacks whose rows all hold at most
+// PSBX_SHORT_ROW entries runs the short-row kernels (Hll32SView).
+static inline bool hll_short_rows(const HllDevice *m) {
+  return m->hackSize == 32 && m->nLong == 0 && m->maxRowLen >= 0 && m->maxRowLen <= PSBX_SHORT_ROW;
 }
 
 template <class View>

@@ -1537,6 +1537,7 @@ static void key_hll(std::vector<uint64_t> &k, const HllView &v, uint64_t tag) {
 static void key_view(std::vector<uint64_t> &k, const HllView &v) { key_hll(k, v, 0); }
 static void key_view(std::vector<uint64_t> &k, const Hll32View &v) { key_hll(k, v, 1); }
 static void key_view(std::vector<uint64_t> &k, const Hll32WView &v) { key_hll(k, v, 2); }
+static void key_view(std::vector<uint64_t> &k, const Hll32SView &v) { key_hll(k, v, 5); }
 static void key_view(std::vector<uint64_t> &k, const EllView &v) {
   k.insert(k.end(), {3, (uint64_t)v.val, (uint64_t)v.ja, (uint64_t)v.irn, (uint64_t)(uint32_t)v.rows,
                      (uint64_t)(uint32_t)v.pitch, (uint64_t)(uint32_t)v.base});
@@ -2387,6 +2388,7 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
       if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
       const HllView v = hll_view(m);
       if (m->hackSize == 32 && v.nLong > 0) return solve_bicg(hll32w_view(v), mat, fmt, dv, bp, xp, n, opt);
+      if (hll_short_rows(m)) return solve_bicg(hll32s_view(v), mat, fmt, dv, bp, xp, n, opt);
       if (m->hackSize == 32) return solve_bicg(hll32_view(v), mat, fmt, dv, bp, xp, n, opt);
       return solve_bicg(v, mat, fmt, dv, bp, xp, n, opt);
     }
@@ -2401,6 +2403,8 @@ extern "C" int psbx_dkrylov(const char *method, void *mat, int fmt, void *dinv, 
     if (m->hackSize == 32) {
       const HllView v = hll_view(m);
       if (v.nLong > 0) return run_method(meth, hll32w_view(v), dv, (const double *)B->v_, (double *)X->v_, n, opt);
+      if (hll_short_rows(m))
+        return run_method(meth, hll32s_view(v), dv, (const double *)B->v_, (double *)X->v_, n, opt);
       return run_method(meth, hll32_view(v), dv, (const double *)B->v_, (double *)X->v_, n, opt);
     }
     return run_method(meth, hll_view(m), dv, (const double *)B->v_, (double *)X->v_, n, opt);

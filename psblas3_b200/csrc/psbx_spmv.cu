@@ -322,6 +322,7 @@ int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, doub
   if (m->hackSize == 32) {
     const HllView v = hll_view(m);
     if (v.nLong > 0) return launch_rows(hll32w_view(v), alpha, x, beta, y, st);
+    if (hll_short_rows(m)) return launch_rows(hll32s_view(v), alpha, x, beta, y, st);
     return launch_rows(hll32_view(v), alpha, x, beta, y, st);
   }
   return launch_rows(hll_view(m), alpha, x, beta, y, st);

@@ -421,6 +421,20 @@ def psb_krylov(method, a, prec, b, x, eps=1e-6, itmax=1000, istop=2, itrace=0, i
     return opt.iter, opt.err
 
 
+def psb_mixed_cg(a, prec, b, x, eps=1e-10, itmax=100000, delta=0.1):
+    """Mixed-precision CG for one system (psbx_dmixed_cg): FP32 iterations
+    with FP64-accumulated dots, FP64 residual replacement, FP64 stop test
+    ||b - A x|| <= eps ||b||.  a: HllMat (hack size 32).  Returns
+    (inner iterations, relative true residual, residual replacements)."""
+    opt = L.SolverOptions()
+    lib.psbx_DefaultSolverOptions(C.byref(opt))
+    opt.eps, opt.itmax, opt.istop = float(eps), int(itmax), 2
+    dinv = None if (prec is None or prec.dv is None) else prec.dv.h
+    nref = C.c_int(0)
+    check(lib.psbx_dmixed_cg(a.h, dinv, b.h, x.h, C.byref(opt), float(delta), C.byref(nref)), "psbx_dmixed_cg")
+    return opt.iter, opt.err, nref.value
+
+
 class BatchSolver:
     """Batched mixed-precision CG engine (psbx_batch_*): FP32 inner Jacobi-CG
     with FP64-accumulated dots inside FP64 iterative refinement, many
