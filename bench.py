@@ -424,8 +424,9 @@ def secondary(args, psb, gen, irp, ja, va, x_host, y_ref, stream):
 
 def c3_cg(psb, gen):
     """C3: SPD 7-point Poisson 256^3, b = A u* (u* uniform [0, 1]); plain FP64
-    device CG to 1e-10 beside the mixed-precision engine (FP32 inner CG,
-    FP64-accumulated dots, FP64 refinement) to the same FP64 tolerance."""
+    device CG to 1e-10 beside the mixed-precision CG (FP32 iterations,
+    FP64-accumulated dots, FP64 residual replacement) to the same FP64
+    tolerance, and the same system through the batched engine."""
     import torch
     qi, qj, qv = gen.poisson7(256)
     n3 = len(qi) - 1
@@ -447,8 +448,24 @@ def c3_cg(psb, gen):
     res = {"rows": n3, "nnz": len(qj),
            "fp64": {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "iters": it3, "err": err3,
                     "max_abs_err_vs_ustar": float(np.max(np.abs(x64 - ustar)))}}
-    # mixed precision: FP32 inner CG, FP64-accumulated dots, FP64 refinement
+    # mixed precision, single-system solver: FP32 iterations (values, vectors),
+    # FP64-accumulated dots, FP64 residual replacement and stop test
     A3.make_single()
+    times = []
+    for _ in range(2):
+        X3.zero()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        itm, errm, nref = psb.psb_mixed_cg(A3, P3, B3, X3, eps=1e-10, itmax=20000, delta=0.1)
+        times.append(time.perf_counter() - t0)
+    xm = X3.get_vect()
+    res["mixed"] = {"solver": "psbx_dmixed_cg", "solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times),
+                    "inner_iters": itm, "residual_replacements": nref, "delta": 0.1, "err": errm,
+                    "converged": errm <= 1e-10,
+                    "max_abs_err_vs_ustar": float(np.max(np.abs(xm - ustar))),
+                    "max_abs_diff_vs_fp64_solve": float(np.max(np.abs(xm - x64)))}
+    res["mixed_speedup_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+    # the same system through the batched engine (restarted inner CG per refinement)
     eng = psb.BatchSolver(1, n3, 1)
     dx = torch.zeros(n3, dtype=torch.float64, device="cuda")
     db = torch.from_numpy(B3.get_vect()).cuda()
@@ -462,12 +479,10 @@ def c3_cg(psb, gen):
         times.append(time.perf_counter() - t0)
         st, outer, its, err = eng.poll(s)
         eng.remove(s)
-    xm = dx.cpu().numpy()
-    res["mixed"] = {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times), "inner_iters": its[0],
-                    "outer": outer, "converged": st == 1, "err": err[0],
-                    "max_abs_err_vs_ustar": float(np.max(np.abs(xm - ustar))),
-                    "max_abs_diff_vs_fp64_solve": float(np.max(np.abs(xm - x64)))}
-    res["mixed_speedup_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+    xe = dx.cpu().numpy()
+    res["mixed_batch_engine"] = {"solve_ms": 1e3 * min(times), "solves_per_s": 1.0 / min(times),
+                                 "inner_iters": its[0], "outer": outer, "converged": st == 1, "err": err[0],
+                                 "max_abs_err_vs_ustar": float(np.max(np.abs(xe - ustar)))}
     eng.free()
     A3.free()
     return res

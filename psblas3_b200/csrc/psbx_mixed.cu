@@ -24,8 +24,8 @@
 //
 // Per inner iteration, three kernels (as the FP64 CG of psbx_krylov.cu):
 //   p = z + beta p (z = d .* rh formed on the fly)
-//   q = A p (FP32 product: exact FP64 products added in FP64, rounded once)
-//     and sigma = (p, q), alpha = rho / sigma
+//   q = A p (FP32 product, two rows per thread: exact FP64 products added
+//     in FP64, rounded once) and sigma = (p, q), alpha = rho / sigma
 //   xh = alpha p + xh, rh = -alpha q + rh, z = d .* rh, rho' = (rh, z),
 //     ||rh||^2, and the replacement test
 // Every kernel returns at once when the status word is not RUN, so eight
@@ -54,14 +54,46 @@ __device__ __forceinline__ bool mx_stopped(const MState *S) {
   return *((volatile const int *)&S->status) != MX_RUN;
 }
 
-// FP32 product of row s (hack size 32)
-template <bool SHORT>
-__device__ __forceinline__ float row32(const HllViewF &A, int s, const float *__restrict__ x) {
-  const int off = ld_ro(A.hkoffs + (s >> 5)) + (s & 31);
-  const int n = ld_ro(A.irn + s);
-  const double a = SHORT ? row_acc_p<float, float, 8, 32>(A.val + off, A.ja + off, 32, n, x - A.base, A.base)
-                         : row_acc<float, float, 8, 32>(A.val + off, A.ja + off, 32, n, x - A.base);
-  return (float)a;
+// FP32 products of the row pair (s0, s0 + 1), s0 even, of a hack-32 matrix,
+// both in one thread.  The two rows are adjacent in every column of their
+// hack, so entry j of both is one float2 (values) and one int2 (indices):
+// each load instruction of a warp moves 256 bytes, as the FP64 kernels' do,
+// where one row per thread would move 128 (measured: 3.6 TB/s for one row
+// per thread on the 7-point operator, against 6.25 TB/s for FP64).  Each
+// row still adds its own entries in stored order, in FP64, from exact
+// products, and rounds once.  Slots past a row's length (padding of the
+// hack) may be loaded but are never added.
+template <int U>
+__device__ __forceinline__ void pair32(const HllViewF &A, int off, int n0, int n1, const float *__restrict__ x,
+                                       float &y0, float &y1) {
+  const float *vp = A.val + off;
+  const int *jp = A.ja + off;
+  const float *xb = x - A.base;
+  const int n = max(n0, n1);
+  double a0 = 0.0, a1 = 0.0;
+  for (int j = 0; j < n; j += U) {
+    int2 c[U];
+    float2 v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool ok = j + u < n;
+      c[u] = ok ? ld_stream((const int2 *)(jp + (j + u) * 32)) : make_int2(A.base, A.base);
+      v[u] = ok ? ld_stream((const float2 *)(vp + (j + u) * 32)) : make_float2(0.0f, 0.0f);
+    }
+    float x0[U], x1[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      x0[u] = j + u < n0 ? ld_ro(xb + c[u].x) : 0.0f;
+      x1[u] = j + u < n1 ? ld_ro(xb + c[u].y) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (j + u < n0) a0 = radd(a0, rmul((double)v[u].x, (double)x0[u]));
+      if (j + u < n1) a1 = radd(a1, rmul((double)v[u].y, (double)x1[u]));
+    }
+  }
+  y0 = (float)a0;
+  y1 = (float)a1;
 }
 
 __device__ __forceinline__ void exact_add(dd_t &acc, float a, float b) {
@@ -162,31 +194,87 @@ __global__ void __launch_bounds__(MT) k_mx_resid(View A, MState *S, const double
   }
 }
 
+// The element-wise kernels take four entries per thread as one float4 per
+// vector (256-byte-aligned workspace; the last n % 4 entries by the block's
+// first threads one at a time).
+__device__ __forceinline__ float4 ld4(const float *p, int k) { return ld_stream((const float4 *)p + k); }
+
 // p = z (after a restart) or p = z + beta p, z = d .* rh
+__device__ __forceinline__ float p_el(bool first, float beta, float d, float r, float p) {
+  const float z = rmulf(d, r);
+  return first ? z : raddf(z, rmulf(beta, p));
+}
 __global__ void __launch_bounds__(MT) k_mx_p(MState *S, int n, const float *__restrict__ d32,
                                              const float *__restrict__ rh, float *__restrict__ p) {
   if (mx_stopped(S)) return;
   const bool first = S->first != 0;
   const float beta = (float)S->beta;
-  for (int i = blockIdx.x * MT + threadIdx.x; i < n; i += gridDim.x * MT) {
-    const float z = rmulf(ld_stream(d32 + i), ld_stream(rh + i));
-    p[i] = first ? z : raddf(z, rmulf(beta, p[i]));
+  const int n4 = n >> 2;
+  for (int k = blockIdx.x * MT + threadIdx.x; k < n4; k += gridDim.x * MT) {
+    const float4 d = ld4(d32, k), r = ld4(rh, k), q = ((const float4 *)p)[k];
+    ((float4 *)p)[k] = make_float4(p_el(first, beta, d.x, r.x, q.x), p_el(first, beta, d.y, r.y, q.y),
+                                   p_el(first, beta, d.z, r.z, q.z), p_el(first, beta, d.w, r.w, q.w));
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+    const int i = 4 * n4 + threadIdx.x;
+    p[i] = p_el(first, beta, d32[i], rh[i], p[i]);
   }
 }
 
-// q = A p ; sigma = (p, q) ; alpha = rho / sigma
-template <bool SHORT>
-__global__ void __launch_bounds__(MT) k_mx_spmv(HllViewF A, MState *S, const float *__restrict__ p,
+// q = A p ; sigma = (p, q) ; alpha = rho / sigma   (hack size 32, row pairs)
+// Capped at 64 registers (4 blocks of 256 per SM, no spills): uncapped, the
+// prefetch of the next pair's header takes it to 80 (3 blocks per SM), and
+// the 7-point 256^3 solve measured 323-331 ms that way against 289 ms capped.
+template <int U>
+__global__ void __launch_bounds__(MT, 4) k_mx_spmv(HllViewF A, MState *S, const float *__restrict__ p,
                                                 float *__restrict__ q, double *__restrict__ part,
                                                 unsigned *__restrict__ ticket, int grid) {
   __shared__ double sm[64];
   if (mx_stopped(S)) return;
   dd_t acc[1] = {{0.0, 0.0}};
-  for (int s = blockIdx.x * MT + threadIdx.x; s < A.rows; s += gridDim.x * MT) {
-    const float t = row32<SHORT>(A, s, p);
-    const int i = A.perm ? ld_ro(A.perm + s) : s;
-    q[i] = t;
-    exact_add(acc[0], ld_ro(p + i), t);
+  const int npair = (A.rows + 1) >> 1;
+  const int step = gridDim.x * MT;
+  // the next pair's row lengths and hack offset are loaded while the
+  // current pair is summed (one dependent round trip less per pair)
+  auto head = [&](int k, int &n0, int &n1, int &off) {
+    if (k < npair) {
+      const int s0 = 2 * k;
+      n0 = ld_ro(A.irn + s0);
+      n1 = s0 + 1 < A.rows ? ld_ro(A.irn + s0 + 1) : 0;
+      off = ld_ro(A.hkoffs + (s0 >> 5)) + (s0 & 31);
+    }
+  };
+  int k = blockIdx.x * MT + threadIdx.x;
+  int n0 = 0, n1 = 0, off = 0;
+  head(k, n0, n1, off);
+  for (; k < npair; k += step) {
+    const int s0 = 2 * k, s1 = s0 + 1;
+    const bool has1 = s1 < A.rows;
+    int m0 = 0, m1 = 0, moff = 0;
+    head(k + step, m0, m1, moff);
+    float t0, t1;
+    pair32<U>(A, off, n0, n1, p, t0, t1);
+    n0 = m0;
+    n1 = m1;
+    off = moff;
+    if (A.perm) {
+      const int i0 = ld_ro(A.perm + s0);
+      q[i0] = t0;
+      exact_add(acc[0], ld_ro(p + i0), t0);
+      if (has1) {
+        const int i1 = ld_ro(A.perm + s1);
+        q[i1] = t1;
+        exact_add(acc[0], ld_ro(p + i1), t1);
+      }
+    } else if (has1) {
+      ((float2 *)q)[k] = make_float2(t0, t1);
+      const float2 pp = ld_ro((const float2 *)p + k);
+      exact_add(acc[0], pp.x, t0);
+      exact_add(acc[0], pp.y, t1);
+    } else {
+      q[s0] = t0;
+      exact_add(acc[0], ld_ro(p + s0), t0);
+    }
   }
   block_sum_dd<1>(acc, sm);
   mx_publish<1>(part, grid, acc);
@@ -205,6 +293,14 @@ __global__ void __launch_bounds__(MT) k_mx_spmv(HllViewF A, MState *S, const flo
 
 // xh = alpha p + xh ; rh = -alpha q + rh ; rho' = (rh, d.*rh) ; ||rh||^2 ;
 // replacement test
+__device__ __forceinline__ void upd_el(float af, float maf, float p, float q, float d, float &xh, float &r,
+                                       dd_t (&acc)[2]) {
+  xh = raddf(rmulf(af, p), xh);
+  r = raddf(rmulf(maf, q), r);
+  const float z = rmulf(d, r);
+  exact_add(acc[0], r, z);
+  exact_add(acc[1], r, r);
+}
 __global__ void __launch_bounds__(MT) k_mx_update(MState *S, int n, const float *__restrict__ p,
                                                   const float *__restrict__ q, const float *__restrict__ d32,
                                                   float *__restrict__ xh, float *__restrict__ rh,
@@ -214,13 +310,23 @@ __global__ void __launch_bounds__(MT) k_mx_update(MState *S, int n, const float 
   if (mx_stopped(S)) return;
   const float af = (float)S->alpha, maf = -af;
   dd_t acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
-  for (int i = blockIdx.x * MT + threadIdx.x; i < n; i += gridDim.x * MT) {
-    xh[i] = raddf(rmulf(af, ld_stream(p + i)), xh[i]);
-    const float r = raddf(rmulf(maf, ld_stream(q + i)), rh[i]);
+  const int n4 = n >> 2;
+  for (int k = blockIdx.x * MT + threadIdx.x; k < n4; k += gridDim.x * MT) {
+    const float4 pp = ld4(p, k), qq = ld4(q, k), d = ld4(d32, k);
+    float4 x = ((const float4 *)xh)[k], r = ((const float4 *)rh)[k];
+    upd_el(af, maf, pp.x, qq.x, d.x, x.x, r.x, acc);
+    upd_el(af, maf, pp.y, qq.y, d.y, x.y, r.y, acc);
+    upd_el(af, maf, pp.z, qq.z, d.z, x.z, r.z, acc);
+    upd_el(af, maf, pp.w, qq.w, d.w, x.w, r.w, acc);
+    ((float4 *)xh)[k] = x;
+    ((float4 *)rh)[k] = r;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+    const int i = 4 * n4 + threadIdx.x;
+    float x = xh[i], r = rh[i];
+    upd_el(af, maf, p[i], q[i], d32[i], x, r, acc);
+    xh[i] = x;
     rh[i] = r;
-    const float z = rmulf(ld_stream(d32 + i), r);
-    exact_add(acc[0], r, z);
-    exact_add(acc[1], r, r);
   }
   block_sum_dd<2>(acc, sm);
   mx_publish<2>(part, grid, acc);
@@ -252,7 +358,7 @@ static int mx_solve(const View &A64, const HllViewF &A32, bool shortRows, const 
   int grid = (n + MT - 1) / MT;
   if (grid > c.sms * 8) grid = c.sms * 8;
   if (grid < 1) grid = 1;
-  const size_t nn = (size_t)(n > 0 ? n : 1);
+  const size_t nn = ((size_t)(n > 0 ? n : 1) + 63) / 64 * 64;  // 256-byte aligned vectors
   float *vec = nullptr;
   double *part = nullptr;
   MState *S = nullptr;
@@ -290,12 +396,17 @@ static int mx_solve(const View &A64, const HllViewF &A32, bool shortRows, const 
     if (ce != cudaSuccess) return psbx_cuda_status(ce, "GraphInstantiate");
     return SPGPU_SUCCESS;
   };
+  // grids: the element-wise kernels take 4 entries per thread, the product
+  // 2 rows per thread
+  int gq = (n / 4 + MT - 1) / MT, gs = ((n + 1) / 2 + MT - 1) / MT;
+  gq = gq < 1 ? 1 : (gq > grid ? grid : gq);
+  gs = gs < 1 ? 1 : (gs > grid ? grid : gs);
   rc = capture(&gi, &ei, [&]() {
     for (int k = 0; k < MX_ITERS; k++) {
-      k_mx_p<<<grid, MT, 0, st>>>(S, n, d32, rh, p);
-      if (shortRows) k_mx_spmv<true><<<grid, MT, 0, st>>>(A32, S, p, q, part, ticket, grid);
-      else k_mx_spmv<false><<<grid, MT, 0, st>>>(A32, S, p, q, part, ticket, grid);
-      k_mx_update<<<grid, MT, 0, st>>>(S, n, p, q, d32, xh, rh, part, ticket, grid);
+      k_mx_p<<<gq, MT, 0, st>>>(S, n, d32, rh, p);
+      if (shortRows) k_mx_spmv<8><<<gs, MT, 0, st>>>(A32, S, p, q, part, ticket, gs);
+      else k_mx_spmv<4><<<gs, MT, 0, st>>>(A32, S, p, q, part, ticket, gs);
+      k_mx_update<<<gq, MT, 0, st>>>(S, n, p, q, d32, xh, rh, part, ticket, gq);
     }
   });
   if (!rc) rc = capture(&gr, &er, [&]() {
@@ -381,8 +492,8 @@ extern "C" int psbx_dmixed_cg(void *mat, void *dinv, void *b, void *x, psbx_Solv
   const double *dv = D ? (const double *)D->v_ : nullptr;
   const double *bp = (const double *)B->v_;
   double *xp = (double *)X->v_;
-  // the FP32 product takes the short-row kernel whenever no row is longer
-  // than PSBX_SHORT_ROW (its wide hacks, if any, are summed thread per row)
+  // the FP32 product reads a row pair's entries in groups of 8 when no row
+  // is longer than PSBX_SHORT_ROW (one group for the 7-point rows), else 4
   const bool shortRows = m->maxRowLen >= 0 && m->maxRowLen <= PSBX_SHORT_ROW;
   if (v.nLong > 0) return mx_solve(hll32w_view(v), A32, shortRows, dv, bp, xp, n, opt, delta, refreshes);
   if (hll_short_rows(m)) return mx_solve(hll32s_view(v), A32, true, dv, bp, xp, n, opt, delta, refreshes);
