@@ -1142,7 +1142,7 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   // one allocation per slot: r64 (K n doubles), r32 z p q d (5 K n floats), dinv (n floats)
   const size_t bytes = sizeof(double) * K * n + sizeof(float) * (5 * K + 1) * n + 256;
   char *buf = nullptr;
-  cudaError_t err = cudaMallocAsync((void **)&buf, bytes, c.stream);
+  cudaError_t err = psbx_malloc_async((void **)&buf, bytes, c.stream);
   if (err != cudaSuccess) return psbx_cuda_status(err, "psbx_batch_add");
   BSys S;
   memset(&S, 0, sizeof(S));

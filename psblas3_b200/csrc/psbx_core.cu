@@ -42,6 +42,14 @@ static int ctx_create(int dev) {
   PSBX_CK(cudaMemset(c.d_ticket, 0, sizeof(unsigned) * 64));
   PSBX_CK(cudaMalloc(&c.d_res, sizeof(double) * 64));
   PSBX_CK(cudaHostAlloc(&c.h_res, sizeof(double) * 64, cudaHostAllocDefault));
+  cudaMemPoolProps pp;
+  memset(&pp, 0, sizeof(pp));
+  pp.allocType = cudaMemAllocationTypePinned;
+  pp.location.type = cudaMemLocationTypeDevice;
+  pp.location.id = dev;
+  PSBX_CK(cudaMemPoolCreate(&c.pool, &pp));
+  uint64_t keep = PSBX_POOL_KEEP;
+  PSBX_CK(cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &keep));
   c.init = true;
   return SPGPU_SUCCESS;
 }
@@ -75,6 +83,8 @@ static void ctx_destroy() {
   cudaFree(c.d_ticket);
   cudaFree(c.d_res);
   cudaFreeHost(c.h_res);
+  cudaStreamSynchronize(c.defaultStream);
+  if (c.pool) cudaMemPoolDestroy(c.pool);
   cudaStreamDestroy(c.defaultStream);
   c = PsbxCtx();
 }

@@ -124,9 +124,20 @@ struct PsbxCtx {
   unsigned *d_ticket = nullptr;   // [64] zero-initialised, reset by users
   double *d_res = nullptr;        // [64] reduction results
   double *h_res = nullptr;        // pinned [64]
+  // Stream-ordered workspace of the solvers comes from this pool, which
+  // keeps up to PSBX_POOL_KEEP bytes of freed memory mapped between calls:
+  // with nothing kept, every solve remapped its workspace (1 GB for CG on
+  // 16.8M rows), and calls of the same solve varied from 0.49 to 1.1 s.
+  cudaMemPool_t pool = nullptr;
 };
+#define PSBX_POOL_KEEP ((uint64_t)4 << 30)
 
 PsbxCtx &psbx_ctx();             // lazily initialises on the current device
+// cudaMallocAsync from the library's pool (freed with cudaFreeAsync)
+template <class T>
+static inline cudaError_t psbx_malloc_async(T **p, size_t bytes, cudaStream_t st) {
+  return cudaMallocFromPoolAsync((void **)p, bytes, psbx_ctx().pool, st);
+}
 int psbx_ensure_init();          // 0 or error code
 int psbx_cuda_status(cudaError_t e, const char *where);
 void psbx_set_error(const char *msg);  // message for psbx_last_error, also printed

@@ -1615,10 +1615,10 @@ static int solve(const View &A, bool bicg, const double *dinv, const double *b, 
     ticket = ce->ticket;
     gexec = ce->gexec;
   } else {
-    PSBX_CK(cudaMallocAsync(&vec, vbytes, st));
-    PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-    PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-    PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+    PSBX_CK(psbx_malloc_async(&vec, vbytes, st));
+    PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+    PSBX_CK(psbx_malloc_async(&S, sizeof(KState), st));
+    PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned) * 8, st));
   }
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(vec, 0, vbytes, st));
@@ -1743,10 +1743,10 @@ static int solve_fcg(const View &A, const double *dinv, const double *b, double 
   double *vec = nullptr, *part = nullptr;
   KState *S = nullptr;
   unsigned *ticket = nullptr;
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * 5 * nn, st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(psbx_malloc_async(&vec, sizeof(double) * 5 * nn, st));
+  PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(psbx_malloc_async(&S, sizeof(KState), st));
+  PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * 5 * nn, st));
   KState *hS = (KState *)c.h_res;
@@ -1831,11 +1831,11 @@ static int solve_gmres(const View &A, const double *dinv, const double *b, doubl
   KState *S = nullptr;
   unsigned *ticket = nullptr;
   // V (ld vectors), w, w1
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * (size_t)(ld + 2) * nn, st));
-  PSBX_CK(cudaMallocAsync(&small, sizeof(double) * ((size_t)ld * ld + 3 * (size_t)ld), st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(psbx_malloc_async(&vec, sizeof(double) * (size_t)(ld + 2) * nn, st));
+  PSBX_CK(psbx_malloc_async(&small, sizeof(double) * ((size_t)ld * ld + 3 * (size_t)ld), st));
+  PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(psbx_malloc_async(&S, sizeof(KState), st));
+  PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * (size_t)(ld + 2) * nn, st));
   PSBX_CK(cudaMemsetAsync(small, 0, sizeof(double) * ((size_t)ld * ld + 3 * (size_t)ld), st));
@@ -1917,10 +1917,10 @@ static int solve_cgs(const View &A, const double *dinv, const double *b, double 
   double *vec = nullptr, *part = nullptr;
   KState *S = nullptr;
   unsigned *ticket = nullptr;
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * 8 * nn, st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(psbx_malloc_async(&vec, sizeof(double) * 8 * nn, st));
+  PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(psbx_malloc_async(&S, sizeof(KState), st));
+  PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * 8 * nn, st));
   KState *hS = (KState *)c.h_res;
@@ -2084,9 +2084,9 @@ static int build_transpose(void *mat, int fmt, int n, int **tirp, int **tja, dou
       tj[pos] = i;
       tv[pos] = vals[k];
     }
-  PSBX_CK(cudaMallocAsync(tirp, sizeof(int) * (n + 1), c.stream));
-  PSBX_CK(cudaMallocAsync(tja, sizeof(int) * tj.size(), c.stream));
-  PSBX_CK(cudaMallocAsync(tval, sizeof(double) * tv.size(), c.stream));
+  PSBX_CK(psbx_malloc_async(tirp, sizeof(int) * (n + 1), c.stream));
+  PSBX_CK(psbx_malloc_async(tja, sizeof(int) * tj.size(), c.stream));
+  PSBX_CK(psbx_malloc_async(tval, sizeof(double) * tv.size(), c.stream));
   PSBX_CK(cudaMemcpyAsync(*tirp, tp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream));
   PSBX_CK(cudaMemcpyAsync(*tja, tj.data(), sizeof(int) * tj.size(), cudaMemcpyHostToDevice, c.stream));
   PSBX_CK(cudaMemcpyAsync(*tval, tv.data(), sizeof(double) * tv.size(), cudaMemcpyHostToDevice, c.stream));
@@ -2112,10 +2112,10 @@ static int solve_bicg(const View &A, void *mat, int fmt, const double *dinv, con
   double *vec = nullptr, *part = nullptr;
   KState *S = nullptr;
   unsigned *ticket = nullptr;
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * 8 * nn, st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(psbx_malloc_async(&vec, sizeof(double) * 8 * nn, st));
+  PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(psbx_malloc_async(&S, sizeof(KState), st));
+  PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * 8 * nn, st));
   KState *hS = (KState *)c.h_res;
@@ -2212,12 +2212,12 @@ static int solve_bicgstabl(const View &A, const double *dinv, const double *b, d
   unsigned *ticket = nullptr;
   // rt0, uh(0..nl), rh(0..nl)
   const size_t nv = 1 + 2 * (size_t)ld;
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(double) * nv * nn, st));
-  PSBX_CK(cudaMallocAsync(&small, sizeof(double) * (4 * (size_t)ld + (size_t)ld * ld), st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(KState), st));
-  PSBX_CK(cudaMallocAsync(&L, sizeof(LState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned) * 8, st));
+  PSBX_CK(psbx_malloc_async(&vec, sizeof(double) * nv * nn, st));
+  PSBX_CK(psbx_malloc_async(&small, sizeof(double) * (4 * (size_t)ld + (size_t)ld * ld), st));
+  PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 2 * KLANES * (size_t)grid, st));
+  PSBX_CK(psbx_malloc_async(&S, sizeof(KState), st));
+  PSBX_CK(psbx_malloc_async(&L, sizeof(LState), st));
+  PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 8, st));
   PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(double) * nv * nn, st));
   PSBX_CK(cudaMemsetAsync(small, 0, sizeof(double) * (4 * (size_t)ld + (size_t)ld * ld), st));

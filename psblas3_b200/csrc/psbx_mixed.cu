@@ -363,10 +363,10 @@ static int mx_solve(const View &A64, const HllViewF &A32, bool shortRows, const 
   double *part = nullptr;
   MState *S = nullptr;
   unsigned *ticket = nullptr;
-  PSBX_CK(cudaMallocAsync(&vec, sizeof(float) * 5 * nn, st));
-  PSBX_CK(cudaMallocAsync(&part, sizeof(double) * 4 * (size_t)grid, st));
-  PSBX_CK(cudaMallocAsync(&S, sizeof(MState), st));
-  PSBX_CK(cudaMallocAsync(&ticket, sizeof(unsigned), st));
+  PSBX_CK(psbx_malloc_async(&vec, sizeof(float) * 5 * nn, st));
+  PSBX_CK(psbx_malloc_async(&part, sizeof(double) * 4 * (size_t)grid, st));
+  PSBX_CK(psbx_malloc_async(&S, sizeof(MState), st));
+  PSBX_CK(psbx_malloc_async(&ticket, sizeof(unsigned), st));
   PSBX_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
   PSBX_CK(cudaMemsetAsync(vec, 0, sizeof(float) * 5 * nn, st));
   float *rh = vec, *xh = vec + nn, *p = vec + 2 * nn, *q = vec + 3 * nn, *d32 = vec + 4 * nn;
