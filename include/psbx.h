@@ -524,7 +524,11 @@ int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x,
  * (1 or 8) right-hand sides interleaved as v[row*nrhs + k].  Per rhs: outer
  * FP64 refinement r = b - A x, stop at ||r|| <= eps ||b||, inner Jacobi-CG
  * in FP32 (FP64-accumulated dots) to a relative reduction inner_tol, then
- * x += ||r|| d.  All systems advance together in one persistent grid whose
+ * x += ||r|| d; the next inner loop keeps the search direction (residual
+ * replacement; restarted only after a breakdown or when the true residual
+ * has drifted from the recursive one).  inner_tol 1e-2 suits it: with 1e-4
+ * the FP32 recursion can lose accuracy before it gets there, and the
+ * safeguards then spend iterations.  All systems advance together in one persistent grid whose
  * iterations are captured in a CUDA graph; each system has its own
  * convergence state and leaves the work when done; systems can be added
  * and removed between steps.  A system's results do not depend on which

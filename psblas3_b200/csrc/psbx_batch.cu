@@ -15,6 +15,14 @@
 //     FP32, every dot product accumulated in FP64 (products of two FP32
 //     numbers are exact in FP64)
 //   x = x + ||r|| d                           (FP64)
+// and the next inner loop keeps the search direction (residual replacement:
+// the FP64 residual, rescaled, replaces the recursive one; p carries over
+// with beta = rho_new / (rho_old * ratio), ratio = old scale / new scale, as
+// the direction is in units of the old scale).  The direction restarts
+// (p = z) on the first inner loop, after an inner breakdown, and when the
+// true residual is more than DRIFT times the recursive one.  Compared with
+// restarting every inner loop, the Krylov space is kept, and the inner
+// iterations stay close to an FP64 CG's.
 //
 // Layout: each system is an HLL-32 matrix (FP64 values, FP32 copy, shared
 // indices) with 1-based local columns, and K interleaved vectors
@@ -64,12 +72,25 @@ struct BState {               // written by the kernels
 struct BSol {                 // one right-hand side
   double rho, sigma, alpha, beta;
   double bn2, rn, scale, tau, eps, inner_tol;
+  double ratio;               // scale before the last refinement / scale after it
+  double rrec;                // recursive residual (true units) when the inner loop stopped
   int it, it_total, itmax, outer_max;
   int active;                 // inner CG running for this rhs
   int done;                   // 0 running, 1 converged, 2 stopped (itmax / breakdown)
   int first;                  // bn2 not yet computed
-  int pad;
+  int restart;                // the next inner loop starts a new direction (p = z)
+  int loop_it, loop_cap;      // iterations of the current inner loop, and its bound
 };
+// A refinement whose true residual is more than DRIFT times the inner loop's
+// recursive one, or more than half the previous refinement's, restarts the
+// search direction instead of keeping it.  An
+// inner loop that continues a direction also stops after 4 times the
+// iterations of the loop before it plus LOOP_SLACK: an FP32 recursion that
+// has lost accuracy may never reach its reduction (measured: with
+// inner_tol 1e-4, 14 of 128 anisotropic systems ran to itmax), and the
+// refinement that follows restarts it.
+#define DRIFT 8.0
+#define LOOP_SLACK 64
 
 struct BTile {
   int sys, row0, nrows, kind;  // kind 1: up to 8 long rows (tile_spmv)
@@ -543,6 +564,11 @@ __global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys 
           } else if (so->it_total >= so->itmax || st->outer >= so->outer_max) {
             so->done = 2;
           } else {
+            if (so->scale > 0.0 && so->rn > 0.0) so->ratio = so->scale / so->rn;
+            // restart the direction when the recursion has drifted from the
+            // true residual, or when the last inner loop did not even halve
+            // the true residual
+            if (!(so->rn <= DRIFT * so->rrec) || !(so->rn <= 0.5 * so->scale)) so->restart = 1;
             so->scale = so->rn;
             so->tau = fmax(so->inner_tol, 0.5 * so->eps * (so->bn2 == 0.0 ? 1.0 : so->bn2) / so->rn);
           }
@@ -628,8 +654,18 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
       if (threadIdx.x < K) {
         BSol *so = sol + S.sol0 + threadIdx.x;
         if (so->done == 0) {
-          so->rho = tot[threadIdx.x];
-          so->it = 1;
+          const double rho = tot[threadIdx.x];
+          if (so->restart || !(so->rho > 0.0) || !(so->ratio > 0.0)) {
+            so->it = 1;  // p = z
+            so->loop_cap = 0x7fffffff;
+          } else {
+            so->beta = rho / (so->rho * so->ratio);
+            so->it = 2;  // p = z + beta p
+            so->loop_cap = 4 * so->loop_it + LOOP_SLACK;
+          }
+          so->loop_it = 0;
+          so->restart = 0;
+          so->rho = rho;
           so->active = so->rho > 0.0 ? 1 : 0;
         }
       }
@@ -744,6 +780,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *_
           } else {
             so->active = 0;  // breakdown of the inner solve: refine with what we have
             so->alpha = 0.0;
+            so->restart = 1;
           }
         } else {
           so->alpha = 0.0;
@@ -838,8 +875,11 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
           const double rz = tot[k];
           const double rr = tot[K + k];
           so->it_total += 1;
-          if (sqrt(rr) <= so->tau || so->it_total >= so->itmax || rz <= 0.0) {
+          so->loop_it += 1;
+          if (sqrt(rr) <= so->tau || so->it_total >= so->itmax || rz <= 0.0 || so->loop_it >= so->loop_cap) {
             so->active = 0;
+            so->rrec = sqrt(rr) * so->scale;  // rho stays: the next inner loop forms beta from it
+            if (rz <= 0.0) so->restart = 1;
           } else {
             so->beta = rz / so->rho;
             so->rho = rz;
@@ -1175,6 +1215,7 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
     so[k].itmax = itmax;
     so[k].outer_max = 64;
     so[k].first = 1;
+    so[k].restart = 1;
   }
   e->h_sys[s] = S;
   e->used[s] = 1;

@@ -447,7 +447,7 @@ class BatchSolver:
         self.h = h
         self.keep = {}
 
-    def add(self, A, d_b, d_x, d_dinv=None, eps=1e-10, inner_tol=1e-4, itmax=100000, keep=None):
+    def add(self, A, d_b, d_x, d_dinv=None, eps=1e-10, inner_tol=1e-2, itmax=100000, keep=None):
         """A: HllMat (hack 32); d_b, d_x, d_dinv: device pointers (ints) or
         torch tensors (rows*nrhs doubles, interleaved).  Returns the slot."""
         def ptr(t):

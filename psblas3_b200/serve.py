@@ -70,7 +70,7 @@ class Request:
 
 
 class Server:
-    def __init__(self, pool, hbm_budget=150e9, max_slots=512, max_rows_total=200_000_000, inner_tol=1e-4,
+    def __init__(self, pool, hbm_budget=150e9, max_slots=512, max_rows_total=200_000_000, inner_tol=1e-2,
                  itmax=200_000, replays_per_step=2, engine=None):
         """engine: a psb.BatchSolver-like object (add/launch/wait/poll/remove/free);
         by default a new 1-rhs batch engine with max_slots slots."""
