@@ -136,3 +136,26 @@ def test_finished_slots_count_until_retired(monkeypatch):
         assert len(srv.eng.slots) <= 2
         t += 1.0
     assert sorted(r.rid for r in srv.done) == list(range(6))
+
+
+def test_stream_window_reports_unfinished(monkeypatch):
+    """run_stream with stop_at: arrivals past the window are not served, the
+    requests not complete at the window's end come back unfinished, and only
+    completions inside the window count."""
+    srv = _server([100, 5000], budget_rows=10**9, max_slots=4, monkeypatch=monkeypatch)
+    t = [0.0]
+
+    def clock():
+        t[0] += 0.01
+        return t[0]
+
+    srv.clock = clock
+    reqs = [serve.Request(i, i % 2, i, 1e-10, 0.05 * i) for i in range(40)]
+    wall, left = serve.run_stream(srv, reqs, clock=clock, stop_at=1.0)
+    done = srv.done
+    assert done and left
+    assert {r.rid for r in done}.isdisjoint({r.rid for r in left})
+    assert len(done) + len(left) == 40
+    end = reqs[0].t_arrive - 0.0 + 1.0  # arrival times were shifted to the stream's start
+    assert all(r.t_done <= end for r in done)
+    assert not srv.running and not srv.queue
