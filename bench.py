@@ -527,6 +527,23 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
         states.append(st)
         iters.extend(its)
         worst = max(worst, max(err))
+    # the same systems through the engine with FP64 inner iterations: the
+    # batched FP64 solve (batching without the FP32 inner iterations)
+    eng64 = psb.BatchSolver(n_sys, total, k, inner_fp64=True)
+    xs64 = [torch.zeros_like(db) for (_, _, _, _, _, _, db, _) in mats]
+    slots64 = [eng64.add(A, db, x64, P.dv.data_ptr, eps=1e-10)
+               for (_, _, _, _, A, P, db, _), x64 in zip(mats, xs64)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng64.run(replays_per_step=4)
+    tb64 = time.perf_counter() - t0
+    states64, iters64 = [], []
+    for s in slots64:
+        st, outer, its, err = eng64.poll(s)
+        states64.append(st)
+        iters64.extend(its)
+    eng64.free()
+    del xs64
     # FP64 check of a few solutions on the host (oracle CSR product)
     checked = 0.0
     for i in rng.choice(n_sys, 4, replace=False):
@@ -555,6 +572,10 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
     solves = n_sys * k
     return {"systems": n_sys, "rhs_per_system": k, "rows_total": total, "batched_s": tb,
             "batched_solves_per_s": solves / tb, "converged": int(sum(1 for s in states if s == 1)),
+            "fp64_batched_s": tb64, "fp64_batched_solves_per_s": solves / tb64,
+            "fp64_batched_converged": int(sum(1 for s in states64 if s == 1)),
+            "fp64_batched_inner_iters_median": float(np.median(iters64)),
+            "mixed_over_fp64_batched": tb64 / tb,
             "max_err": worst, "host_checked_max_relres": checked, "inner_iters_max": int(max(iters)),
             "inner_iters_median": float(np.median(iters)), "kernel_launches": int(launches),
             "fp64_one_at_a_time_solves_per_s": len(pairs) / t64, "fp64_sample": len(pairs),

@@ -543,6 +543,11 @@ int psbx_hll_spmv_raw(void *deviceMat, double alpha, const double *x,
  *   poll   : state 0 running / 1 converged / 2 stopped (itmax, breakdown);
  *            outer steps, inner iterations and ||b-Ax||/||b|| per rhs */
 int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs);
+/* The same engine with the inner iterations in FP32 (inner_bits 32, as
+ * psbx_batch_create) or in FP64 (64: FP64 values and vectors throughout --
+ * the batched FP64 solve, to tell the gain of batching from that of the
+ * FP32 inner iterations). */
+int psbx_batch_create_prec(void **eng, int max_systems, int max_rows_total, int nrhs, int inner_bits);
 int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, const double *d_dinv, double eps,
                    double inner_tol, int itmax, int *slot);
 int psbx_batch_step(void *eng, int replays, int *n_running);

@@ -145,7 +145,7 @@ _SIGS = {
     "psbx_wrapMultiVecDevice": (I, [PP, P, U, U]), "psbx_multivec_data": (P, [P]),
     "psbx_hll_spmv_raw": (I, [P, D, P, D, P]),
     "psbx_dot_noalloc": (I, [P, I, I, P, P, I, P]),
-    "psbx_batch_create": (I, [PP, I, I, I]),
+    "psbx_batch_create": (I, [PP, I, I, I]), "psbx_batch_create_prec": (I, [PP, I, I, I, I]),
     "psbx_batch_add": (I, [P, P, P, P, P, D, D, I, PI]),
     "psbx_batch_step": (I, [P, I, PI]),
     "psbx_batch_launch": (I, [P, I]), "psbx_batch_wait": (I, [P, PI]),

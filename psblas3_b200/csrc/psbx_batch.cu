@@ -57,10 +57,16 @@ struct BSys {                 // read-only for the kernels
   const int *ja, *irn, *hkoffs;
   const double *b;
   double *x, *r64;
-  float *r32, *z, *p, *q, *d;
-  const float *dinv;
+  void *r32, *z, *p, *q, *d;  // inner vectors, of the engine's inner type (float, or double)
+  const void *dinv;           // inverse diagonal, inner type
   int rows, sol0, tile0, ntiles;
 };
+
+// The inner iterations' values: the FP32 copy, or the FP64 values for an
+// engine whose inner iterations run in FP64 (the batched FP64 comparison).
+template <class TI> __device__ __forceinline__ const TI *inner_val(const BSys &S);
+template <> __device__ __forceinline__ const float *inner_val<float>(const BSys &S) { return S.val32; }
+template <> __device__ __forceinline__ const double *inner_val<double>(const BSys &S) { return S.val64; }
 
 struct BState {               // written by the kernels
   int phase;
@@ -105,6 +111,7 @@ struct BCtl {                 // read by every kernel at launch; lets the tile
 
 struct Eng {
   int K = 1, max_sys = 0, max_tiles = 0, grid = 0;
+  int fp64 = 0;               // inner iterations in FP64 (the batched FP64 comparison) instead of FP32
   BSys *d_sys = nullptr;
   BState *d_state = nullptr;
   BSol *d_sol = nullptr;
@@ -588,7 +595,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::resid_blocks) kb_resid(const BSys 
 }
 
 // PH_INIT: r32 = r/scale, z = D r32, d = 0; rho = (r32, z).
-template <int K>
+template <int K, class TI>
 __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__restrict__ sys, BState *state,
                                                               BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 2 : 1;  // rows per thread whose loads are in flight together
@@ -611,16 +618,16 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
       inv[k] = live[k] ? 1.0 / so->scale : 0.0;
     }
     const double *__restrict__ r64 = S.r64;
-    const float *__restrict__ dinv = S.dinv;
-    float *__restrict__ r32 = S.r32;
-    float *__restrict__ z = S.z;
-    float *__restrict__ d = S.d;
+    const TI *__restrict__ dinv = (const TI *)S.dinv;
+    TI *__restrict__ r32 = (TI *)S.r32;
+    TI *__restrict__ z = (TI *)S.z;
+    TI *__restrict__ d = (TI *)S.d;
     double v[1][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = 0.0;
     for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
       double rv64[RB][K];
-      float dg[RB];
+      TI dg[RB];
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
@@ -635,12 +642,12 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
         const size_t r = (size_t)T.row0 + i;
-        float rv[K], zv[K], dz[K];
+        TI rv[K], zv[K], dz[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-          rv[k] = live[k] ? (float)rmul(rv64[u][k], inv[k]) : 0.0f;
-          zv[k] = rmulf(dg[u], rv[k]);
-          dz[k] = 0.0f;
+          rv[k] = live[k] ? (TI)rmul(rv64[u][k], inv[k]) : TI(0);
+          zv[k] = rmul(dg[u], rv[k]);
+          dz[k] = TI(0);
           v[0][k] = radd(v[0][k], rmul((double)rv[k], (double)zv[k]));
         }
         st_row<K>(r32 + r * K, rv);
@@ -680,7 +687,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_init(const BSys *__rest
 }
 
 // PH_INNER: p = z (it == 1) or p = z + beta p, for active rhs.
-template <int K>
+template <int K, class TI>
 __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restrict__ sys, const BState *state,
                                                            const BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
@@ -691,17 +698,17 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
     const BTile T = tiles[t];
     if (state[T.sys].phase != PH_INNER) continue;
     const BSys &S = sys[T.sys];
-    float beta[K];
+    TI beta[K];
     bool act[K], first[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const BSol *so = sol + S.sol0 + k;
       act[k] = so->active;
       first[k] = so->it == 1;
-      beta[k] = (float)so->beta;
+      beta[k] = (TI)so->beta;
     }
-    const float *__restrict__ z = S.z;
-    float *__restrict__ p = S.p;
+    const TI *__restrict__ z = (const TI *)S.z;
+    TI *__restrict__ p = (TI *)S.p;
     // p of a stopped rhs keeps its value; it is read only when some rhs
     // is past its first inner iteration or stopped
     bool any_act = false, need_p = false;
@@ -712,13 +719,13 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
     }
     if (!any_act) continue;
     for (int i0 = threadIdx.x; i0 < T.nrows; i0 += RB * BT) {
-      float zv[RB][K], pv[RB][K];
+      TI zv[RB][K], pv[RB][K];
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
         const size_t o = ((size_t)T.row0 + i) * K;
 #pragma unroll
-        for (int k = 0; k < K; k++) pv[u][k] = 0.0f;
+        for (int k = 0; k < K; k++) pv[u][k] = TI(0);
         if (i < T.nrows) {
           ld_row<K>(z + o, zv[u]);
           if (need_p) ld_row<K>(p + o, pv[u]);
@@ -729,10 +736,10 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
         const size_t o = ((size_t)T.row0 + i) * K;
-        float pn[K];
+        TI pn[K];
 #pragma unroll
         for (int k = 0; k < K; k++)
-          pn[k] = !act[k] ? pv[u][k] : first[k] ? zv[u][k] : raddf(zv[u][k], rmulf(beta[k], pv[u][k]));
+          pn[k] = !act[k] ? pv[u][k] : first[k] ? zv[u][k] : radd(zv[u][k], rmul(beta[k], pv[u][k]));
         st_row<K>(p + o, pn);
       }
     }
@@ -740,7 +747,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_p(const BSys *__restric
 }
 
 // PH_INNER: q = A32 p ; sigma = (p, q) ; alpha = rho / sigma.
-template <int K>
+template <int K, class TI>
 __global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *__restrict__ sys, BState *state,
                                                               BSol *sol, const BCtl *ctl) {
   __shared__ double sm[32 * 2 * MAXK];
@@ -756,14 +763,14 @@ __global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *_
     double v[1][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = 0.0;
-    const float *__restrict__ p = S.p;
-    float *__restrict__ q = S.q;
-    tile_spmv<float, float, K>(S, T, S.val32, p, [&](int r, const double (&aq)[K]) {
-      float pv[K], qv[K];
+    const TI *__restrict__ p = (const TI *)S.p;
+    TI *__restrict__ q = (TI *)S.q;
+    tile_spmv<TI, TI, K>(S, T, inner_val<TI>(S), p, [&](int r, const double (&aq)[K]) {
+      TI pv[K], qv[K];
       ld_row<K>(p + (size_t)r * K, pv);
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        qv[k] = (float)aq[k];
+        qv[k] = (TI)aq[k];
         v[0][k] = radd(v[0][k], rmul((double)pv[k], (double)qv[k]));
       }
       st_row<K>(q + (size_t)r * K, qv);
@@ -794,7 +801,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::spmv_blocks) kb_spmv(const BSys *_
 
 // PH_INNER: d += alpha p ; r -= alpha q ; z = D r ; (r,z), (r,r) ; inner stop
 // test per rhs ; all rhs stopped -> PH_XUPD.
-template <int K>
+template <int K, class TI>
 __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSys *__restrict__ sys, BState *state,
                                                                 BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
@@ -808,20 +815,20 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
     BState *st = state + T.sys;
     if (st->phase != PH_INNER) continue;
     const BSys &S = sys[T.sys];
-    float alpha[K];
+    TI alpha[K];
     bool act[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const BSol *so = sol + S.sol0 + k;
       act[k] = so->active;
-      alpha[k] = (float)so->alpha;
+      alpha[k] = (TI)so->alpha;
     }
-    const float *__restrict__ p = S.p;
-    const float *__restrict__ q = S.q;
-    const float *__restrict__ dinv = S.dinv;
-    float *__restrict__ d = S.d;
-    float *__restrict__ r32 = S.r32;
-    float *__restrict__ z = S.z;
+    const TI *__restrict__ p = (const TI *)S.p;
+    const TI *__restrict__ q = (const TI *)S.q;
+    const TI *__restrict__ dinv = (const TI *)S.dinv;
+    TI *__restrict__ d = (TI *)S.d;
+    TI *__restrict__ r32 = (TI *)S.r32;
+    TI *__restrict__ z = (TI *)S.z;
     double v[2][K];
 #pragma unroll
     for (int k = 0; k < K; k++) v[0][k] = v[1][k] = 0.0;
@@ -831,7 +838,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
 #pragma unroll
     for (int k = 0; k < K; k++) any_act |= act[k];
     for (int i0 = threadIdx.x; any_act && i0 < T.nrows; i0 += RB * BT) {
-      float dv[RB][K], pv[RB][K], rv[RB][K], qv[RB][K], dg[RB];
+      TI dv[RB][K], pv[RB][K], rv[RB][K], qv[RB][K], dg[RB];
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
@@ -849,12 +856,12 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
         const int i = i0 + u * BT;
         if (i >= T.nrows) continue;
         const size_t o = ((size_t)T.row0 + i) * K;
-        float dn[K], rn[K], zn[K];
+        TI dn[K], rn[K], zn[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-          dn[k] = act[k] ? raddf(dv[u][k], rmulf(alpha[k], pv[u][k])) : dv[u][k];
-          rn[k] = act[k] ? raddf(rv[u][k], -rmulf(alpha[k], qv[u][k])) : rv[u][k];
-          zn[k] = rmulf(dg[u], rn[k]);
+          dn[k] = act[k] ? radd(dv[u][k], rmul(alpha[k], pv[u][k])) : dv[u][k];
+          rn[k] = act[k] ? radd(rv[u][k], -rmul(alpha[k], qv[u][k])) : rv[u][k];
+          zn[k] = rmul(dg[u], rn[k]);
           if (act[k]) {
             v[0][k] = radd(v[0][k], rmul((double)rn[k], (double)zn[k]));
             v[1][k] = radd(v[1][k], rmul((double)rn[k], (double)rn[k]));
@@ -899,7 +906,7 @@ __global__ void __launch_bounds__(BT, Occ<K>::update_blocks) kb_update(const BSy
 }
 
 // PH_XUPD: x += scale * d (FP64) for rhs still running ; -> PH_RESID.
-template <int K>
+template <int K, class TI>
 __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__restrict__ sys, BState *state,
                                                               const BSol *sol, const BCtl *ctl) {
   constexpr int RB = K == 1 ? 4 : 1;
@@ -918,13 +925,13 @@ __global__ void __launch_bounds__(BT, Occ<K>::blocks) kb_xupd(const BSys *__rest
       sc[k] = so->done == 0 ? so->scale : 0.0;
     }
     double *__restrict__ x = S.x;
-    const float *__restrict__ d = S.d;
+    const TI *__restrict__ d = (const TI *)S.d;
     bool any = false;
 #pragma unroll
     for (int k = 0; k < K; k++) any |= sc[k] != 0.0;
     for (int i0 = threadIdx.x; any && i0 < T.nrows; i0 += RB * BT) {
       double xv[RB][K];
-      float dv[RB][K];
+      TI dv[RB][K];
 #pragma unroll
       for (int u = 0; u < RB; u++) {
         const int i = i0 + u * BT;
@@ -969,21 +976,22 @@ __global__ void kb_set_phase(BState *state, int *count, int slot, int phase) {
   if (phase != PH_IDLE) atomicAdd(count + phase, 1);
 }
 
-__global__ void kb_d2f_inv(int n, const double *__restrict__ dinv, float *__restrict__ out) {
+template <class TI>
+__global__ void kb_dinv(int n, const double *__restrict__ dinv, TI *__restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = dinv ? (float)dinv[i] : 1.0f;
+    out[i] = dinv ? (TI)dinv[i] : TI(1);
 }
 
 // --------------------------------------------------------------- host side
-template <int K>
+template <int K, class TI>
 static void capture_iters(Eng *e, cudaStream_t st) {
   for (int it = 0; it < ITERS; it++) {
-    kb_xupd<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_xupd<K, TI><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
     kb_resid<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
-    kb_init<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
-    kb_p<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
-    kb_spmv<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
-    kb_update<K><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_init<K, TI><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_p<K, TI><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_spmv<K, TI><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
+    kb_update<K, TI><<<e->grid, BT, 0, st>>>(e->d_sys, e->d_state, e->d_sol, e->d_ctl);
   }
 }
 
@@ -1094,12 +1102,18 @@ static int upload_tables(Eng *e, cudaStream_t st) {
 extern "C" {
 
 int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs) {
+  return psbx_batch_create_prec(eng, max_systems, max_rows_total, nrhs, 32);
+}
+
+int psbx_batch_create_prec(void **eng, int max_systems, int max_rows_total, int nrhs, int inner_bits) {
   int rc = psbx_ensure_init();
   if (rc) return rc;
   if (!eng || max_systems <= 0 || max_rows_total <= 0 || (nrhs != 1 && nrhs != 8)) return SPGPU_UNSUPPORTED;
+  if (inner_bits != 32 && inner_bits != 64) return SPGPU_UNSUPPORTED;
   PsbxCtx &c = psbx_ctx();
   Eng *e = new Eng();
   e->K = nrhs;
+  e->fp64 = inner_bits == 64;
   e->max_sys = max_systems;
   e->max_tiles = max_rows_total / tile_rows(e->K) + max_systems + 1;
   e->grid = c.sms * 8;
@@ -1137,8 +1151,8 @@ int psbx_batch_create(void **eng, int max_systems, int max_rows_total, int nrhs)
   if (!rc) {
     err = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
-      if (nrhs == 1) capture_iters<1>(e, c.stream);
-      else capture_iters<8>(e, c.stream);
+      if (nrhs == 1) e->fp64 ? capture_iters<1, double>(e, c.stream) : capture_iters<1, float>(e, c.stream);
+      else e->fp64 ? capture_iters<8, double>(e, c.stream) : capture_iters<8, float>(e, c.stream);
       err = cudaStreamEndCapture(c.stream, &e->graph);
     }
     if (err == cudaSuccess) err = cudaGraphInstantiate(&e->gexec, e->graph, 0);
@@ -1179,8 +1193,9 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   PsbxCtx &c = psbx_ctx();
   const int K = e->K;
   const size_t n = (size_t)m->rows;
-  // one allocation per slot: r64 (K n doubles), r32 z p q d (5 K n floats), dinv (n floats)
-  const size_t bytes = sizeof(double) * K * n + sizeof(float) * (5 * K + 1) * n + 256;
+  // one allocation per slot: r64 (K n doubles), r32 z p q d (5 K n inner values), dinv (n inner values)
+  const size_t ti = e->fp64 ? sizeof(double) : sizeof(float);
+  const size_t bytes = sizeof(double) * K * n + ti * (5 * K + 1) * n + 256;
   char *buf = nullptr;
   cudaError_t err = psbx_malloc_async((void **)&buf, bytes, c.stream);
   if (err != cudaSuccess) return psbx_cuda_status(err, "psbx_batch_add");
@@ -1194,18 +1209,19 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   S.b = d_b;
   S.x = d_x;
   S.r64 = (double *)buf;
-  float *f = (float *)(buf + sizeof(double) * K * n);
+  char *f = buf + sizeof(double) * K * n;
   S.r32 = f;
-  S.z = f + K * n;
-  S.p = f + 2 * K * n;
-  S.q = f + 3 * K * n;
-  S.d = f + 4 * K * n;
-  float *dv = f + 5 * K * n;
+  S.z = f + ti * K * n;
+  S.p = f + 2 * ti * K * n;
+  S.q = f + 3 * ti * K * n;
+  S.d = f + 4 * ti * K * n;
+  char *dv = f + 5 * ti * K * n;
   S.dinv = dv;
   S.rows = (int)n;
   S.sol0 = s * K;
   e->plan[s].assign(m->tplan, m->tplan + 3 * (size_t)m->ntplan);
-  kb_d2f_inv<<<psbx_grid_for(n, 256), 256, 0, c.stream>>>((int)n, d_dinv, dv);
+  if (e->fp64) kb_dinv<double><<<psbx_grid_for(n, 256), 256, 0, c.stream>>>((int)n, d_dinv, (double *)dv);
+  else kb_dinv<float><<<psbx_grid_for(n, 256), 256, 0, c.stream>>>((int)n, d_dinv, (float *)dv);
   psbx_count_launch();
   std::vector<BSol> so(K);
   memset(so.data(), 0, sizeof(BSol) * K);

@@ -440,10 +440,13 @@ class BatchSolver:
     with FP64-accumulated dots inside FP64 iterative refinement, many
     systems advancing together; systems join and leave between steps."""
 
-    def __init__(self, max_systems, max_rows_total, nrhs=1):
+    def __init__(self, max_systems, max_rows_total, nrhs=1, inner_fp64=False):
+        """inner_fp64: inner iterations in FP64 instead of FP32 (the batched
+        FP64 solve)."""
         self.nrhs = int(nrhs)
         h = C.c_void_p()
-        check(lib.psbx_batch_create(C.byref(h), int(max_systems), int(max_rows_total), self.nrhs), "batch_create")
+        check(lib.psbx_batch_create_prec(C.byref(h), int(max_systems), int(max_rows_total), self.nrhs,
+                                         64 if inner_fp64 else 32), "batch_create")
         self.h = h
         self.keep = {}
 

@@ -169,3 +169,33 @@ def test_remove_and_reuse_slot(psb):
         eng.remove(s)
         xs.append((db, dx))
     eng.free()
+
+
+@pytest.mark.parametrize("k", [1, 8])
+def test_fp64_inner_engine(psb, k):
+    """The engine with FP64 inner iterations (the batched FP64 solve): every
+    right-hand side reaches the FP64 tolerance, and its iterations stay
+    close to the FP64 device CG's on the same system (its refinements keep
+    the search direction)."""
+    import torch
+    systems = _aniso_set(11, 5, k)
+    total = sum(len(s[0]) - 1 for s in systems)
+    eng = psb.BatchSolver(len(systems), total, k, inner_fp64=True)
+    keep, slots = [], []
+    for irp, ja, va, rhs in systems:
+        A, P = _system(psb, irp, ja, va)
+        db = torch.from_numpy(np.ascontiguousarray(rhs.reshape(-1))).cuda()
+        dx = torch.zeros_like(db)
+        slots.append(eng.add(A, db, dx, P.dv.data_ptr, eps=EPS))
+        keep.append((A, P, db, dx))
+    eng.run()
+    for (irp, ja, va, rhs), s, (A, P, db, dx) in zip(systems, slots, keep):
+        st, outer, its, err = eng.poll(s)
+        assert st == 1, (st, its, err)
+        x = dx.cpu().numpy().reshape(-1, k)
+        for j in range(k):
+            assert _true_relres(irp, ja, va, x[:, j], rhs[:, j]) <= 1.01 * EPS
+        B, X = psb.DVect.bld(rhs[:, 0]), psb.DVect(len(irp) - 1)
+        it64, _ = psb.psb_krylov("CG", A, P, B, X, eps=EPS, itmax=100000)
+        assert its[0] <= 1.1 * it64 + 10, (its[0], it64)
+    eng.free()
