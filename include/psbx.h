@@ -483,12 +483,13 @@ int psbx_hll_from_csr_device(void **deviceMat, int rows, int cols, int nnz,
  * row" of the GPU HLL SpMV; the reference fixes hksz = 32,
  * psb_d_cuda_cp_hlg_from_coo.F90:60): builds each candidate layout -- hack
  * size 32, 64 or 128 and, for hack size 32, the width above which a hack
- * takes the wide path (its products formed by all blocks at once, then
- * added in stored order by a warp per hack: 32, 64, 128, 256, 1024 or
- * never) -- times its SpMV on the library stream and keeps the fastest.
- * All candidates sum every row in stored order, so the products are the
- * same bits; *hksz, *wide_w (-1 never, 0 not applicable) and *ms (one SpMV)
- * describe the choice.  Arguments otherwise as psbx_hll_from_csr_device. */
+ * takes the wide path (32, 64, 128, 256, 1024 or never) and the threads per
+ * row of the other hacks (two rows per thread, one, or two threads per row)
+ * -- times its SpMV on the library stream and keeps the fastest.  The handle
+ * comes back in the tolerance mode; after psbx_hll_set_wide_split(m, 0)
+ * every layout gives the CPU csmv's bits.  *hksz, *wide_w (-1 never, 0 not
+ * applicable) and *ms (one SpMV) describe the choice, psbx_hll_get_layout
+ * the row mapping.  Arguments otherwise as psbx_hll_from_csr_device. */
 int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int cols,
                                       int nnz, const int *d_irp,
                                       const int *d_ja, const double *d_val,
@@ -497,10 +498,37 @@ int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int cols,
 
 /* Sets the wide-hack threshold of a hack-32 HLL matrix built by this
  * library (0: default -- 64 or four times the mean hack width, whichever is
- * larger; < 0: never) and rebuilds its wide-hack lists.  Every threshold
- * gives the same bits; only the time changes.  Returns SPGPU_UNSUPPORTED for
+ * larger; < 0: never) and rebuilds its wide-hack lists.  In the exact mode
+ * every threshold gives the same bits; only the time changes.  Returns SPGPU_UNSUPPORTED for
  * another hack size unless wide_w is 0. */
 int psbx_hll_set_wide(void *deviceMat, int wide_w);
+
+/* Tolerance or exact mode of an HLL handle.  1 (the default), tolerance:
+ * each 64-column chunk of a wide hack (hack size 32) is summed by a block
+ * (its 8 warps taking interleaved columns) and the chunks' row partials are
+ * added in column order, in the same launch as the other rows -- no product
+ * buffer, no long serial chain -- and the standalone SpMV may take two
+ * threads per row (psbx_hll_set_threads_per_row); every row is then within
+ * |dy_i| <= len_i u sum_j |a_ij x_j| of the stored-order sum.  0, exact:
+ * every row in stored order (wide hacks: products by all blocks, then a warp
+ * per hack adds them in order), the CPU csmv's bits.  Every solver and
+ * product on the handle follows it.  The reference's own GPU HLL kernels
+ * (fused multiply-add, two-thread rows) are a tolerance mode too. */
+int psbx_hll_set_wide_split(void *deviceMat, int split);
+
+/* Row mapping of the standalone SpMV on a hack-32 HLL handle: 0 auto (two
+ * rows per thread when there are wide hacks, one otherwise), 1 one thread
+ * per row, 2 two threads per row (entries of even and odd position summed
+ * apart and then added -- the reference's two-thread HLL mode,
+ * hell_spmv_base_template.cuh:63; tolerance mode only, the exact mode takes
+ * -2 instead), -2 two adjacent rows per thread (double2/int2 loads, stored
+ * order).  Other hack sizes accept 0 and 1.  The solvers' fused kernels keep
+ * their own mapping.  psbx_hll_autotune_from_csr_device picks it. */
+int psbx_hll_set_threads_per_row(void *deviceMat, int tpr);
+
+/* The layout of an HLL handle: hack size, wide threshold as set (0
+ * default), tolerance (1) or exact (0) mode, row mapping. */
+int psbx_hll_get_layout(void *deviceMat, int *hksz, int *wide_w, int *split, int *tpr);
 
 /* Adds an FP32 copy of the values of an FP64 HLL handle (for the FP32 inner
  * iterations of the mixed-precision solver). */

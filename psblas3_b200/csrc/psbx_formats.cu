@@ -65,6 +65,7 @@ int FallocHllDevice(void **deviceMat, unsigned hksize, unsigned rows, unsigned n
   m->elemType = (int)elementType;
   m->cols = (int)rows;
   m->maxRowLen = -1;
+  m->wideSplit = 1;  // tolerance mode by default; psbx_hll_set_wide_split(m, 0) for the exact sums
   rc = dmalloc((void **)&m->rP, sizeof(int) * (size_t)allocsize);
   if (!rc) rc = dmalloc((void **)&m->rS, sizeof(int) * (size_t)rows);
   if (!rc) rc = dmalloc((void **)&m->diag, sizeof(int) * (size_t)rows);
@@ -96,6 +97,9 @@ void freeHllDevice(void *deviceMat) {
   cudaFree(m->wideBase);
   cudaFree(m->wchunk);
   cudaFree(m->wprod);
+  cudaFree(m->wpart);
+  cudaFree(m->wticket);
+  cudaFree(m->wcbase);
   free(m->tplan);
   free(m);
 }
@@ -1059,10 +1063,11 @@ int d_spmvCSRGDevice(psbx_d_Cmat *Mat, double alpha, void *deviceX, double beta,
 // keeps the one with the fastest SpMV (CUDA events on the library stream,
 // 2 warm-up and 5 timed products with x = 0): hack size 32, 64 or 128 and,
 // for hack size 32, the width above which a hack takes the wide path
-// (products formed by all blocks at once, then added in order by a warp per
-// hack): 32, 64, 128, 256, 1024 or never.
-// Every candidate sums each row in stored order, so all give the same bits;
-// the choice changes time only.
+// (summed by all blocks in 64-column chunks): 32, 64, 128, 256, 1024 or
+// never, and the threads per row of the narrow hacks: two rows per thread,
+// one, or two threads per row (entries of even and odd position).  The
+// result is in the tolerance mode (the default); psbx_hll_set_wide_split(m,
+// 0) afterwards gives the stored-order sums, the same bits for every layout.
 static int cst(cudaError_t e, const char *where) { return e == cudaSuccess ? 0 : psbx_cuda_status(e, where); }
 
 static int time_hll(HllDevice *m, const double *x, double *y, double *ms) {
@@ -1102,12 +1107,16 @@ extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int
   static const int hks[] = {32, 64, 128};
   static const int ws[] = {32, 64, 128, 256, 1024, -1};
   const int nws = (int)(sizeof(ws) / sizeof(ws[0]));
+  static const int tps[] = {-2, 1, 2};
+  const int ntps = (int)(sizeof(tps) / sizeof(tps[0]));
+  int best_tp = 0;
   for (int hi = 0; hi < 3 && !rc; hi++) {
     HllDevice *m = nullptr;
     rc = psbx_hll_from_csr_device((void **)&m, rows, cols, nnz, d_irp, d_ja, d_val, hks[hi], d_perm);
     if (rc) break;
     const int nw = hks[hi] == 32 ? nws : 1;
-    int m_best_w = 0;
+    const int ntp = hks[hi] == 32 ? ntps : 1;
+    int m_best_w = 0, m_best_tp = 0;
     double m_best = -1.0;
     for (int wi = 0; wi < nw && !rc; wi++) {
       if (hks[hi] == 32) {
@@ -1117,11 +1126,15 @@ extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int
         rc = psbx_hll_index_long(m);
         if (rc) break;
       }
-      double t = 0.0;
-      rc = time_hll(m, x, y, &t);
-      if (!rc && (m_best < 0.0 || t < m_best)) {
-        m_best = t;
-        m_best_w = hks[hi] == 32 ? ws[wi] : 0;
+      for (int ti = 0; ti < ntp && !rc; ti++) {
+        m->tpr = hks[hi] == 32 ? tps[ti] : 0;
+        double t = 0.0;
+        rc = time_hll(m, x, y, &t);
+        if (!rc && (m_best < 0.0 || t < m_best)) {
+          m_best = t;
+          m_best_w = hks[hi] == 32 ? ws[wi] : 0;
+          m_best_tp = m->tpr;
+        }
       }
     }
     if (!rc && (!best || m_best < best_ms)) {
@@ -1129,12 +1142,14 @@ extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int
       best = m;
       best_ms = m_best;
       best_w = m_best_w;
+      best_tp = m_best_tp;
     } else {
       freeHllDevice(m);
     }
   }
   if (!rc && best && best->hackSize == 32) {
     best->longW = best_w;
+    best->tpr = best_tp;
     rc = psbx_hll_index_long(best);
   }
   cudaFree(x);
@@ -1152,8 +1167,8 @@ extern "C" int psbx_hll_autotune_from_csr_device(void **deviceMat, int rows, int
 }
 
 // Sets the wide-hack threshold of a hack-32 HLL matrix (0: default, < 0:
-// never) and rebuilds its wide-hack lists; results are the same bits for
-// every threshold.
+// never) and rebuilds its wide-hack lists; in the exact mode the results are
+// the same bits for every threshold.
 extern "C" int psbx_hll_set_wide(void *deviceMat, int wide_w) {
   int rc = psbx_ensure_init();
   if (rc) return rc;
@@ -1162,4 +1177,34 @@ extern "C" int psbx_hll_set_wide(void *deviceMat, int wide_w) {
   if (m->hackSize != 32) return wide_w == 0 ? SPGPU_SUCCESS : SPGPU_UNSUPPORTED;
   m->longW = wide_w;
   return psbx_hll_index_long(m);
+}
+
+// Tolerance mode (1, the default: wide hacks summed split over 8 warps, two
+// threads per row allowed) or exact mode (0: every row in stored order, the
+// CPU csmv's bits).  See k_hll_wide_split.
+extern "C" int psbx_hll_set_wide_split(void *deviceMat, int split) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m || (split != 0 && split != 1)) return SPGPU_UNSUPPORTED;
+  m->wideSplit = split;
+  return SPGPU_SUCCESS;
+}
+
+// Row mapping of the standalone HLL SpMV (hack size 32): 0 auto, 1 or 2
+// threads per row, -2 two rows per thread.  Other hack sizes take 0 or 1.
+extern "C" int psbx_hll_set_threads_per_row(void *deviceMat, int tpr) {
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m || (tpr != 0 && tpr != 1 && tpr != 2 && tpr != -2)) return SPGPU_UNSUPPORTED;
+  if (m->hackSize != 32 && tpr != 0 && tpr != 1) return SPGPU_UNSUPPORTED;
+  m->tpr = tpr;
+  return SPGPU_SUCCESS;
+}
+
+extern "C" int psbx_hll_get_layout(void *deviceMat, int *hksz, int *wide_w, int *split, int *tpr) {
+  const HllDevice *m = (const HllDevice *)deviceMat;
+  if (!m) return SPGPU_UNSUPPORTED;
+  if (hksz) *hksz = m->hackSize;
+  if (wide_w) *wide_w = m->longW;
+  if (split) *split = m->wideSplit;
+  if (tpr) *tpr = m->tpr;
+  return SPGPU_SUCCESS;
 }

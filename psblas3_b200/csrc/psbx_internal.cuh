@@ -58,6 +58,13 @@ struct HllDevice {
   int *wchunk;       // 2*nWChunks: (wide hack index, first entry column) per product block
   int nWChunks;
   double *wprod;     // products of the wide hacks, laid out as their values
+  int wideSplit;     // 1 (default): tolerance mode -- wide hacks summed in column chunks, two
+                     // threads per row allowed; 0: every row in stored order (exact)
+  int tpr;           // standalone SpMV row mapping (hack size 32): 0 auto, 1 or 2 threads per
+                     // row, -2 two rows per thread
+  double *wpart;     // split mode: 32 row partials per product block (nWChunks x 32)
+  unsigned *wticket; // split mode: per wide hack, product blocks done (kept at zero between calls)
+  int *wcbase;       // nLong+1: first product block of each wide hack
 };
 
 // Default width above which a hack of 32 rows takes the wide-hack path.
@@ -395,6 +402,10 @@ struct HllView {
   const int *wchunk;     // (wide hack index, first column) of each product block
   double *wprod;
   int nWChunks;
+  int wideSplit;         // wide rows summed in column chunks (see psbx_hll_set_wide_split)
+  double *wpart;
+  unsigned *wticket;
+  const int *wcbase;
 };
 
 struct HllViewF {  // FP32 values, FP32 x
@@ -535,7 +546,9 @@ __device__ __forceinline__ double row_dot(const Hll32WView &A, int s, const doub
   // long-row kernel launched just before with the same x
   if (((ld_ro(A.hkoffs + (s >> 5) + 1) - h0) >> 5) > A.longW) return __ldcg(A.lres + s);
   const int off = h0 + (s & 31);
-  return row_acc<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base);
+  // the narrow rows of a skewed matrix are mostly short: their last group of
+  // loads is issued at once (same sum, same bits)
+  return row_acc_p<double, double, 8, 32>(A.val + off, A.ja + off, 32, ld_ro(A.irn + s), x - A.base, A.base);
 }
 
 __device__ __forceinline__ double row_dot(const HllView &A, int s, const double *__restrict__ x) {

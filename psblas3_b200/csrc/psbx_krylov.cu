@@ -1478,10 +1478,10 @@ extern "C" int psbx_diag_prec_build(void *mat, int fmt, void *dinv) {
 // ---------------------------------------------------------------- driver
 #define KGRAPH_ITERS 8
 
-// 2 when the matrix has wide hacks, whose rows two kernels sum before each
-// product (psbx_long_rows); 0 otherwise.
+// The kernels that sum the wide hacks' rows before each product
+// (psbx_long_rows): 2 (ordered), 1 (split), 0 without wide hacks.
 template <class View> static inline int long_launch(const View &) { return 0; }
-static inline int long_launch(const Hll32WView &) { return 2; }
+static inline int long_launch(const Hll32WView &A) { return A.wideSplit ? 1 : 2; }
 
 // Replays a captured batch of iterations until running(status) is false,
 // with 1, 2, 4, then 8 replays between two reads of the status word: a long
@@ -1532,7 +1532,8 @@ static void key_hll(std::vector<uint64_t> &k, const HllView &v, uint64_t tag) {
                      (uint64_t)(uint32_t)v.rows, (uint64_t)(uint32_t)v.hksz, (uint64_t)(uint32_t)v.base,
                      (uint64_t)v.longHacks, (uint64_t)v.lres, (uint64_t)(uint32_t)v.nLong,
                      (uint64_t)(uint32_t)v.longW, (uint64_t)v.wideBase, (uint64_t)v.wchunk, (uint64_t)v.wprod,
-                     (uint64_t)(uint32_t)v.nWChunks});
+                     (uint64_t)(uint32_t)v.nWChunks, (uint64_t)(uint32_t)v.wideSplit, (uint64_t)v.wpart,
+                     (uint64_t)v.wticket, (uint64_t)v.wcbase});
 }
 static void key_view(std::vector<uint64_t> &k, const HllView &v) { key_hll(k, v, 0); }
 static void key_view(std::vector<uint64_t> &k, const Hll32View &v) { key_hll(k, v, 1); }

@@ -51,6 +51,10 @@ HllView hll_view(const HllDevice *m) {
   v.wchunk = wide ? m->wchunk : nullptr;
   v.wprod = wide ? m->wprod : nullptr;
   v.nWChunks = wide ? m->nWChunks : 0;
+  v.wideSplit = wide ? m->wideSplit : 0;
+  v.wpart = wide ? m->wpart : nullptr;
+  v.wticket = wide ? m->wticket : nullptr;
+  v.wcbase = wide ? m->wcbase : nullptr;
   return v;
 }
 
@@ -179,8 +183,80 @@ __global__ void __launch_bounds__(32 * WS_WARPS) k_hll_wsum(Hll32WView A, double
   if (s < A.rows) lres[s] = acc;
 }
 
+// Split mode (psbx_hll_set_wide_split): the product blocks of the ordered
+// path (WP_COLS columns of one wide hack each, every block at once), but
+// each block sums its products instead of storing them.  Warp w of the
+// block takes columns c0 + w + 8u (u < WP_COLS/8) of each of the hack's 32
+// rows (lane = row), all their loads in flight; the block adds its 8 warps'
+// sums in warp order into one partial per row; the last block of the hack
+// (ticket) adds the hack's partials in column order into the row sums.  No
+// product makes a round trip through memory and no row has a long serial
+// chain; the sum order is not the stored order, so the row sum agrees with
+// the sequential one to rounding (|dy_i| <= len_i u sum_j |a_ij x_j|).
+// Block b of the split wide-hack sum (256 threads).  True in warp 0 of the
+// hack's last block, which then holds the sum of row s (its lane's row) in t.
+__device__ __forceinline__ bool wide_split_chunk(const Hll32WView &A, const double *__restrict__ x, int b, double &t,
+                                                 int &s) {
+  __shared__ double red[8][32];
+  __shared__ bool last;
+  const int i = A.wchunk[2 * b], c0 = A.wchunk[2 * b + 1];
+  const int h = A.longHacks[i];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t off = (size_t)A.hkoffs[h] + lane;
+  s = h * 32 + lane;
+  const int len = s < A.rows ? A.irn[s] : 0;
+  const double *xb = x - A.base;
+  constexpr int PER = WP_COLS / 8;
+  int c[PER];
+  double v[PER], xv[PER];
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int j = c0 + w + 8 * u;
+    const bool ok = j < len;
+    c[u] = ok ? ld_stream(A.ja + off + (size_t)j * 32) : A.base;
+    v[u] = ok ? ld_stream(A.val + off + (size_t)j * 32) : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < PER; u++) xv[u] = c0 + w + 8 * u < len ? ld_ro(xb + c[u]) : 0.0;
+  double acc = 0.0;
+#pragma unroll
+  for (int u = 0; u < PER; u++)
+    if (c0 + w + 8 * u < len) acc = radd(acc, rmul(v[u], xv[u]));
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0) {
+    double r = red[0][lane];
+#pragma unroll
+    for (int k = 1; k < 8; k++) r = radd(r, red[k][lane]);
+    A.wpart[(size_t)b * 32 + lane] = r;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(A.wticket + i, 1u) == (unsigned)(A.wcbase[i + 1] - A.wcbase[i] - 1);
+  __syncthreads();
+  if (!last || w != 0) return false;
+  __threadfence();
+  t = 0.0;
+  for (int k = A.wcbase[i]; k < A.wcbase[i + 1]; k++) t = radd(t, __ldcg(A.wpart + (size_t)k * 32 + lane));
+  if (lane == 0) A.wticket[i] = 0;
+  return true;
+}
+
+__global__ void __launch_bounds__(256) k_hll_wide_split(Hll32WView A, const double *__restrict__ x,
+                                                        double *__restrict__ lres, const int *status) {
+  if (status && *((volatile const int *)status) != 0) return;
+  double t;
+  int s;
+  if (wide_split_chunk(A, x, blockIdx.x, t, s) && s < A.rows) lres[s] = t;
+}
+
 int psbx_long_rows32(const Hll32WView &A, const double *x, const int *status, cudaStream_t st) {
   if (A.nLong <= 0) return SPGPU_SUCCESS;
+  if (A.wideSplit) {
+    k_hll_wide_split<<<A.nWChunks, 256, 0, st>>>(A, x, const_cast<double *>(A.lres), status);
+    PSBX_LAUNCH_CK("k_hll_wide_split");
+    return SPGPU_SUCCESS;
+  }
   k_hll_wprod<<<A.nWChunks, 256, 0, st>>>(A, x, status);
   PSBX_LAUNCH_CK("k_hll_wprod");
   k_hll_wsum<<<(A.nLong + WS_WARPS - 1) / WS_WARPS, 32 * WS_WARPS, WS_SMEM, st>>>(A, const_cast<double *>(A.lres),
@@ -205,11 +281,17 @@ int psbx_hll_index_long(HllDevice *m) {
   cudaFree(m->wideBase);
   cudaFree(m->wchunk);
   cudaFree(m->wprod);
+  cudaFree(m->wpart);
+  cudaFree(m->wticket);
+  cudaFree(m->wcbase);
   m->longHacks = nullptr;
   m->lres = nullptr;
   m->wideBase = nullptr;
   m->wchunk = nullptr;
   m->wprod = nullptr;
+  m->wpart = nullptr;
+  m->wticket = nullptr;
+  m->wcbase = nullptr;
   m->nLong = 0;
   m->nWChunks = 0;
   if (m->hackSize != 32 || m->rows <= 0 || !m->hackOffs || m->longW < 0) return SPGPU_SUCCESS;
@@ -229,7 +311,7 @@ int psbx_hll_index_long(HllDevice *m) {
   for (int h = 0; h < nh; h++)
     if (((hk[h + 1] - hk[h]) >> 5) > lw) list.push_back(h);
   std::stable_sort(list.begin(), list.end(), [&](int a, int b) { return hk[a + 1] - hk[a] > hk[b + 1] - hk[b]; });
-  std::vector<int> wide, base(1, 0), chunks;
+  std::vector<int> wide, base(1, 0), chunks, cbase(1, 0);
   for (int h : list) {
     const int w = (hk[h + 1] - hk[h]) >> 5;
     for (int c0 = 0; c0 < w; c0 += WP_COLS) {
@@ -238,6 +320,7 @@ int psbx_hll_index_long(HllDevice *m) {
     }
     wide.push_back(h);
     base.push_back(base.back() + w * 32);
+    cbase.push_back((int)(chunks.size() / 2));
   }
   if (wide.empty()) return SPGPU_SUCCESS;
   PSBX_CK(cudaMalloc(&m->longHacks, sizeof(int) * wide.size()));
@@ -245,6 +328,11 @@ int psbx_hll_index_long(HllDevice *m) {
   PSBX_CK(cudaMalloc(&m->wideBase, sizeof(int) * base.size()));
   PSBX_CK(cudaMalloc(&m->wchunk, sizeof(int) * chunks.size()));
   PSBX_CK(cudaMalloc(&m->wprod, sizeof(double) * (size_t)base.back()));
+  PSBX_CK(cudaMalloc(&m->wpart, sizeof(double) * 32 * (chunks.size() / 2)));
+  PSBX_CK(cudaMalloc(&m->wticket, sizeof(unsigned) * wide.size()));
+  PSBX_CK(cudaMalloc(&m->wcbase, sizeof(int) * cbase.size()));
+  PSBX_CK(cudaMemsetAsync(m->wticket, 0, sizeof(unsigned) * wide.size(), c.stream));
+  PSBX_CK(cudaMemcpyAsync(m->wcbase, cbase.data(), sizeof(int) * cbase.size(), cudaMemcpyHostToDevice, c.stream));
   PSBX_CK(cudaMemcpyAsync(m->longHacks, wide.data(), sizeof(int) * wide.size(), cudaMemcpyHostToDevice, c.stream));
   PSBX_CK(cudaMemcpyAsync(m->wideBase, base.data(), sizeof(int) * base.size(), cudaMemcpyHostToDevice, c.stream));
   PSBX_CK(cudaMemcpyAsync(m->wchunk, chunks.data(), sizeof(int) * chunks.size(), cudaMemcpyHostToDevice, c.stream));
@@ -300,6 +388,210 @@ __global__ void __launch_bounds__(SPMV_T) k_hll_spmv_f32(HllViewF A, float alpha
   y[r] = MODE == 1 ? t : raddf(t, rmulf(beta, y[r]));
 }
 
+// Skewed matrices (hack size 32 with wide hacks: a row-sorted power-law
+// matrix) are mostly rows of 1-4 entries, for which one row per thread is a
+// chain of dependent round trips with little in flight.  Here a thread
+// takes R adjacent rows of a hack -- entry j of two of them is one double2
+// (values) and one int2 (indices), so a warp load moves 512 bytes -- and
+// each row still adds its own entries in stored order (the same bits as
+// k_spmv_rows).
+#ifndef PSBX_HLL_R
+#define PSBX_HLL_R 2
+#endif
+#ifndef PSBX_HLL_U
+#define PSBX_HLL_U 4
+#endif
+template <int U, int R>
+__device__ __forceinline__ void rgroup64(const HllView &A, int off, const int (&len)[R],
+                                         const double *__restrict__ x, double (&acc)[R]) {
+  static_assert(R % 2 == 0 && 32 % R == 0, "R adjacent rows of one hack, in pairs");
+  const double *vp = A.val + off;
+  const int *jp = A.ja + off;
+  const double *xb = x - A.base;
+  int n = 0;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    n = max(n, len[r]);
+    acc[r] = 0.0;
+  }
+  for (int j = 0; j < n; j += U) {
+    int2 c[U][R / 2];
+    double2 v[U][R / 2];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int q = 0; q < R / 2; q++) {
+        const bool ok = j + u < n;
+        c[u][q] = ok ? ld_stream((const int2 *)(jp + (j + u) * 32 + 2 * q)) : make_int2(A.base, A.base);
+        v[u][q] = ok ? ld_stream((const double2 *)(vp + (j + u) * 32 + 2 * q)) : make_double2(0.0, 0.0);
+      }
+    double xv[U][R];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int q = 0; q < R / 2; q++) {
+        xv[u][2 * q] = j + u < len[2 * q] ? ld_ro(xb + c[u][q].x) : 0.0;
+        xv[u][2 * q + 1] = j + u < len[2 * q + 1] ? ld_ro(xb + c[u][q].y) : 0.0;
+      }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int q = 0; q < R / 2; q++) {
+        if (j + u < len[2 * q]) acc[2 * q] = radd(acc[2 * q], rmul(v[u][q].x, xv[u][2 * q]));
+        if (j + u < len[2 * q + 1]) acc[2 * q + 1] = radd(acc[2 * q + 1], rmul(v[u][q].y, xv[u][2 * q + 1]));
+      }
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void put_row(int i, double alpha, double a, double beta, double *y) {
+  const double t = rmul(alpha, a);
+  y[i] = MODE == 1 ? t : radd(t, rmul(beta, y[i]));
+}
+
+// Rows of the narrow hacks, R per thread, from block `first` on; the rows
+// of wide hacks come from lres (SPLIT 0) or are written by the wide blocks
+// 0 .. first-1 of the same launch (SPLIT 1), which run the split sum and
+// store y themselves: the long rows then overlap the short ones instead of
+// running before them.
+template <int MODE, int SPLIT>
+__global__ void __launch_bounds__(SPMV_T) k_hll_rgroup(Hll32WView A, double alpha, const double *__restrict__ x,
+                                                       double beta, double *__restrict__ y) {
+  constexpr int R = PSBX_HLL_R;
+  const int first = SPLIT ? A.nWChunks : 0;
+  if (SPLIT && (int)blockIdx.x < first) {
+    double t;
+    int s;
+    if (wide_split_chunk(A, x, blockIdx.x, t, s) && s < A.rows)
+      put_row<MODE>(A.perm ? ld_ro(A.perm + s) : s, alpha, t, beta, y);
+    return;
+  }
+  const int s0 = R * ((blockIdx.x - first) * SPMV_T + threadIdx.x);
+  if (s0 >= A.rows) return;
+  // the destinations are read with the offsets, not after the sums: one
+  // round trip less per thread
+  int dst[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) dst[r] = A.perm && s0 + r < A.rows ? ld_ro(A.perm + s0 + r) : s0 + r;
+  const int h0 = ld_ro(A.hkoffs + (s0 >> 5));
+  double a[R];
+  if (A.nLong > 0 && ((ld_ro(A.hkoffs + (s0 >> 5) + 1) - h0) >> 5) > A.longW) {
+    if constexpr (SPLIT) {
+      return;
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; r++) a[r] = s0 + r < A.rows ? __ldcg(A.lres + s0 + r) : 0.0;
+    }
+  } else {
+    int len[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) len[r] = s0 + r < A.rows ? ld_ro(A.irn + s0 + r) : 0;
+    rgroup64<PSBX_HLL_U, R>(A, h0 + (s0 & 31), len, x, a);
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++)
+    if (s0 + r < A.rows) put_row<MODE>(dst[r], alpha, a[r], beta, y);
+}
+
+// Two threads per row (the reference's two-thread HLL mode): lanes 2k and
+// 2k+1 take the entries of row s at even and at odd positions, each adding
+// its own in stored order, and the row sum is (even sum) + (odd sum) -- the
+// tolerance mode only (|dy_i| <= len_i u sum_j |a_ij x_j|).  A warp holds 16
+// rows of one hack, so the wide-hack test is the same for the whole warp.
+template <int MODE, int SPLIT>
+__global__ void __launch_bounds__(SPMV_T) k_hll_tpr2(Hll32WView A, double alpha, const double *__restrict__ x,
+                                                     double beta, double *__restrict__ y) {
+  const int first = SPLIT ? A.nWChunks : 0;
+  if (SPLIT && (int)blockIdx.x < first) {
+    double t;
+    int s;
+    if (wide_split_chunk(A, x, blockIdx.x, t, s) && s < A.rows)
+      put_row<MODE>(A.perm ? ld_ro(A.perm + s) : s, alpha, t, beta, y);
+    return;
+  }
+  const int g = (blockIdx.x - first) * SPMV_T + threadIdx.x;
+  const int s = g >> 1, p = g & 1;
+  if ((s & ~15) >= A.rows) return;  // the whole warp is past the last row
+  const bool ok = s < A.rows;
+  const int h0 = ld_ro(A.hkoffs + (s >> 5));
+  const int dst = ok && p == 0 ? (A.perm ? ld_ro(A.perm + s) : s) : 0;
+  if (A.nLong > 0 && ((ld_ro(A.hkoffs + (s >> 5) + 1) - h0) >> 5) > A.longW) {
+    if constexpr (!SPLIT) {
+      if (ok && p == 0) put_row<MODE>(dst, alpha, __ldcg(A.lres + s), beta, y);
+    }
+    return;
+  }
+  const int len = ok ? ld_ro(A.irn + s) : 0;
+  const size_t off = (size_t)h0 + (s & 31);
+  const double *xb = x - A.base;
+  constexpr int U = 4;
+  double acc = 0.0;
+  for (int j = p; j < len; j += 2 * U) {
+    int c[U];
+    double v[U], xv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const bool in = j + 2 * u < len;
+      c[u] = in ? ld_stream(A.ja + off + (size_t)(j + 2 * u) * 32) : A.base;
+      v[u] = in ? ld_stream(A.val + off + (size_t)(j + 2 * u) * 32) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) xv[u] = j + 2 * u < len ? ld_ro(xb + c[u]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (j + 2 * u < len) acc = radd(acc, rmul(v[u], xv[u]));
+  }
+  const double odd = __shfl_xor_sync(0xffffffffu, acc, 1);
+  if (ok && p == 0) put_row<MODE>(dst, alpha, radd(acc, odd), beta, y);
+}
+
+static int launch_tpr2(const Hll32WView &A, double alpha, const double *x, double beta, double *y,
+                       cudaStream_t st) {
+  if (A.rows <= 0) return SPGPU_SUCCESS;
+  if (alpha == 0.0) return psbx_launch_scale(A.rows, beta, y, st);
+  const int g = (int)(((long long)A.rows * 2 + SPMV_T - 1) / SPMV_T);
+  if (A.nLong > 0 && A.wideSplit) {
+    if (beta == 0.0)
+      k_hll_tpr2<1, 1><<<A.nWChunks + g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+    else
+      k_hll_tpr2<0, 1><<<A.nWChunks + g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+    PSBX_LAUNCH_CK("k_hll_tpr2");
+    return SPGPU_SUCCESS;
+  }
+  int rc = psbx_long_rows32(A, x, nullptr, st);
+  if (rc) return rc;
+  if (beta == 0.0)
+    k_hll_tpr2<1, 0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  else
+    k_hll_tpr2<0, 0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  PSBX_LAUNCH_CK("k_hll_tpr2");
+  return SPGPU_SUCCESS;
+}
+
+static int launch_rgroup(const Hll32WView &A, double alpha, const double *x, double beta, double *y,
+                         cudaStream_t st) {
+  static_assert(SPMV_T == 256, "the wide blocks of k_hll_rgroup run 256 threads");
+  if (A.rows <= 0) return SPGPU_SUCCESS;
+  if (alpha == 0.0) return psbx_launch_scale(A.rows, beta, y, st);
+  const int g = ((A.rows + PSBX_HLL_R - 1) / PSBX_HLL_R + SPMV_T - 1) / SPMV_T;
+  if (A.nLong > 0 && A.wideSplit) {
+    if (beta == 0.0)
+      k_hll_rgroup<1, 1><<<A.nWChunks + g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+    else
+      k_hll_rgroup<0, 1><<<A.nWChunks + g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+    PSBX_LAUNCH_CK("k_hll_rgroup");
+    return SPGPU_SUCCESS;
+  }
+  int rc = psbx_long_rows32(A, x, nullptr, st);
+  if (rc) return rc;
+  if (beta == 0.0)
+    k_hll_rgroup<1, 0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  else
+    k_hll_rgroup<0, 0><<<g, SPMV_T, 0, st>>>(A, alpha, x, beta, y);
+  PSBX_LAUNCH_CK("k_hll_rgroup");
+  return SPGPU_SUCCESS;
+}
+
 template <class View>
 static int launch_rows(const View &A, double alpha, const double *x, double beta, double *y, cudaStream_t st) {
   if (A.rows <= 0) return SPGPU_SUCCESS;
@@ -320,7 +612,12 @@ int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, doub
   if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
   if (alpha == 0.0 && m->perm == nullptr) return psbx_launch_scale(m->rows, beta, y, st);
   if (m->hackSize == 32) {
+    // row mapping: two threads per row only in the tolerance mode; two rows
+    // per thread by default when there are wide hacks (skewed rows)
     const HllView v = hll_view(m);
+    if (m->tpr == 2 && m->wideSplit) return launch_tpr2(hll32w_view(v), alpha, x, beta, y, st);
+    if (m->tpr == -2 || m->tpr == 2 || (m->tpr == 0 && v.nLong > 0))
+      return launch_rgroup(hll32w_view(v), alpha, x, beta, y, st);
     if (v.nLong > 0) return launch_rows(hll32w_view(v), alpha, x, beta, y, st);
     if (hll_short_rows(m)) return launch_rows(hll32s_view(v), alpha, x, beta, y, st);
     return launch_rows(hll32_view(v), alpha, x, beta, y, st);

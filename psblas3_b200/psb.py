@@ -180,8 +180,9 @@ class HllMat:
     @classmethod
     def autotune_from_csr_device(cls, rows, cols, nnz, d_irp, d_ja, d_val, d_perm=None):
         """Device CSR (raw device pointers, 1-based) -> the HLL layout with the
-        fastest SpMV among hack sizes 32/64/128 and wide-hack thresholds;
-        returns (HllMat, {"hksz", "wide_w", "ms"})."""
+        fastest SpMV among hack sizes 32/64/128, wide-hack thresholds and
+        threads per row; returns (HllMat, {"hksz", "wide_w", "tpr", "ms"}),
+        the matrix in the tolerance mode."""
         h = C.c_void_p()
         hk, ww, ms = C.c_int(0), C.c_int(0), C.c_double(0.0)
         check(lib.psbx_hll_autotune_from_csr_device(C.byref(h), rows, cols, nnz, C.c_void_p(d_irp),
@@ -189,13 +190,34 @@ class HllMat:
                                                     None if d_perm is None else C.c_void_p(d_perm),
                                                     C.byref(hk), C.byref(ww), C.byref(ms)),
               "psbx_hll_autotune_from_csr_device")
-        return cls(h, rows), {"hksz": hk.value, "wide_w": ww.value, "ms": ms.value}
+        mat = cls(h, rows)
+        return mat, {"hksz": hk.value, "wide_w": ww.value, "tpr": mat.layout()["tpr"], "ms": ms.value}
 
     def set_wide(self, wide_w):
-        """Wide-hack threshold (hack size 32): 0 default, < 0 never; the same
-        bits for every choice."""
+        """Wide-hack threshold (hack size 32): 0 default, < 0 never; in the
+        exact mode the same bits for every choice."""
         check(lib.psbx_hll_set_wide(self.h, int(wide_w)), "psbx_hll_set_wide")
         return self
+
+    def set_wide_split(self, split=True):
+        """Tolerance mode (True, the default: wide hacks summed split over 8
+        warps, two threads per row allowed; every row within 1e-13 of
+        (|A||x|)_i) or exact mode (False: every row in stored order, the CPU
+        csmv's bits)."""
+        check(lib.psbx_hll_set_wide_split(self.h, int(bool(split))), "psbx_hll_set_wide_split")
+        return self
+
+    def set_threads_per_row(self, tpr):
+        """Row mapping of the standalone SpMV (hack size 32): 0 auto, 1 or 2
+        threads per row (2: tolerance mode only), -2 two rows per thread."""
+        check(lib.psbx_hll_set_threads_per_row(self.h, int(tpr)), "psbx_hll_set_threads_per_row")
+        return self
+
+    def layout(self):
+        hk, ww, sp, tp = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        check(lib.psbx_hll_get_layout(self.h, C.byref(hk), C.byref(ww), C.byref(sp), C.byref(tp)),
+              "psbx_hll_get_layout")
+        return {"hksz": hk.value, "wide_w": ww.value, "split": sp.value, "tpr": tp.value}
 
     def params(self):
         v = [C.c_int() for _ in range(7)]

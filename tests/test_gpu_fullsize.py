@@ -116,18 +116,35 @@ def test_c2b_full_size_powerlaw(psb):
     d = _dev_csr(irp, ja, va)
     H = psb.HllMat.from_csr_device(n, n, nnz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
     psb.psb_spmm(1.0, H, X, 0.0, Y)
-    assert np.array_equal(Y.get_vect(), ref), "HLL as stored"
+    assert np.all(np.abs(Y.get_vect() - ref) <= TOL * scale), "HLL as stored, tolerance mode"
+    H.set_wide_split(False)
+    psb.psb_spmm(1.0, H, X, 0.0, Y)
+    assert np.array_equal(Y.get_vect(), ref), "HLL as stored, exact mode"
     H.free()
     order = torch.from_numpy(np.argsort(-lens, kind="stable").astype(np.int32)).cuda()
     H = psb.HllMat.from_csr_device(n, n, nnz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32,
                                    order.data_ptr())
+    H.set_wide_split(False)
     psb.psb_spmm(1.0, H, X, 0.0, Y)
     assert np.array_equal(Y.get_vect(), ref), "HLL rows in length order"
+    # tolerance mode (the default): wide hacks summed in chunks by all SMs, same launch
+    H.set_wide_split(True)
+    psb.psb_spmm(1.0, H, X, 0.0, Y)
+    got = Y.get_vect()
+    assert np.all(np.abs(got - ref) <= TOL * scale), "split wide hacks"
+    # rows of hacks at most 64 wide (below any wide threshold) keep the stored order
+    slen = lens[order.cpu().numpy()]
+    width = np.repeat(np.maximum.reduceat(slen, np.arange(0, n, 32)), 32)[:n]
+    narrow = order.cpu().numpy()[width <= 64]
+    assert np.array_equal(got[narrow], ref[narrow])
     H.free()
     T, info = psb.HllMat.autotune_from_csr_device(n, n, nnz, d[0].data_ptr(), d[1].data_ptr(),
                                                   d[2].data_ptr(), order.data_ptr())
     psb.psb_spmm(1.0, T, X, 0.0, Y)
-    assert np.array_equal(Y.get_vect(), ref), ("autotuned", info)
+    assert np.all(np.abs(Y.get_vect() - ref) <= TOL * scale), ("autotuned", info)
+    T.set_wide_split(False)
+    psb.psb_spmm(1.0, T, X, 0.0, Y)
+    assert np.array_equal(Y.get_vect(), ref), ("autotuned, exact mode", info)
     T.free()
 
 

@@ -358,11 +358,12 @@ def test_distributed_parts_on_device(psb):
 
 @pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0), (2.5, -0.5)])
 def test_hll_wide_hacks_bitexact(psb, alpha, beta):
-    """Row-sorted power-law matrix (rows up to 4,000 entries at the front):
-    the products of the wide hacks are formed by all blocks and each row's
-    products added in entry order by a warp per hack, so the HLL SpMV stays
-    bit-identical to the CPU csmv; host-written, device-built and permuted
-    (perm = the length order) layouts alike."""
+    """Exact mode on a row-sorted power-law matrix (rows up to 4,000 entries
+    at the front): the products of the wide hacks are formed by all blocks
+    and each row's products added in entry order by a warp per hack, so the
+    HLL SpMV stays bit-identical to the CPU csmv for every row mapping;
+    host-written, device-built and permuted (perm = the length order)
+    layouts alike."""
     import torch
     irp, ja, va = gen.powerlaw(60000, kmax=4000, seed=21)
     sirp, sja, sva, order = gen.sort_rows_by_length(irp, ja, va)
@@ -376,23 +377,122 @@ def test_hll_wide_hacks_bitexact(psb, alpha, beta):
     mats.append(psb.HllMat.from_csr_device(n, n, len(sja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32))
     want = O.csr_csmv(sirp, sja, sva, alpha, x, beta, y0)
     for A in mats:
-        X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
-        A.spmv(alpha, X, beta, Y)
-        assert np.array_equal(Y.get_vect(), want)
+        A.set_wide_split(False)  # exact mode
+        for tpr in (0, 1, -2, 2):  # two threads per row falls back to the stored order here
+            A.set_threads_per_row(tpr)
+            X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+            A.spmv(alpha, X, beta, Y)
+            assert np.array_equal(Y.get_vect(), want), tpr
     # the unsorted matrix stored in length order through a permutation
     e = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
     d_perm = torch.from_numpy(np.ascontiguousarray(order, dtype=np.int32)).cuda()
     P = psb.HllMat.from_csr_device(n, n, len(ja), e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(), 32,
                                    d_perm.data_ptr())
+    P.set_wide_split(False)
     X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
     P.spmv(alpha, X, beta, Y)
     assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, alpha, x, beta, y0))
 
 
+@pytest.mark.parametrize("wide", [0, 1, 33, 200])
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.5, 0.5)])
+def test_hll_wide_split_tolerance(psb, wide, alpha, beta):
+    """Tolerance mode (the default): each wide hack is summed
+    in 64-column chunks by all SMs, in the launch of the other rows; every
+    row agrees with the CPU csmv within 1e-13 (|A||x| + |beta y|)_i, also
+    on a second call (the per-hack tickets reset); host-built, device-built and permuted
+    layouts; the CG over the same matrix converges as in the stored-order
+    mode (iterations within 2)."""
+    import torch
+    irp, ja, va = gen.powerlaw(60000, kmax=4000, seed=21)
+    sirp, sja, sva, order = gen.sort_rows_by_length(irp, ja, va)
+    n = len(irp) - 1
+    rng = np.random.default_rng(14)
+    x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    h = _host_hll(sirp, sja, sva)
+    d = [torch.from_numpy(a).cuda() for a in (sirp, sja, sva)]
+    e = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+    d_perm = torch.from_numpy(np.ascontiguousarray(order, dtype=np.int32)).cuda()
+    cases = [
+        (psb.HllMat.from_host_hll(n, 32, h["irn"], h["hkoffs"], h["ja"], h["val"], h["idiag"]), (sirp, sja, sva)),
+        (psb.HllMat.from_csr_device(n, n, len(sja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32),
+         (sirp, sja, sva)),
+        (psb.HllMat.from_csr_device(n, n, len(ja), e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(), 32,
+                                    d_perm.data_ptr()), (irp, ja, va)),
+    ]
+    for A, (ri, rj, rv) in cases:
+        A.set_wide(wide)
+        assert A.layout()["split"] == 1  # the default
+        want = O.csr_csmv(ri, rj, rv, alpha, x, beta, y0)
+        scale = O.csr_csmv(ri, rj, np.abs(rv), abs(alpha), np.abs(x), abs(beta), np.abs(y0))
+        X = psb.DVect.bld(x)
+        for _ in range(2):  # a second call reuses the per-hack tickets
+            Y = psb.DVect.bld(y0)
+            A.spmv(alpha, X, beta, Y)
+            got = Y.get_vect()
+            assert np.all(np.abs(got - want) <= TOL * scale)
+        A.free()
+    sirp, sja, sva = gen.powerlaw_spd(20000, kmax=3000, seed=6)
+    sirp, sja, sva, _ = gen.sort_rows_by_length(sirp, sja, sva)
+    n = len(sirp) - 1
+    f = [torch.from_numpy(a).cuda() for a in (sirp, sja, sva)]
+    S = psb.HllMat.from_csr_device(n, n, len(sja), f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), 32)
+    S.set_wide(wide)
+    P = psb.DiagPrec("DIAG").build(S)
+    b = rng.uniform(-1, 1, n)
+    its = []
+    for split in (0, 1):
+        S.set_wide_split(split)
+        B, Xs = psb.DVect.bld(b), psb.DVect(n)
+        it, err = psb.psb_krylov("CG", S, P, B, Xs, eps=1e-10, itmax=1000)
+        assert err <= 1e-10
+        its.append(it)
+    assert abs(its[1] - its[0]) <= 2
+
+
+@pytest.mark.parametrize("tpr", [0, 1, 2, -2])
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.5, 0.5)])
+def test_hll_threads_per_row(psb, tpr, alpha, beta):
+    """Every row mapping of the standalone HLL SpMV (auto, one or two
+    threads per row, two rows per thread) on a stencil, a row-sorted
+    power-law matrix with wide hacks, and an odd row count: within 1e-13 of
+    the CPU csmv in the tolerance mode, its bits in the exact mode (two
+    threads per row then runs as two rows per thread)."""
+    import torch
+    mats = [gen.stencil27(13), gen.sort_rows_by_length(*gen.powerlaw(30007, kmax=3000, seed=9))[:3],
+            gen.powerlaw(1037, kmax=90, seed=2)]
+    for irp, ja, va in mats:
+        n = len(irp) - 1
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
+        A.set_threads_per_row(tpr)
+        assert A.layout()["tpr"] == tpr
+        rng = np.random.default_rng(n)
+        x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+        want = O.csr_csmv(irp, ja, va, alpha, x, beta, y0)
+        scale = O.csr_csmv(irp, ja, np.abs(va), abs(alpha), np.abs(x), abs(beta), np.abs(y0))
+        X = psb.DVect.bld(x)
+        Y = psb.DVect.bld(y0)
+        A.spmv(alpha, X, beta, Y)
+        assert np.all(np.abs(Y.get_vect() - want) <= TOL * scale), (n, tpr)
+        A.set_wide_split(False)
+        Y = psb.DVect.bld(y0)
+        A.spmv(alpha, X, beta, Y)
+        assert np.array_equal(Y.get_vect(), want), (n, tpr)
+        A.free()
+    with pytest.raises(RuntimeError):
+        irp, ja, va = gen.stencil27(5)
+        n = len(irp) - 1
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                   64).set_threads_per_row(2)
+
+
 def test_hll_autotune(psb):
-    """The autotuned layout (hack size, wide-hack threshold) gives the same
-    bits as the CPU csmv for a stencil and a skewed row-sorted matrix, and
-    its choice lies in the candidate set."""
+    """The autotuned layout (hack size, wide-hack threshold, threads per
+    row) comes back in the tolerance mode, within 1e-13 of the CPU csmv, and
+    in the exact mode gives its bits, for a stencil and a skewed row-sorted
+    matrix; its choice lies in the candidate set."""
     import torch
     for irp, ja, va in (gen.stencil27(40), gen.sort_rows_by_length(*gen.powerlaw(80000, kmax=4000, seed=2))[:3]):
         n = len(irp) - 1
@@ -401,15 +501,22 @@ def test_hll_autotune(psb):
                                                      d[2].data_ptr())
         assert info["hksz"] in (32, 64, 128) and info["ms"] > 0
         assert info["wide_w"] in ((32, 64, 128, 256, 1024, -1) if info["hksz"] == 32 else (0,))
+        assert info["tpr"] in ((-2, 1, 2) if info["hksz"] == 32 else (0,))
+        assert A.layout()["split"] == 1
         x = np.random.default_rng(3).uniform(-1, 1, n)
         X, Y = psb.DVect.bld(x), psb.DVect(n)
         A.spmv(1.0, X, 0.0, Y)
-        assert np.array_equal(Y.get_vect(), O.csr_csmv(irp, ja, va, 1.0, x, 0.0, np.zeros(n))), info
+        want = O.csr_csmv(irp, ja, va, 1.0, x, 0.0, np.zeros(n))
+        scale = O.csr_csmv(irp, ja, np.abs(va), 1.0, np.abs(x), 0.0, np.zeros(n))
+        assert np.all(np.abs(Y.get_vect() - want) <= TOL * scale), info
+        A.set_wide_split(False)  # the exact mode: the same bits whatever the layout
+        A.spmv(1.0, X, 0.0, Y)
+        assert np.array_equal(Y.get_vect(), want), info
 
 
 @pytest.mark.parametrize("wide", [-1, 0, 1, 33, 64, 200])
 def test_hll_wide_threshold_same_bits(psb, wide):
-    """Every wide-hack threshold gives the CPU csmv's bits: 1 sends almost
+    """In the exact mode every wide-hack threshold gives the CPU csmv's bits: 1 sends almost
     every hack down the wide path (partial product blocks, partial ring
     chunks, rows ending inside a chunk), -1 none; an unsorted power-law
     matrix puts wide hacks between narrow ones."""
@@ -418,7 +525,7 @@ def test_hll_wide_threshold_same_bits(psb, wide):
     n = len(irp) - 1
     d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
     A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
-    A.set_wide(wide)
+    A.set_wide(wide).set_wide_split(False)
     rng = np.random.default_rng(8)
     x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
     X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
@@ -428,6 +535,7 @@ def test_hll_wide_threshold_same_bits(psb, wide):
     sirp, sja, sva = gen.powerlaw_spd(20000, kmax=3000, seed=6)
     e = [torch.from_numpy(a).cuda() for a in (sirp, sja, sva)]
     S = psb.HllMat.from_csr_device(n, n, len(sja), e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(), 32)
+    S.set_wide_split(False)
     P = psb.DiagPrec("DIAG").build(S)
     b = rng.uniform(-1, 1, n)
     runs = []
