@@ -603,6 +603,18 @@ def c2b_powerlaw(psb, gen, stream, steps=10):
            "csr": {"gb_s": B2 / ms / 1e6, "ms": ms}}
     y_csr = Y2.get_vect()
     Cm.free()
+    # the gather floor: the reads of x at this matrix's column indices alone
+    # (one L2 sector request each, columns being random), no values, no sums
+    import ctypes as C
+    from psblas3_b200._lib import check, lib
+    d_ja = torch.from_numpy(pj).cuda()
+    d_out = torch.empty((nnz2 + 7) // 8, dtype=torch.float64, device="cuda")
+    g_ms = C.c_double(0.0)
+    check(lib.psbx_probe_gather(C.c_void_p(d_ja.data_ptr()), nnz2, int(pi[0]), C.c_void_p(X2.data_ptr),
+                                C.c_void_p(d_out.data_ptr()), 10, C.byref(g_ms)), "psbx_probe_gather")
+    del d_ja, d_out
+    res["gather_floor"] = {"ms": g_ms.value, "gathers": nnz2, "g_per_s": nnz2 / g_ms.value / 1e6,
+                           "gb_s_at_floor": B2 / g_ms.value / 1e6}
     d_irp, d_ja, d_va = (torch.from_numpy(a).cuda() for a in (pi, pj, pv))
     H = psb.HllMat.from_csr_device(n2, n2, nnz2, d_irp.data_ptr(), d_ja.data_ptr(), d_va.data_ptr(), 32)
     del d_irp, d_ja, d_va
@@ -646,8 +658,10 @@ def c2b_powerlaw(psb, gen, stream, steps=10):
     del d_irp, d_ja, d_va, d_perm
     ms = _time_spmv(T, X2, Y2, steps, stream)
     yt = Y2.get_vect()
-    res["hll_row_sorted_autotuned"] = dict(info, gb_s=B2 / ms / 1e6, ms=ms,
-                                           within_1e-13=bool(np.all(np.abs(yt - yh) <= 1e-13 * scale)))
+    res["hll_row_sorted_autotuned"] = dict(info, gb_s=B2 / ms / 1e6, ms=ms)
+    res["hll_row_sorted_autotuned"]["within_1e-13"] = bool(np.all(np.abs(yt - yh) <= 1e-13 * scale))
+    for k in ("csr", "hll_row_sorted", "hll_row_sorted_split", "hll_row_sorted_autotuned"):
+        res[k]["frac_of_gather_floor"] = res["gather_floor"]["ms"] / res[k]["ms"]
     T.set_wide_split(False)
     T.spmv(1.0, X2, 0.0, Y2)
     res["hll_row_sorted_autotuned"]["exact_mode_bitexact_vs_unsorted_hll"] = bool(np.array_equal(Y2.get_vect(), yh))

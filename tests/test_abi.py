@@ -1,5 +1,5 @@
 """CPU checks of the drop-in boundary: libpsbx.so builds for sm_100a, loads
-without a GPU, and exports every entry point include/psbx.h declares (no
+without a GPU, and exports every entry point include/*.h declares (no
 compute call is made here)."""
 import os
 import re
@@ -8,11 +8,12 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "psbx.h")
+HEADERS = sorted(os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))
+                 if f.endswith(".h"))
 
 
 def declared_functions():
-    src = open(HEADER).read()
+    src = "\n".join(open(h).read() for h in HEADERS)
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     names = set()
     for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(", src, re.M):
@@ -115,3 +116,22 @@ def test_fortran_modules_link_against_library(libpath):
         if miss:
             missing[m] = miss
     assert not missing, missing
+
+
+def test_fortran_shim_matches_the_header(libpath):
+    """psbx_krylov_shim.F90 (the psb_krylov routing a maintainer compiles
+    with the PSBLAS modules; no Fortran compiler here): its bind(c) name is
+    exported and its options struct has psbx_SolverOptions' field order and
+    types."""
+    src = open(os.path.join(ROOT, "psbx_krylov_shim.F90")).read().lower()
+    names = re.findall(r"bind\(c,\s*name='(\w+)'\)", src)
+    assert names == ["psbx_dkrylov"]
+    assert "psbx_dkrylov" in declared_functions()
+    body = src[src.index("type, bind(c) :: psbx_solveroptions"):src.index("end type psbx_solveroptions")]
+    fort = [(t, f.strip()) for t, fs in re.findall(r"(integer\(c_int\)|real\(c_double\))\s*::\s*([\w, ]+)", body)
+            for f in fs.split(",")]
+    hdr = "\n".join(open(h).read() for h in HEADERS)
+    cbody = hdr[hdr.index("typedef struct psbx_SolverOptions"):hdr.index("} psbx_SolverOptions;")]
+    cfields = re.findall(r"^\s*(int|double)\s+(\w+);", cbody, re.M)
+    ctype = {"int": "integer(c_int)", "double": "real(c_double)"}
+    assert [(ctype[t], f.lower()) for t, f in cfields] == fort

@@ -549,3 +549,22 @@ def test_hll_wide_threshold_same_bits(psb, wide):
     assert runs[1][1] <= 1e-10
     r = O.csr_csmv(sirp, sja, sva, -1.0, runs[1][2], 1.0, b)
     assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b)
+
+
+def test_probe_gather(psb):
+    """The gather-floor probe (psbx_probe_gather) reads x at every index
+    pair (an odd last index skipped) and returns a positive time."""
+    import ctypes as C
+
+    import torch
+    from psblas3_b200._lib import check, lib
+    n = 1001
+    idx = np.random.default_rng(1).integers(1, 5001, n).astype(np.int32)
+    X = psb.DVect.bld(np.ones(5000))
+    d_idx = torch.from_numpy(idx).cuda()
+    out = torch.zeros((n + 7) // 8, dtype=torch.float64, device="cuda")
+    ms = C.c_double(0.0)
+    check(lib.psbx_probe_gather(C.c_void_p(d_idx.data_ptr()), n, 1, C.c_void_p(X.data_ptr),
+                                C.c_void_p(out.data_ptr()), 3, C.byref(ms)), "psbx_probe_gather")
+    assert ms.value > 0
+    assert out.sum().item() == 2 * (n // 2)  # every pair read once, x = 1
