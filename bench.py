@@ -140,6 +140,14 @@ def dist_setup():
     return world, rank, local
 
 
+def local_device(local):
+    """The GPU of a rank: its local rank, wrapped over the visible devices
+    (ranks beyond the device count share GPUs, as in a one-GPU check of the
+    sharded paths)."""
+    import torch
+    return local % max(1, torch.cuda.device_count())
+
+
 def dist_max(v, world):
     if world == 1:
         return v
@@ -154,6 +162,16 @@ def dist_barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def host_residual(irp, ja, va, x, b):
+    """||b - A x|| / ||b|| on the host (scipy CSR product) for the spot
+    checks of solver outputs; CSR arrays with base irp[0]."""
+    import scipy.sparse as sp
+    b0 = int(irp[0])
+    n = len(irp) - 1
+    A = sp.csr_matrix((va, np.asarray(ja) - b0, np.asarray(irp) - b0), shape=(n, n))
+    return float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
 
 
 def cpu_spmv_gbs(irp, ja, va, x, seconds=12.0, max_reps=30):
@@ -488,22 +506,33 @@ def c3_cg(psb, gen):
     return res
 
 
-def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
+def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32, world=1, rank=0):
     """C4: 512 SPD 2-D anisotropic systems -eps u_xx - u_yy on n x n grids
     (n uniform in [32, 256], eps log-uniform in [1e-2, 1]), 8 right-hand
     sides each (uniform [-1, 1]), solved to ||r|| <= 1e-10 ||b|| by the
-    batched mixed-precision engine; beside it the plain FP64 device CG one
-    solve at a time on a random sample of the same (system, rhs) pairs."""
+    batched mixed-precision engine; beside it the same systems through the
+    engine with FP64 inner iterations, and the plain FP64 device CG one
+    solve at a time on a random sample of the same (system, rhs) pairs.
+    Under torchrun the systems are split over the ranks by shard.assign
+    (work ~ rows; nothing crosses ranks on the data path), each rank solves
+    its share on its own GPU, and the times are the max over ranks."""
     import torch
-    import oracle as O
+    from psblas3_b200 import shard
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
     rng = np.random.default_rng(seed)
-    mats, keep, total = [], [], 0
-    for _ in range(n_sys):
-        m = int(rng.integers(32, 257))
-        eps = float(np.exp(rng.uniform(np.log(1e-2), 0.0)))
+    specs = [(int(rng.integers(32, 257)), float(np.exp(rng.uniform(np.log(1e-2), 0.0)))) for _ in range(n_sys)]
+    mine = shard.assign([m * m for m, _ in specs], world)[rank]
+    mats, total = [], 0
+    for i in mine:
+        m, eps = specs[i]
         irp, ja, va = gen.aniso2d(m, eps)
         n = len(irp) - 1
-        rhs = rng.uniform(-1, 1, (n, k))
+        rhs = np.random.default_rng((seed, i)).uniform(-1, 1, (n, k))
         d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
         A = psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32)
         A.make_single()
@@ -512,10 +541,12 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
         dx = torch.zeros_like(db)
         mats.append((irp, ja, va, rhs, A, P, db, dx))
         total += n
-    eng = psb.BatchSolver(n_sys, total, k)
+    nm = len(mats)
+    eng = psb.BatchSolver(nm, total, k)
     slots = [eng.add(A, db, dx, P.dv.data_ptr, eps=1e-10)
              for (_, _, _, _, A, P, db, dx) in mats]
     torch.cuda.synchronize()
+    barrier()
     l0 = psb.kernel_launches()
     t0 = time.perf_counter()
     eng.run(replays_per_step=4)
@@ -529,11 +560,12 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
         worst = max(worst, max(err))
     # the same systems through the engine with FP64 inner iterations: the
     # batched FP64 solve (batching without the FP32 inner iterations)
-    eng64 = psb.BatchSolver(n_sys, total, k, inner_fp64=True)
+    eng64 = psb.BatchSolver(nm, total, k, inner_fp64=True)
     xs64 = [torch.zeros_like(db) for (_, _, _, _, _, _, db, _) in mats]
     slots64 = [eng64.add(A, db, x64, P.dv.data_ptr, eps=1e-10)
                for (_, _, _, _, A, P, db, _), x64 in zip(mats, xs64)]
     torch.cuda.synchronize()
+    barrier()
     t0 = time.perf_counter()
     eng64.run(replays_per_step=4)
     tb64 = time.perf_counter() - t0
@@ -544,18 +576,18 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
         iters64.extend(its)
     eng64.free()
     del xs64
-    # FP64 check of a few solutions on the host (oracle CSR product)
+    # FP64 check of a few solutions on the host (scipy CSR product)
     checked = 0.0
-    for i in rng.choice(n_sys, 4, replace=False):
+    for i in rng.choice(nm, min(4, nm), replace=False):
         irp, ja, va, rhs, A, P, db, dx = mats[i]
         x = dx.cpu().numpy().reshape(-1, k)
         for j in range(k):
-            r = O.csr_csmv(irp, ja, va, -1.0, x[:, j], 1.0, rhs[:, j])
-            checked = max(checked, np.linalg.norm(r) / np.linalg.norm(rhs[:, j]))
+            checked = max(checked, host_residual(irp, ja, va, x[:, j], rhs[:, j]))
     eng.free()
-    # plain FP64 GPU path, one solve at a time, on a sample
-    t64, it64 = 0.0, []
-    pairs = [(int(i), int(j)) for i, j in zip(rng.integers(0, n_sys, fp64_sample), rng.integers(0, k, fp64_sample))]
+    # plain FP64 GPU path, one solve at a time, on a sample (rank 0's systems)
+    t64, it64, pairs = 0.0, [], []
+    if rank == 0:
+        pairs = [(int(i), int(j)) for i, j in zip(rng.integers(0, nm, fp64_sample), rng.integers(0, k, fp64_sample))]
     for i, j in pairs:
         irp, ja, va, rhs, A, P, db, dx = mats[i]
         B, X = psb.DVect.bld(rhs[:, j]), psb.DVect(len(irp) - 1)
@@ -569,18 +601,30 @@ def c4_batched(psb, gen, n_sys=512, k=8, seed=0, fp64_sample=32):
             best = dt if best is None else min(best, dt)
         t64 += best
         it64.append(it)
+    tb, tb64 = shard.max_over_ranks(tb, world), shard.max_over_ranks(tb64, world)
+    conv = int(shard.sum_over_ranks(sum(1 for s in states if s == 1), world))
+    conv64 = int(shard.sum_over_ranks(sum(1 for s in states64 if s == 1), world))
+    worst = shard.max_over_ranks(worst, world)
+    checked = shard.max_over_ranks(checked, world)
+    launches = int(shard.sum_over_ranks(launches, world))
+    total = int(shard.sum_over_ranks(total, world))
+    got = shard.gather_to_root((iters, iters64), world, rank)
+    if rank != 0:
+        return None
+    iters = [v for g in got for v in g[0]]
+    iters64 = [v for g in got for v in g[1]]
     solves = n_sys * k
-    return {"systems": n_sys, "rhs_per_system": k, "rows_total": total, "batched_s": tb,
-            "batched_solves_per_s": solves / tb, "converged": int(sum(1 for s in states if s == 1)),
+    return {"systems": n_sys, "rhs_per_system": k, "rows_total": total, "ranks": world, "batched_s": tb,
+            "batched_solves_per_s": solves / tb, "converged": conv,
             "fp64_batched_s": tb64, "fp64_batched_solves_per_s": solves / tb64,
-            "fp64_batched_converged": int(sum(1 for s in states64 if s == 1)),
+            "fp64_batched_converged": conv64,
             "fp64_batched_inner_iters_median": float(np.median(iters64)),
             "mixed_over_fp64_batched": tb64 / tb,
             "max_err": worst, "host_checked_max_relres": checked, "inner_iters_max": int(max(iters)),
-            "inner_iters_median": float(np.median(iters)), "kernel_launches": int(launches),
+            "inner_iters_median": float(np.median(iters)), "kernel_launches": launches,
             "fp64_one_at_a_time_solves_per_s": len(pairs) / t64, "fp64_sample": len(pairs),
             "fp64_iters_median": float(np.median(it64)),
-            "speedup_vs_fp64_one_at_a_time": (solves / tb) / (len(pairs) / t64)}
+            "speedup_vs_fp64_one_at_a_time": (solves / tb) / (len(pairs) / t64 * world)}
 
 
 def c2b_powerlaw(psb, gen, stream, steps=10):
@@ -699,7 +743,7 @@ def _c5_stream(rate, window, n_each, seed, keep_every=499):
 
 
 def c5_serving(psb, gen, rate=2000.0, window=60.0, pool_each=16, seed=0, replays_per_step=2, window_b=30.0,
-               fp64_seconds=15.0):
+               fp64_seconds=15.0, world=1, rank=0):
     """C5: Poisson arrivals of solve requests drawn 50/50 from 3-D 7-point
     Poisson grids (side uniform in [10, 128]) and power-law unstructured SPD
     matrices (rows log-uniform in [1e3, 2e6], alpha 2.1, diagonally dominant)
@@ -713,23 +757,39 @@ def c5_serving(psb, gen, rate=2000.0, window=60.0, pool_each=16, seed=0, replays
          latency there is service time, not backlog.
       FP64: the plain FP64 device CG serving the same streams one request at
          a time in arrival order, for fp64_seconds each: its capacity (stream
-         A) and its latency at the rate of B."""
+         A) and its latency at the rate of B.
+    Under torchrun the pool's matrices are split over the ranks by
+    shard.assign (work ~ rows); every rank draws the same global stream and
+    serves the requests for its own matrices on its own GPU (nothing crosses
+    ranks on the data path); counts are summed and latencies pooled at rank
+    0."""
     import concurrent.futures as cf
     import multiprocessing as mp
-    import oracle as O
-    from psblas3_b200 import serve
+    from psblas3_b200 import serve, shard
     rng = np.random.default_rng(seed)
     specs = [("poisson", int(rng.integers(10, 129)), 0) for _ in range(pool_each)]
     specs += [("powerlaw", int(np.exp(rng.uniform(np.log(1e3), np.log(2e6)))), int(rng.integers(1 << 30)))
               for _ in range(pool_each)]
+    mine = shard.assign([sz ** 3 if kind == "poisson" else sz for kind, sz, _ in specs], world)[rank]
+    local = {g: l for l, g in enumerate(mine)}
     t_gen = time.perf_counter()
-    with cf.ProcessPoolExecutor(max_workers=min(len(specs), os.cpu_count() or 1),
+    with cf.ProcessPoolExecutor(max_workers=min(len(mine), os.cpu_count() or 1),
                                 mp_context=mp.get_context("spawn")) as ex:
-        host = list(ex.map(_c5_matrix, specs))
+        host = list(ex.map(_c5_matrix, [specs[i] for i in mine]))
     t_gen = time.perf_counter() - t_gen
     pool = serve.Pool()
     for irp, ja, va in host:
         pool.add_csr(irp, ja, va)
+
+    def my_share(reqs):
+        return [serve.Request(r.rid, local[r.mat], r.seed, r.eps, r.t_arrive, keep=r.keep)
+                for r in reqs if r.mat in local]
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
     # warm-up: one small request through each path
     w = serve.Server(pool, hbm_budget=150e9, replays_per_step=replays_per_step)
     serve.run_stream(w, [serve.Request(0, 0, 1, 1e-10, 0.0)])
@@ -741,45 +801,66 @@ def c5_serving(psb, gen, rate=2000.0, window=60.0, pool_each=16, seed=0, replays
         for r in [q for q in done if q.keep and q.x is not None][:6]:
             irp, ja, va = host[r.mat]
             b = serve.request_rhs(r, pool.mats[r.mat]["n"]).cpu().numpy()
-            res = O.csr_csmv(irp, ja, va, -1.0, r.x, 1.0, b)
-            worst = max(worst, np.linalg.norm(res) / np.linalg.norm(b))
-        return worst
+            worst = max(worst, host_residual(irp, ja, va, r.x, b))
+        return shard.max_over_ranks(worst, world)
+
+    def pooled_latency(done):
+        lat = shard.gather_to_root([r.t_done - r.t_arrive for r in done], world, rank)
+        if rank != 0:
+            return {}
+        lat = np.array([v for g in lat for v in g])
+        if lat.size == 0:
+            return {}
+        return {"count": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3)}
 
     def served(rate_, window_, seed_, stop):
-        reqs = _c5_stream(rate_, window_, pool_each, seed_)
+        allreqs = _c5_stream(rate_, window_, pool_each, seed_)
+        reqs = my_share(allreqs)
         srv = serve.Server(pool, hbm_budget=150e9, replays_per_step=replays_per_step)
+        barrier()
         l0 = psb.kernel_launches()
         wall, left = serve.run_stream(srv, reqs, stop_at=window_ if stop else None)
         done = srv.done
         srv.close()
+        wall = shard.max_over_ranks(wall, world)
         span = window_ if stop else wall
-        return {"arrival_rate_per_s": rate_, "window_s": window_, "requests": len(reqs),
-                "completed": len(done), "unfinished_at_window_end": len(left) if stop else 0,
-                "converged": sum(1 for r in done if r.state == 1), "wall_s": wall,
-                "solves_per_s": len(done) / span, "latency": serve.latency_stats(done),
-                "host_checked_max_relres": check(done), "kernel_launches": int(psb.kernel_launches() - l0)}
+        completed = int(shard.sum_over_ranks(len(done), world))
+        return {"arrival_rate_per_s": rate_, "window_s": window_, "requests": len(allreqs),
+                "completed": completed,
+                "unfinished_at_window_end": int(shard.sum_over_ranks(len(left) if stop else 0, world)),
+                "converged": int(shard.sum_over_ranks(sum(1 for r in done if r.state == 1), world)),
+                "wall_s": wall, "solves_per_s": completed / span, "latency": pooled_latency(done),
+                "host_checked_max_relres": check(done),
+                "kernel_launches": int(shard.sum_over_ranks(psb.kernel_launches() - l0, world))}
 
-    out = {"pool_matrices": len(pool.mats), "pool_rows": [m["n"] for m in pool.mats],
+    out = {"pool_matrices": len(specs), "pool_rows": [m["n"] for m in pool.mats], "ranks": world,
            "pool_generation_s": t_gen, "request_mix": "50/50 Poisson / power-law, uniform over the pool's matrices"}
     a = served(rate, window, seed + 1, stop=True)
     out["A_stated_stream"] = a
     cap = a["solves_per_s"]
     b = served(0.8 * cap, window_b, seed + 2, stop=False)
     out["B_0p8_capacity"] = b
-    # the plain FP64 path on the same streams, one request at a time
-    fa_wall, fa = serve.serve_fp64(pool, _c5_stream(rate, window, pool_each, seed + 1), fp64_seconds)
-    fb_wall, fb = serve.serve_fp64(pool, _c5_stream(0.8 * cap, window_b, pool_each, seed + 2), fp64_seconds)
+    # the plain FP64 path on the same streams, one request at a time per GPU
+    barrier()
+    fa_wall, fa = serve.serve_fp64(pool, my_share(_c5_stream(rate, window, pool_each, seed + 1)), fp64_seconds)
+    fb_wall, fb = serve.serve_fp64(pool, my_share(_c5_stream(0.8 * cap, window_b, pool_each, seed + 2)),
+                                   fp64_seconds)
+    fa_rate = shard.sum_over_ranks(len(fa) / fa_wall if fa_wall > 0 else 0.0, world)
+    fb_rate = shard.sum_over_ranks(len(fb) / fb_wall if fb_wall > 0 else 0.0, world)
     out["fp64_one_at_a_time"] = {
         "method": "the same arrival streams served one request at a time in arrival order (psb_krylov CG, DIAG)",
-        "A_completed": len(fa), "A_solves_per_s": len(fa) / fa_wall, "A_seconds": fa_wall,
-        "A_converged": sum(1 for r in fa if r.state == 1),
-        "B_completed": len(fb), "B_solves_per_s": len(fb) / fb_wall, "B_seconds": fb_wall,
-        "B_latency": serve.latency_stats(fb), "host_checked_max_relres": check(fa + fb)}
-    out["speedup_vs_fp64_A"] = cap / out["fp64_one_at_a_time"]["A_solves_per_s"]
-    out["speedup_vs_fp64_B"] = b["solves_per_s"] / out["fp64_one_at_a_time"]["B_solves_per_s"]
+        "A_completed": int(shard.sum_over_ranks(len(fa), world)), "A_solves_per_s": fa_rate,
+        "A_seconds": shard.max_over_ranks(fa_wall, world),
+        "A_converged": int(shard.sum_over_ranks(sum(1 for r in fa if r.state == 1), world)),
+        "B_completed": int(shard.sum_over_ranks(len(fb), world)), "B_solves_per_s": fb_rate,
+        "B_seconds": shard.max_over_ranks(fb_wall, world),
+        "B_latency": pooled_latency(fb), "host_checked_max_relres": check(fa + fb)}
+    out["speedup_vs_fp64_A"] = cap / fa_rate
+    out["speedup_vs_fp64_B"] = b["solves_per_s"] / fb_rate
     for m in pool.mats:
         m["A"].free()
-    return out
+    return out if rank == 0 else None
 
 
 def run_ours(args):
@@ -901,18 +982,31 @@ def main():
 
 def run_only(name):
     """One secondary workload by itself (C2b power-law SpMV, C3 CG solves,
-    C4 batched, C5 serving) on cuda:0; prints {"only": name, "result": {...}}."""
+    C4 batched, C5 serving); prints {"only": name, "result": {...}} at rank
+    0.  Under torchrun C4 and C5 are sharded over the ranks (shard.assign:
+    independent systems, one GPU each); C2b and C3 run on rank 0's GPU."""
+    world, rank, local = dist_setup()
     import torch
     from psblas3_b200 import gen, psb
-    psb.init(0)
-    torch.cuda.set_device(0)
-    if name == "c2b":
-        from psblas3_b200._lib import lib
-        stream = torch.cuda.ExternalStream(lib.psb_cudaGetStream(), device="cuda:0")
-        res = c2b_powerlaw(psb, gen, stream)
-    else:
-        res = {"c3": c3_cg, "c4": c4_batched, "c5": c5_serving}[name](psb, gen)
-    print(json.dumps({"only": name, "result": res}), flush=True)
+    local = local_device(local)
+    torch.cuda.set_device(local)
+    psb.init(local)
+    res = None
+    if name in ("c4", "c5"):
+        res = {"c4": c4_batched, "c5": c5_serving}[name](psb, gen, world=world, rank=rank)
+    elif rank == 0:
+        if name == "c2b":
+            from psblas3_b200._lib import lib
+            stream = torch.cuda.ExternalStream(lib.psb_cudaGetStream(), device=f"cuda:{local}")
+            res = c2b_powerlaw(psb, gen, stream)
+        else:
+            res = c3_cg(psb, gen)
+    if rank == 0:
+        print(json.dumps({"only": name, "n_gpus": world, "result": res}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

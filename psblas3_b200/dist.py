@@ -28,7 +28,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 __all__ = ["partition_rows", "LocalPart", "local_part", "ExchangePlan", "exchange_plan",
-           "build_part_on_rank", "halo_exchange", "DistSpMV"]
+           "build_part_on_rank", "halo_exchange", "DistSpMV", "allreduce_sum", "dist_cg", "DeviceCGOps"]
 
 
 def partition_rows(n, world):
@@ -226,3 +226,106 @@ class DistSpMV:
         if self.And is not None:
             self.scatter(x)
             self.And.spmv(alpha, x, 1.0, y)
+
+
+# ------------------------------------------------------------ distributed CG
+def allreduce_sum(vals):
+    """The sums over ranks of a few scalars in ONE all_reduce (psb_sum of
+    base/psblas/psb_ddot.f90:150, for several dots at once): a CPU tensor
+    under gloo, a CUDA tensor under NCCL.  Identity on one rank."""
+    import torch
+    import torch.distributed as dist
+    vals = [float(v) for v in vals]
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return vals
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    dist.all_reduce(t)
+    return t.tolist()
+
+
+def dist_cg(ops, b, x, eps=1e-6, itmax=1000, istop=2, allreduce=allreduce_sum):
+    """psb_dcg (krylov/psb_dcg.F90:218-295, DIAG preconditioner) on a
+    row-block distribution; returns (iter, err) like psb_krylov.
+
+    `ops` holds this rank's rows: spmv(alpha, x, beta, y) is the distributed
+    product (halo exchange, then the local blocks), dot(u, v) the local part
+    of a dot product, axpby / copy / prec the local vector updates, new(ext)
+    a zero vector (ext: with room for the halo, for the vectors the product
+    reads: x and p).  b holds the owned entries, x the owned entries of x0 on
+    entry (room for the halo) and of the solution on exit.
+
+    Per iteration the reference takes three global reductions: rho = (r, z)
+    and sigma = (p, q) through psb_gedot and ||r|| through psb_genrm2 in
+    psb_check_conv.  Here z = D^-1 r is formed right after the update of r,
+    so ||r||^2 and the next rho travel in one all_reduce: two per iteration.
+    The stop test is the reference's (krylov/psb_d_krylov_conv_mod.f90:
+    127-202): istop 2, ||r|| <= eps ||b||; istop 3, ||r|| <= eps ||r0||;
+    err = ||r|| / ||b|| (or / ||r0||).  The sums over ranks change the
+    rounding of the dots, so iterations agree with the serial method to
+    within a step or two."""
+    import math
+    if istop not in (2, 3):
+        raise ValueError("dist_cg: istop 2 or 3")
+    r, z, q = ops.new(), ops.new(), ops.new()
+    p = ops.new(ext=True)
+    ops.copy(b, r)
+    ops.spmv(-1.0, x, 1.0, r)                       # r = b - A x0
+    ops.prec(r, z)                                  # z = D^-1 r
+    bb, rr, rho = allreduce([ops.dot(b, b), ops.dot(r, r), ops.dot(r, z)])
+    den = math.sqrt(bb) if istop == 2 else math.sqrt(rr)
+    it, err = 0, 0.0
+    rho_old = 0.0
+    while it < itmax:
+        it += 1
+        if it == 1:
+            ops.copy(z, p)
+        else:
+            if rho_old == 0.0:
+                break                               # breakdown on rho
+            ops.axpby(1.0, z, rho / rho_old, p)     # p = z + beta p
+        ops.spmv(1.0, p, 0.0, q)                    # q = A p
+        (sigma,) = allreduce([ops.dot(p, q)])
+        if sigma == 0.0:
+            break                                   # breakdown on sigma
+        alpha = rho / sigma
+        ops.axpby(alpha, p, 1.0, x)
+        ops.axpby(-alpha, q, 1.0, r)
+        ops.prec(r, z)
+        rr, rz = allreduce([ops.dot(r, r), ops.dot(r, z)])
+        rn = math.sqrt(rr)
+        err = rn / den if den != 0.0 else rn
+        if (rn <= eps * den) if den != 0.0 else (rn <= eps):
+            break
+        rho_old, rho = rho, rz
+    return it, err
+
+
+class DeviceCGOps:
+    """The local operations of dist_cg on this rank's GPU: the DistSpMV
+    product and the library's vector kernels over the nl owned entries (the
+    extended vectors x and p carry the halo after them).  `exchange` is
+    passed to the DistSpMV (None: all_to_all over the default group)."""
+
+    def __init__(self, op: DistSpMV, dinv, exchange=None):
+        from . import psb
+        self.psb, self.op, self.dinv, self.exchange = psb, op, dinv, exchange
+        self.nl, self.ncol = op.part.nl, op.part.ncol
+
+    def new(self, ext=False):
+        return self.psb.DVect(self.ncol if ext else self.nl)
+
+    def spmv(self, alpha, x, beta, y):
+        self.op(alpha, x, beta, y, exchange=self.exchange)
+
+    def dot(self, u, v):
+        return self.psb.psb_gedot(u, v, n=self.nl)
+
+    def axpby(self, a, u, b, v):
+        self.psb.psb_geaxpby(a, u, b, v, n=self.nl)
+
+    def copy(self, u, v):
+        self.psb.psb_geaxpby(1.0, u, 0.0, v, n=self.nl)
+
+    def prec(self, r, z):
+        self.psb.psb_gemlt(1.0, self.dinv, r, 0.0, z, n=self.nl)

@@ -152,3 +152,120 @@ def test_two_rank_gloo_halo_exchange():
     assert [g[2] for g in got] == [True, True]
     assert got[0][0] == 0 and got[0][1] == got[1][0]
     assert all(g[3] > 0 for g in got)
+
+
+# ---- distributed CG (psb_dcg.F90:218-295 over the row-block product) ----
+class _HostCGOps:
+    """dist_cg's local operations on the host for the gloo ranks: the halo
+    through the all-to-all, the local blocks through the oracle's csmv."""
+
+    def __init__(self, part, plan, dinv):
+        self.part, self.plan, self.dinv = part, plan, dinv
+        self.nl, self.ncol = part.nl, part.ncol
+
+    def new(self, ext=False):
+        import numpy as np
+        return np.zeros(self.ncol if ext else self.nl)
+
+    def spmv(self, alpha, x, beta, y):
+        import numpy as np
+        import torch
+
+        import oracle as O
+        from psblas3_b200 import dist as D
+        send = torch.from_numpy(x[self.plan.send_idx - 1].copy())
+        recv = torch.zeros(sum(self.plan.recv_counts), dtype=torch.float64)
+        D.halo_exchange(send, recv, self.plan)
+        x[self.nl:] = recv.numpy()
+        t = O.csr_csmv(*self.part.ad, alpha, x, beta, np.asarray(y[:self.nl]), nc=self.ncol)
+        y[:self.nl] = O.csr_csmv(*self.part.and_, alpha, x, 1.0, t, nc=self.ncol)
+
+    def dot(self, u, v):
+        import oracle as O
+        return O.dot(u[:self.nl], v[:self.nl])
+
+    def axpby(self, a, u, b, v):
+        import oracle as O
+        v[:self.nl] = O.axpby(a, u[:self.nl], b, v[:self.nl])
+
+    def copy(self, u, v):
+        v[:self.nl] = u[:self.nl]
+
+    def prec(self, r, z):
+        z[:self.nl] = self.dinv * r[:self.nl]
+
+
+def _cg_system():
+    import numpy as np
+
+    import oracle as O
+    from psblas3_b200 import gen
+    irp, ja, va = gen.pde3d(12, a=(1, 1, 1), b=(0.0, 0.0, 0.0))   # SPD 7-point operator
+    n = len(irp) - 1
+    ustar = np.random.default_rng(3).uniform(0, 1, n)
+    b = O.csr_csmv(irp, ja, va, 1.0, ustar, 0.0, np.zeros(n))
+    rows = np.repeat(np.arange(n), np.diff(irp))
+    diag = np.zeros(n)
+    on = ja - 1 == rows
+    diag[rows[on]] = va[on]
+    return irp, ja, va, b, O.diag_prec_build(diag)
+
+
+def _cg_worker(rank, world, port, q):
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from psblas3_b200 import dist as D
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    irp, ja, va, b, dinv = _cg_system()
+    part, plan, blocks = D.build_part_on_rank(irp, ja, va, rank, world)
+    ops = _HostCGOps(part, plan, dinv[part.lo:part.hi])
+    x = ops.new(ext=True)
+    calls = {"n": 0}
+
+    def counted(vals):
+        calls["n"] += 1
+        return D.allreduce_sum(vals)
+
+    it, err = D.dist_cg(ops, b[part.lo:part.hi].copy(), x, eps=1e-9, itmax=500, allreduce=counted)
+    got = [None] * world
+    dist.all_gather_object(got, (part.lo, part.hi, it, err, calls["n"], x[:part.nl].copy()))
+    if rank == 0:
+        q.put(got)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_distributed_cg(world):
+    """Row-block CG over gloo ranks (halo all-to-all in every product, the
+    per-iteration scalars in two all_reduces): every rank reports the same
+    iterations and error, within +-2 iterations of the oracle's serial CG,
+    the tolerance reached, and the assembled x equal to the oracle's to
+    1e-8."""
+    import numpy as np
+
+    import oracle as O
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_cg_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=180)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    irp, ja, va, b, dinv = _cg_system()
+    xo, ito, erro = O.krylov("CG", irp, ja, va, b, dinv=dinv, eps=1e-9, itmax=500)
+    its = {g[2] for g in got}
+    assert len(its) == 1 and len({g[3] for g in got}) == 1
+    it, err = got[0][2], got[0][3]
+    assert abs(it - ito) <= 2, (it, ito)
+    assert err <= 1e-9
+    assert got[0][4] == 1 + 2 * it  # one at the start, two per iteration
+    x = np.concatenate([g[5] for g in sorted(got, key=lambda g: g[0])])
+    assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))
