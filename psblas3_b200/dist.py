@@ -28,7 +28,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 __all__ = ["partition_rows", "LocalPart", "local_part", "ExchangePlan", "exchange_plan",
-           "build_part_on_rank", "halo_exchange", "DistSpMV", "allreduce_sum", "dist_cg", "DeviceCGOps"]
+           "build_part_on_rank", "halo_exchange", "DistSpMV", "allreduce_sum", "dist_cg", "dist_cg1",
+           "DeviceCGOps"]
 
 
 def partition_rows(n, world):
@@ -298,6 +299,62 @@ def dist_cg(ops, b, x, eps=1e-6, itmax=1000, istop=2, allreduce=allreduce_sum):
         if (rn <= eps * den) if den != 0.0 else (rn <= eps):
             break
         rho_old, rho = rho, rz
+    return it, err
+
+
+def dist_cg1(ops, b, x, eps=1e-6, itmax=1000, istop=2, allreduce=allreduce_sum):
+    """CG with ONE all_reduce per iteration (Chronopoulos & Gear 1989, the
+    s-step form with s = 1): the product w = A z is formed right after
+    z = M^-1 r, so (r, z), (z, w) and (r, r) of the same residual travel
+    together, and sigma = (p, A p) comes from the recurrence
+    sigma = (z, w) - beta * rho / alpha_old instead of a second dot; q = A p
+    is carried as q = w + beta q.  Same iterates as psb_dcg in exact
+    arithmetic, one more vector update per iteration, one reduction fewer;
+    the rounding differs, so iterations agree with the serial method to
+    within a step or two.  Stop test and (iter, err) as dist_cg."""
+    import math
+    if istop not in (2, 3):
+        raise ValueError("dist_cg1: istop 2 or 3")
+    r, z, w, q = ops.new(), ops.new(), ops.new(), ops.new()
+    p = ops.new(ext=True)
+    zx = ops.new(ext=True)                          # z with room for the halo: the product reads it
+    ops.copy(b, r)
+    ops.spmv(-1.0, x, 1.0, r)                       # r = b - A x0
+    (bb,) = allreduce([ops.dot(b, b)]) if istop == 2 else (None,)
+    it, err, den = 0, 0.0, None
+    rho_old = alpha_old = 0.0
+    while True:
+        ops.prec(r, zx)                             # z = M^-1 r
+        ops.copy(zx, z)
+        ops.spmv(1.0, zx, 0.0, w)                   # w = A z
+        rho, delta, rr = allreduce([ops.dot(r, z), ops.dot(z, w), ops.dot(r, r)])
+        rn = math.sqrt(rr)
+        if den is None:                             # r0: no test before the first update
+            den = math.sqrt(bb) if istop == 2 else rn
+        else:
+            err = rn / den if den != 0.0 else rn
+            if ((rn <= eps * den) if den != 0.0 else (rn <= eps)) or it >= itmax:
+                break
+        it += 1
+        if it == 1:
+            beta, sigma = 0.0, delta
+        else:
+            if rho_old == 0.0:
+                break
+            beta = rho / rho_old
+            sigma = delta - beta * rho / alpha_old
+        if sigma == 0.0:
+            break
+        alpha = rho / sigma
+        if it == 1:
+            ops.copy(z, p)
+            ops.copy(w, q)
+        else:
+            ops.axpby(1.0, z, beta, p)              # p = z + beta p
+            ops.axpby(1.0, w, beta, q)              # q = w + beta q  (= A p)
+        ops.axpby(alpha, p, 1.0, x)
+        ops.axpby(-alpha, q, 1.0, r)
+        rho_old, alpha_old = rho, alpha
     return it, err
 
 

@@ -211,7 +211,7 @@ def _cg_system():
     return irp, ja, va, b, O.diag_prec_build(diag)
 
 
-def _cg_worker(rank, world, port, q):
+def _cg_worker(rank, world, port, q, single=False):
     import datetime
 
     import numpy as np
@@ -230,7 +230,8 @@ def _cg_worker(rank, world, port, q):
         calls["n"] += 1
         return D.allreduce_sum(vals)
 
-    it, err = D.dist_cg(ops, b[part.lo:part.hi].copy(), x, eps=1e-9, itmax=500, allreduce=counted)
+    solver = D.dist_cg1 if single else D.dist_cg
+    it, err = solver(ops, b[part.lo:part.hi].copy(), x, eps=1e-9, itmax=500, allreduce=counted)
     got = [None] * world
     dist.all_gather_object(got, (part.lo, part.hi, it, err, calls["n"], x[:part.nl].copy()))
     if rank == 0:
@@ -239,20 +240,22 @@ def _cg_worker(rank, world, port, q):
     dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("single", [False, True])
 @pytest.mark.parametrize("world", [2, 3])
-def test_gloo_distributed_cg(world):
-    """Row-block CG over gloo ranks (halo all-to-all in every product, the
-    per-iteration scalars in two all_reduces): every rank reports the same
-    iterations and error, within +-2 iterations of the oracle's serial CG,
-    the tolerance reached, and the assembled x equal to the oracle's to
-    1e-8."""
+def test_gloo_distributed_cg(world, single):
+    """Row-block CG over gloo ranks (halo all-to-all in every product; the
+    per-iteration scalars in two all_reduces with the reference's
+    recurrences, or in one with the single-reduction form): every rank
+    reports the same iterations and error, within +-2 iterations of the
+    oracle's serial CG, the tolerance reached, and the assembled x equal to
+    the oracle's to 1e-8."""
     import numpy as np
 
     import oracle as O
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_cg_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_cg_worker, args=(r, world, port, q, single)) for r in range(world)]
     for p in procs:
         p.start()
     got = q.get(timeout=180)
@@ -266,6 +269,8 @@ def test_gloo_distributed_cg(world):
     it, err = got[0][2], got[0][3]
     assert abs(it - ito) <= 2, (it, ito)
     assert err <= 1e-9
-    assert got[0][4] == 1 + 2 * it  # one at the start, two per iteration
+    # all_reduces: the reference's recurrences take one at the start and two
+    # per iteration; the single-reduction form one for ||b||, one per pass
+    assert got[0][4] == (2 + it if single else 1 + 2 * it)
     x = np.concatenate([g[5] for g in sorted(got, key=lambda g: g[0])])
     assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))

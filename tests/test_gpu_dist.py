@@ -28,7 +28,7 @@ def _system():
     return irp, ja, va, b, O.diag_prec_build(diag)
 
 
-def _solve_rank(rank, world, exchange=None):
+def _solve_rank(rank, world, exchange=None, single=False):
     from psblas3_b200 import dist as D
     from psblas3_b200 import psb
     irp, ja, va, b, dinv = _system()
@@ -37,13 +37,14 @@ def _solve_rank(rank, world, exchange=None):
     ops = D.DeviceCGOps(op, psb.DVect.bld(dinv[part.lo:part.hi]), exchange=exchange)
     B = psb.DVect.bld(b[part.lo:part.hi])
     X = ops.new(ext=True)
-    it, err = D.dist_cg(ops, B, X, eps=1e-9, itmax=1000)
+    it, err = (D.dist_cg1 if single else D.dist_cg)(ops, B, X, eps=1e-9, itmax=1000)
     return part, it, err, X.get_vect()[:part.nl]
 
 
-def test_device_dist_cg_one_rank(psb):
+@pytest.mark.parametrize("single", [False, True])
+def test_device_dist_cg_one_rank(psb, single):
     irp, ja, va, b, dinv = _system()
-    part, it, err, x = _solve_rank(0, 1)
+    part, it, err, x = _solve_rank(0, 1, single=single)
     xo, ito, erro = O.krylov("CG", irp, ja, va, b, dinv=dinv, eps=1e-9, itmax=1000)
     assert abs(it - ito) <= 2 and err <= 1e-9
     assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))
@@ -68,7 +69,7 @@ def _host_staged(send, recv, plan):
     return None
 
 
-def _worker(rank, world, port, q):
+def _worker(rank, world, port, q, single):
     import datetime
 
     import torch
@@ -78,7 +79,7 @@ def _worker(rank, world, port, q):
     torch.cuda.set_device(0)
     from psblas3_b200 import psb
     psb.init(0)
-    part, it, err, x = _solve_rank(rank, world, exchange=_host_staged)
+    part, it, err, x = _solve_rank(rank, world, exchange=_host_staged, single=single)
     got = [None] * world
     dist.all_gather_object(got, (part.lo, part.hi, part.nh, it, err, x))
     if rank == 0:
@@ -87,12 +88,13 @@ def _worker(rank, world, port, q):
     dist.destroy_process_group()
 
 
-def test_device_dist_cg_two_ranks(psb):
+@pytest.mark.parametrize("single", [False, True])
+def test_device_dist_cg_two_ranks(psb, single):
     irp, ja, va, b, dinv = _system()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q, single)) for r in range(2)]
     for p in procs:
         p.start()
     got = q.get(timeout=300)
