@@ -516,6 +516,20 @@ int psbx_hll_set_wide(void *deviceMat, int wide_w);
  * (fused multiply-add, two-thread rows) are a tolerance mode too. */
 int psbx_hll_set_wide_split(void *deviceMat, int split);
 
+/* y = alpha*A*x + beta*y with x and y in HOST memory (page-locked for the
+ * copies to overlap; pageable works, serialised): the composition of
+ * writeMultiVecDeviceDouble (x, and y when beta != 0), spmvHllDeviceDouble
+ * and readMultiVecDeviceDouble (hlldev.c:185-207, dvectordev.c) in one
+ * call, with the copies overlapped with the product: the rows are cut into
+ * `chunks` blocks of whole hacks (0: 16; 1: no overlap), x goes up block by
+ * block, each row block starts once the part of x holding its largest
+ * column is on the device, and its part of y goes down as soon as it is
+ * done.  The same bits as the three calls.  Overlap needs hack size 32, no
+ * wide hacks and no row permutation; other handles take the three steps one
+ * after the other.  Device staging vectors are kept in the handle.  x may
+ * be the same array as y.  Returns once y is on the host. */
+int psbx_hll_spmv_host(void *deviceMat, double alpha, const double *x, double beta, double *y, int chunks);
+
 /* Row mapping of the standalone SpMV on a hack-32 HLL handle: 0 auto (two
  * rows per thread when there are wide hacks, one otherwise), 1 one thread
  * per row, 2 two threads per row (entries of even and odd position summed

@@ -142,7 +142,7 @@ _SIGS = {
     "psbx_hll_from_csr_device": (I, [PP, I, I, I, P, P, P, I, P]),
     "psbx_hll_autotune_from_csr_device": (I, [PP, I, I, I, P, P, P, P, PI, PI, PD]),
     "psbx_hll_make_single": (I, [P]), "psbx_hll_set_wide": (I, [P, I]), "psbx_hll_set_wide_split": (I, [P, I]),
-    "psbx_hll_set_threads_per_row": (I, [P, I]), "psbx_probe_gather": (I, [P, C.c_longlong, I, P, P, I, PD]), "psbx_hll_get_layout": (I, [P, PI, PI, PI, PI]),
+    "psbx_hll_set_threads_per_row": (I, [P, I]), "psbx_hll_spmv_host": (I, [P, D, P, D, P, I]), "psbx_probe_gather": (I, [P, C.c_longlong, I, P, P, I, PD]), "psbx_hll_get_layout": (I, [P, PI, PI, PI, PI]),
     "psbx_wrapMultiVecDevice": (I, [PP, P, U, U]), "psbx_multivec_data": (P, [P]),
     "psbx_hll_spmv_raw": (I, [P, D, P, D, P]),
     "psbx_dot_noalloc": (I, [P, I, I, P, P, I, P]),

@@ -84,6 +84,9 @@ static void ctx_destroy() {
   cudaFree(c.d_res);
   cudaFreeHost(c.h_res);
   cudaStreamSynchronize(c.defaultStream);
+  for (cudaEvent_t e : c.xev) cudaEventDestroy(e);
+  if (c.h2d) cudaStreamDestroy(c.h2d);
+  if (c.d2h) cudaStreamDestroy(c.d2h);
   if (c.pool) cudaMemPoolDestroy(c.pool);
   cudaStreamDestroy(c.defaultStream);
   c = PsbxCtx();

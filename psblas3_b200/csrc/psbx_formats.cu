@@ -100,6 +100,10 @@ void freeHllDevice(void *deviceMat) {
   cudaFree(m->wpart);
   cudaFree(m->wticket);
   cudaFree(m->wcbase);
+  cudaFree(m->hx);
+  cudaFree(m->hy);
+  free(m->hcmin);
+  free(m->hcmax);
   free(m->tplan);
   free(m);
 }

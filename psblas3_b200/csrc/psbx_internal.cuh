@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <atomic>
+#include <vector>
 
 #include "../../include/psbx.h"
 
@@ -65,6 +66,11 @@ struct HllDevice {
   double *wpart;     // split mode: 32 row partials per product block (nWChunks x 32)
   unsigned *wticket; // split mode: per wide hack, product blocks done (kept at zero between calls)
   int *wcbase;       // nLong+1: first product block of each wide hack
+  // host-buffer SpMV (psbx_hll_spmv_host): device staging vectors, and per
+  // hack the smallest and largest column it holds (host arrays, built on
+  // first use, dropped when the arrays are rewritten)
+  double *hx, *hy;
+  int *hcmin, *hcmax;
 };
 
 // Default width above which a hack of 32 rows takes the wide-hack path.
@@ -136,6 +142,10 @@ struct PsbxCtx {
   // with nothing kept, every solve remapped its workspace (1 GB for CG on
   // 16.8M rows), and calls of the same solve varied from 0.49 to 1.1 s.
   cudaMemPool_t pool = nullptr;
+  // copy streams and events of the host-buffer SpMV (psbx_hll_spmv_host),
+  // created on first use
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> xev;
 };
 #define PSBX_POOL_KEEP ((uint64_t)4 << 30)
 

@@ -276,6 +276,9 @@ int psbx_hll_index_long(HllDevice *m) {
   free(m->tplan);  // the arrays changed: the batch engine's tile plan is redone
   m->tplan = nullptr;
   m->ntplan = 0;
+  free(m->hcmin);  // and the host-buffer SpMV's column ranges
+  free(m->hcmax);
+  m->hcmin = m->hcmax = nullptr;
   cudaFree(m->longHacks);
   cudaFree(m->lres);
   cudaFree(m->wideBase);
@@ -623,6 +626,163 @@ int psbx_launch_hll_spmv(const HllDevice *m, double alpha, const double *x, doub
     return launch_rows(hll32_view(v), alpha, x, beta, y, st);
   }
   return launch_rows(hll_view(m), alpha, x, beta, y, st);
+}
+
+// ------------------------------------------------- host-buffer SpMV
+// y_host = alpha*A*x_host + beta*y_host with the copies overlapped with the
+// product (psbx_hll_spmv_host).  The rows are cut into `chunks` blocks of
+// whole hacks, x into blocks of the same size; x's blocks go up on one
+// stream, in order, and row block k starts on the library stream once the
+// block holding its largest column has arrived (from the per-hack column
+// ranges, found once per matrix); its part of y goes down on a third stream
+// as soon as it is done.  A banded matrix then costs about one copy of x
+// up and one of y down running side by side, instead of copy, product and
+// copy one after the other.  Each row is summed as by psbx_launch_hll_spmv
+// (the same kernels over a row range), so the results are the same bits.
+
+// Smallest and largest column of each hack (a warp per hack; rows of
+// length 0 count for nothing: INT_MAX / INT_MIN).
+__global__ void k_hll_colrange(HllView A, int nh, int *__restrict__ cmin, int *__restrict__ cmax) {
+  const int h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (h >= nh) return;  // whole warps: blockDim is a multiple of 32
+  const int s = h * 32 + lane;
+  const int len = s < A.rows ? A.irn[s] : 0;
+  const size_t off = (size_t)A.hkoffs[h] + lane;
+  int lo = 0x7fffffff, hi = (int)0x80000000;
+  for (int j = 0; j < len; j++) {
+    const int c = A.ja[off + (size_t)j * 32];
+    lo = min(lo, c);
+    hi = max(hi, c);
+  }
+  lo = __reduce_min_sync(0xffffffffu, lo);
+  hi = __reduce_max_sync(0xffffffffu, hi);
+  if (lane == 0) {
+    cmin[h] = lo;
+    cmax[h] = hi;
+  }
+}
+
+static int hll_colranges(HllDevice *m, cudaStream_t st) {
+  if (m->hcmin) return SPGPU_SUCCESS;
+  const int nh = (m->rows + 31) / 32;
+  int *d = nullptr;
+  PSBX_CK(cudaMalloc(&d, sizeof(int) * 2 * (size_t)nh));
+  k_hll_colrange<<<(nh + 7) / 8, 256, 0, st>>>(hll_view(m), nh, d, d + nh);
+  psbx_count_launch();
+  cudaError_t e = cudaGetLastError();
+  int *lo = (int *)malloc(sizeof(int) * (size_t)nh), *hi = (int *)malloc(sizeof(int) * (size_t)nh);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lo, d, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hi, d + nh, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    free(lo);
+    free(hi);
+    return psbx_cuda_status(e, "hll column ranges");
+  }
+  m->hcmin = lo;
+  m->hcmax = hi;
+  return SPGPU_SUCCESS;
+}
+
+// rows [r0, r0 + nr) of a hack-32 matrix without wide hacks or permutation
+static int launch_hll_rows_range(const HllDevice *m, int r0, int nr, double alpha, const double *x, double beta,
+                                 double *y, cudaStream_t st) {
+  HllView v = hll_view(m);
+  v.irn += r0;
+  v.hkoffs += r0 / 32;
+  v.rows = nr;
+  if (hll_short_rows(m)) return launch_rows(hll32s_view(v), alpha, x, beta, y + r0, st);
+  return launch_rows(hll32_view(v), alpha, x, beta, y + r0, st);
+}
+
+extern "C" int psbx_hll_spmv_host(void *deviceMat, double alpha, const double *x, double beta, double *y,
+                                  int chunks) {
+  int rc = psbx_ensure_init();
+  if (rc) return rc;
+  HllDevice *m = (HllDevice *)deviceMat;
+  if (!m || !x || !y || chunks < 0) return SPGPU_UNSUPPORTED;
+  if (m->elemType != SPGPU_TYPE_DOUBLE) return SPGPU_UNSUPPORTED;
+  const int n = m->rows, nc = m->cols;
+  if (n <= 0) return SPGPU_SUCCESS;
+  PsbxCtx &c = psbx_ctx();
+  cudaStream_t st = c.stream;
+  if (!m->hx) PSBX_CK(cudaMalloc(&m->hx, sizeof(double) * (size_t)(nc > 0 ? nc : 1)));
+  if (!m->hy) PSBX_CK(cudaMalloc(&m->hy, sizeof(double) * (size_t)n));
+  const size_t xb = sizeof(double) * (size_t)nc, yb = sizeof(double) * (size_t)n;
+  const bool pipe = chunks != 1 && m->hackSize == 32 && m->nLong == 0 && !m->perm && alpha != 0.0;
+  if (!pipe) {
+    // one copy up, the product, one copy down, all on the library stream
+    if (nc > 0) PSBX_CK(cudaMemcpyAsync(m->hx, x, xb, cudaMemcpyHostToDevice, st));
+    if (beta != 0.0) PSBX_CK(cudaMemcpyAsync(m->hy, y, yb, cudaMemcpyHostToDevice, st));
+    rc = psbx_launch_hll_spmv(m, alpha, m->hx, beta, m->hy, st);
+    if (rc) return rc;
+    PSBX_CK(cudaMemcpyAsync(y, m->hy, yb, cudaMemcpyDeviceToHost, st));
+    PSBX_CK(cudaStreamSynchronize(st));
+    return SPGPU_SUCCESS;
+  }
+  rc = hll_colranges(m, st);
+  if (rc) return rc;
+  const int nh = (n + 31) / 32;
+  int k = chunks == 0 ? 16 : chunks;
+  if (k > nh) k = nh;
+  const int hb = (nh + k - 1) / k;  // hacks per row block
+  k = (nh + hb - 1) / hb;
+  const int B = hb * 32;            // rows per block, and columns per block of x
+  const int kx = nc > 0 ? (nc + B - 1) / B : 0;
+  if (!c.h2d) PSBX_CK(cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking));
+  if (!c.d2h) PSBX_CK(cudaStreamCreateWithFlags(&c.d2h, cudaStreamNonBlocking));
+  const size_t nev = (size_t)kx + 2 * (size_t)k + 1;
+  while (c.xev.size() < nev) {
+    cudaEvent_t e;
+    PSBX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c.xev.push_back(e);
+  }
+  cudaEvent_t *ex = c.xev.data(), *ey = ex + kx, *ec = ey + k;  // x blocks, y blocks, row blocks
+  cudaEvent_t e0 = c.xev[nev - 1];
+  // the copies start after whatever the library stream still runs
+  PSBX_CK(cudaEventRecord(e0, st));
+  PSBX_CK(cudaStreamWaitEvent(c.h2d, e0, 0));
+  PSBX_CK(cudaStreamWaitEvent(c.d2h, e0, 0));
+  for (int b = 0; b < kx || b < k; b++) {
+    if (b < kx) {
+      const size_t c0 = (size_t)b * B, len = std::min((size_t)B, (size_t)nc - c0);
+      PSBX_CK(cudaMemcpyAsync(m->hx + c0, x + c0, len * sizeof(double), cudaMemcpyHostToDevice, c.h2d));
+      PSBX_CK(cudaEventRecord(ex[b], c.h2d));
+    }
+    if (b < k && beta != 0.0) {
+      const size_t r0 = (size_t)b * B, len = std::min((size_t)B, (size_t)n - r0);
+      PSBX_CK(cudaMemcpyAsync(m->hy + r0, y + r0, len * sizeof(double), cudaMemcpyHostToDevice, c.h2d));
+      PSBX_CK(cudaEventRecord(ey[b], c.h2d));
+    }
+  }
+  for (int b = 0; b < k; b++) {
+    const int r0 = b * B, nr = std::min(B, n - r0);
+    int hi = (int)0x80000000;
+    for (int h = b * hb; h < std::min(nh, (b + 1) * hb); h++) hi = std::max(hi, m->hcmax[h]);
+    if (kx > 0) {
+      // the block of x holding the largest column, and at least x's block
+      // b itself: its copy down may overwrite that host memory when x and y
+      // are the same array
+      int need = hi == (int)0x80000000 ? 0 : (hi - m->baseIndex) / B;
+      need = std::max(need, b);
+      need = need < 0 ? 0 : (need >= kx ? kx - 1 : need);
+      PSBX_CK(cudaStreamWaitEvent(st, ex[need], 0));
+    }
+    if (beta != 0.0) PSBX_CK(cudaStreamWaitEvent(st, ey[b], 0));
+    rc = launch_hll_rows_range(m, r0, nr, alpha, m->hx, beta, m->hy, st);
+    if (rc) return rc;
+    PSBX_CK(cudaEventRecord(ec[b], st));
+    PSBX_CK(cudaStreamWaitEvent(c.d2h, ec[b], 0));
+    PSBX_CK(cudaMemcpyAsync(y + r0, m->hy + r0, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, c.d2h));
+  }
+  // the library stream resumes after the last copy down; the call returns
+  // with y on the host
+  PSBX_CK(cudaEventRecord(e0, c.d2h));
+  PSBX_CK(cudaStreamWaitEvent(st, e0, 0));
+  PSBX_CK(cudaStreamSynchronize(c.d2h));
+  PSBX_CK(cudaStreamSynchronize(st));
+  return SPGPU_SUCCESS;
 }
 
 int psbx_launch_ell_spmv(const EllDevice *m, double alpha, const double *x, double beta, double *y,

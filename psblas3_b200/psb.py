@@ -207,6 +207,17 @@ class HllMat:
         check(lib.psbx_hll_set_wide_split(self.h, int(bool(split))), "psbx_hll_set_wide_split")
         return self
 
+    def spmv_host(self, alpha, x, beta, y, chunks=0):
+        """y = alpha*A*x + beta*y for host arrays (numpy float64, or pinned
+        torch tensors for overlapped copies): copies up, the product and the
+        copy down in one call, overlapped block by block
+        (psbx_hll_spmv_host)."""
+        def ptr(a):
+            return C.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else a.ctypes.data_as(C.c_void_p)
+        check(lib.psbx_hll_spmv_host(self.h, float(alpha), ptr(x), float(beta), ptr(y), int(chunks)),
+              "psbx_hll_spmv_host")
+        return y
+
     def set_threads_per_row(self, tpr):
         """Row mapping of the standalone SpMV (hack size 32): 0 auto, 1 or 2
         threads per row (2: tolerance mode only), -2 two rows per thread."""

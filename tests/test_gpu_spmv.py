@@ -568,3 +568,49 @@ def test_probe_gather(psb):
                                 C.c_void_p(out.data_ptr()), 3, C.byref(ms)), "psbx_probe_gather")
     assert ms.value > 0
     assert out.sum().item() == 2 * (n // 2)  # every pair read once, x = 1
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.5, 0.5), (0.0, 2.0)])
+def test_hll_spmv_host(psb, alpha, beta):
+    """psbx_hll_spmv_host (host x and y, copies overlapped with the product
+    block by block) gives the bits of write + spmvHllDeviceDouble + read for
+    every block count, with pageable and page-locked host arrays, on banded
+    operators (overlapped) and on handles that take the three steps in turn
+    (wide hacks, a row permutation); x may be the same array as y."""
+    import torch
+    rng = np.random.default_rng(17)
+    cases = []
+    for irp, ja, va in (gen.stencil27(30), gen.pde3d(21, a=(1, 1, 1), b=(0.5, 0.5, 0.5))):
+        n = len(irp) - 1
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        cases.append((psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(),
+                                                 d[2].data_ptr(), 32), n))
+    sirp, sja, sva, order = gen.sort_rows_by_length(*gen.powerlaw(20011, kmax=3000, seed=4))
+    n = len(sirp) - 1
+    d = [torch.from_numpy(a).cuda() for a in (sirp, sja, sva)]
+    cases.append((psb.HllMat.from_csr_device(n, n, len(sja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                             32), n))
+    irp, ja, va = gen.pde3d(17)
+    n = len(irp) - 1
+    perm = torch.from_numpy(rng.permutation(n).astype(np.int32)).cuda()
+    d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+    cases.append((psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32,
+                                             perm.data_ptr()), n))
+    for A, n in cases:
+        x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+        X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+        A.spmv(alpha, X, beta, Y)
+        want = Y.get_vect()
+        for chunks in (0, 1, 3, 7, 10 ** 6):
+            y = y0.copy()
+            A.spmv_host(alpha, x, beta, y, chunks=chunks)
+            assert np.array_equal(y, want), (n, chunks)
+            xp = torch.from_numpy(x).pin_memory()
+            yp = torch.from_numpy(y0.copy()).pin_memory()
+            A.spmv_host(alpha, xp, beta, yp, chunks=chunks)
+            assert np.array_equal(yp.numpy(), want), (n, chunks, "pinned")
+        if beta == 0.0:  # y = A y in place
+            yy = x.copy()
+            A.spmv_host(alpha, yy, 0.0, yy)
+            assert np.array_equal(yy, want)
+        A.free()
