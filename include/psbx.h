@@ -521,7 +521,7 @@ int psbx_hll_set_wide_split(void *deviceMat, int split);
  * writeMultiVecDeviceDouble (x, and y when beta != 0), spmvHllDeviceDouble
  * and readMultiVecDeviceDouble (hlldev.c:185-207, dvectordev.c) in one
  * call, with the copies overlapped with the product: the rows are cut into
- * `chunks` blocks of whole hacks (0: 16; 1: no overlap), x goes up block by
+ * `chunks` blocks of whole hacks (0: 8; 1: no overlap), x goes up block by
  * block, each row block starts once the part of x holding its largest
  * column is on the device, and its part of y goes down as soon as it is
  * done.  The same bits as the three calls.  Overlap needs hack size 32, no

@@ -724,7 +724,10 @@ extern "C" int psbx_hll_spmv_host(void *deviceMat, double alpha, const double *x
   rc = hll_colranges(m, st);
   if (rc) return rc;
   const int nh = (n + 31) / 32;
-  int k = chunks == 0 ? 16 : chunks;
+  // 8 blocks by default: on the 27-point 200^3 operator (64 MB each way)
+  // 1 / 2 / 4 / 8 / 16 / 32 / 64 blocks took 2.74 / 2.59 / 2.07 / 1.95 /
+  // 2.03 / 2.20 / 2.44 ms -- each copy costs a fixed few microseconds
+  int k = chunks == 0 ? 8 : chunks;
   if (k > nh) k = nh;
   const int hb = (nh + k - 1) / k;  // hacks per row block
   k = (nh + hb - 1) / hb;
