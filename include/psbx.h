@@ -524,10 +524,13 @@ int psbx_hll_set_wide_split(void *deviceMat, int split);
  * `chunks` blocks of whole hacks (0: 8; 1: no overlap), x goes up block by
  * block, each row block starts once the part of x holding its largest
  * column is on the device, and its part of y goes down as soon as it is
- * done.  The same bits as the three calls.  Overlap needs hack size 32, no
- * wide hacks and no row permutation; other handles take the three steps one
- * after the other.  Device staging vectors are kept in the handle.  x may
- * be the same array as y.  Returns once y is on the host. */
+ * done -- or, when beta is 0 and y is page-locked, each row block stores
+ * its part of y straight into it (no copy down), so the two directions of
+ * the link carry x and y at the same time.  The same bits as the three
+ * calls.  Overlap needs hack size 32, no wide hacks and no row permutation;
+ * other handles take the three steps one after the other.  Device staging
+ * vectors are kept in the handle.  x may be the same array as y.  Returns
+ * once y is on the host. */
 int psbx_hll_spmv_host(void *deviceMat, double alpha, const double *x, double beta, double *y, int chunks);
 
 /* Row mapping of the standalone SpMV on a hack-32 HLL handle: 0 auto (two

@@ -733,6 +733,19 @@ extern "C" int psbx_hll_spmv_host(void *deviceMat, double alpha, const double *x
   k = (nh + hb - 1) / hb;
   const int B = hb * 32;            // rows per block, and columns per block of x
   const int kx = nc > 0 ? (nc + B - 1) / B : 0;
+  // y in page-locked host memory that the device can address (and beta = 0,
+  // so y is only written): the row blocks store their part of y straight
+  // into it over PCIe, in the other direction than x's copies, instead of
+  // through a device copy and a copy down -- the two directions of the link
+  // then carry the two vectors at the same time
+  double *ydev = nullptr;
+  if (beta == 0.0) {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, y) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer)
+      ydev = (double *)pa.devicePointer;
+    else
+      cudaGetLastError();  // pageable memory: not an error, the copies are used
+  }
   if (!c.h2d) PSBX_CK(cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking));
   if (!c.d2h) PSBX_CK(cudaStreamCreateWithFlags(&c.d2h, cudaStreamNonBlocking));
   const size_t nev = (size_t)kx + 2 * (size_t)k + 1;
@@ -773,8 +786,9 @@ extern "C" int psbx_hll_spmv_host(void *deviceMat, double alpha, const double *x
       PSBX_CK(cudaStreamWaitEvent(st, ex[need], 0));
     }
     if (beta != 0.0) PSBX_CK(cudaStreamWaitEvent(st, ey[b], 0));
-    rc = launch_hll_rows_range(m, r0, nr, alpha, m->hx, beta, m->hy, st);
+    rc = launch_hll_rows_range(m, r0, nr, alpha, m->hx, beta, ydev ? ydev : m->hy, st);
     if (rc) return rc;
+    if (ydev) continue;  // written in place
     PSBX_CK(cudaEventRecord(ec[b], st));
     PSBX_CK(cudaStreamWaitEvent(c.d2h, ec[b], 0));
     PSBX_CK(cudaMemcpyAsync(y + r0, m->hy + r0, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, c.d2h));

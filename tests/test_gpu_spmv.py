@@ -574,7 +574,8 @@ def test_probe_gather(psb):
 def test_hll_spmv_host(psb, alpha, beta):
     """psbx_hll_spmv_host (host x and y, copies overlapped with the product
     block by block) gives the bits of write + spmvHllDeviceDouble + read for
-    every block count, with pageable and page-locked host arrays, on banded
+    every block count, with pageable and page-locked host arrays (beta = 0
+    and page-locked y: the row blocks store into y directly), on banded
     operators (overlapped) and on handles that take the three steps in turn
     (wide hacks, a row permutation); x may be the same array as y."""
     import torch
@@ -609,8 +610,13 @@ def test_hll_spmv_host(psb, alpha, beta):
             yp = torch.from_numpy(y0.copy()).pin_memory()
             A.spmv_host(alpha, xp, beta, yp, chunks=chunks)
             assert np.array_equal(yp.numpy(), want), (n, chunks, "pinned")
-        if beta == 0.0:  # y = A y in place
+        if beta == 0.0:  # y = A y in place, pageable and page-locked
             yy = x.copy()
             A.spmv_host(alpha, yy, 0.0, yy)
             assert np.array_equal(yy, want)
+            yp = torch.from_numpy(x.copy()).pin_memory()
+            for _ in range(2):
+                yp.copy_(torch.from_numpy(x))
+                A.spmv_host(alpha, yp, 0.0, yp)
+                assert np.array_equal(yp.numpy(), want)
         A.free()
