@@ -605,6 +605,11 @@ int psbx_batch_step(void *eng, int replays, int *n_running);
 int psbx_batch_launch(void *eng, int replays);
 int psbx_batch_wait(void *eng, int *n_running);
 int psbx_batch_poll(void *eng, int slot, int *state, int *outer, int *iters, double *err);
+/* The slots whose solve has ended as of the last wait (phase done, not yet
+ * removed), in slot order: the first `max` go to slots[], *count receives
+ * how many there are (call again with a larger array if it exceeds max).
+ * One call instead of a poll per running slot. */
+int psbx_batch_finished(void *eng, int *slots, int max, int *count);
 int psbx_batch_remove(void *eng, int slot);
 int psbx_batch_destroy(void *eng);
 

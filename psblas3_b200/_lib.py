@@ -150,7 +150,7 @@ _SIGS = {
     "psbx_batch_add": (I, [P, P, P, P, P, D, D, I, PI]),
     "psbx_batch_step": (I, [P, I, PI]),
     "psbx_batch_launch": (I, [P, I]), "psbx_batch_wait": (I, [P, PI]),
-    "psbx_batch_poll": (I, [P, I, PI, PI, PI, PD]),
+    "psbx_batch_poll": (I, [P, I, PI, PI, PI, PD]), "psbx_batch_finished": (I, [P, PI, I, PI]),
     "psbx_batch_remove": (I, [P, I]),
     "psbx_batch_destroy": (I, [P]),
     "psbx_kernel_launches": (C.c_uint64, []), "psbx_last_error": (C.c_char_p, []),

@@ -1324,6 +1324,19 @@ int psbx_batch_poll(void *eng, int slot, int *state, int *outer, int *iters, dou
   return SPGPU_SUCCESS;
 }
 
+int psbx_batch_finished(void *eng, int *slots, int max, int *count) {
+  Eng *e = (Eng *)eng;
+  if (!e || !count || max < 0 || (max > 0 && !slots)) return SPGPU_UNSUPPORTED;
+  int n = 0;
+  for (int s = 0; s < e->max_sys; s++)
+    if (e->used[s] && e->h_state_pinned[s].phase == PH_DONE) {
+      if (n < max) slots[n] = s;
+      n++;
+    }
+  *count = n;
+  return SPGPU_SUCCESS;
+}
+
 int psbx_batch_remove(void *eng, int slot) {
   Eng *e = (Eng *)eng;
   if (!e || slot < 0 || slot >= e->max_sys || !e->used[slot]) return SPGPU_UNSUPPORTED;

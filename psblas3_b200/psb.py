@@ -482,6 +482,8 @@ class BatchSolver:
                                          64 if inner_fp64 else 32), "batch_create")
         self.h = h
         self.keep = {}
+        self.max_systems = int(max_systems)
+        self._fin = (C.c_int * max(1, self.max_systems))()
 
     def add(self, A, d_b, d_x, d_dinv=None, eps=1e-10, inner_tol=1e-2, itmax=100000, keep=None):
         """A: HllMat (hack 32); d_b, d_x, d_dinv: device pointers (ints) or
@@ -515,6 +517,13 @@ class BatchSolver:
         err = (C.c_double * self.nrhs)()
         check(lib.psbx_batch_poll(self.h, int(slot), C.byref(st), C.byref(outer), its, err), "batch_poll")
         return st.value, outer.value, list(its), list(err)
+
+    def finished(self):
+        """Slots whose solve has ended as of the last wait, in slot order (one
+        call; poll them for their results)."""
+        cnt = C.c_int(0)
+        check(lib.psbx_batch_finished(self.h, self._fin, len(self._fin), C.byref(cnt)), "batch_finished")
+        return list(self._fin[:min(cnt.value, len(self._fin))])
 
     def remove(self, slot):
         check(lib.psbx_batch_remove(self.h, int(slot)), "batch_remove")

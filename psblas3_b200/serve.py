@@ -138,7 +138,12 @@ class Server:
         """Requests whose solve ended, as of the last wait (removed from the
         running set)."""
         finished = []
-        for slot in list(self.running):
+        # one call lists the ended slots (a poll per running slot would keep
+        # the device idle for a host loop over all of them between replays)
+        slots = self.eng.finished() if hasattr(self.eng, "finished") else list(self.running)
+        for slot in slots:
+            if slot not in self.running:
+                continue
             st, outer, its, err = self.eng.poll(slot)
             if st == 0:
                 continue

@@ -199,3 +199,33 @@ def test_fp64_inner_engine(psb, k):
         it64, _ = psb.psb_krylov("CG", A, P, B, X, eps=EPS, itmax=100000)
         assert its[0] <= 1.1 * it64 + 10, (its[0], it64)
     eng.free()
+
+
+def test_finished_lists_ended_slots(psb):
+    """psbx_batch_finished returns, after each step, exactly the slots that
+    poll reports ended (state != 0) and that are not removed yet, in slot
+    order; removing one takes it off the list."""
+    import torch
+    sizes = (6, 10, 16, 24)
+    eng = psb.BatchSolver(8, sum(s ** 3 for s in sizes), 1)
+    slots, keep = [], []
+    for m in sizes:
+        irp, ja, va = gen.poisson7(m)
+        n = len(irp) - 1
+        A, P = _system(psb, irp, ja, va)
+        db = torch.from_numpy(np.random.default_rng(m).uniform(-1, 1, n)).cuda()
+        dx = torch.zeros_like(db)
+        keep.append((A, P, db, dx))
+        slots.append(eng.add(A, db, dx, P.dv.data_ptr, eps=EPS))
+    seen_partial = False
+    for _ in range(200):
+        running = eng.step(1)
+        ended = [s for s in slots if eng.poll(s)[0] != 0]
+        assert eng.finished() == sorted(ended)
+        seen_partial |= 0 < len(ended) < len(slots)
+        if running == 0:
+            break
+    assert eng.finished() == sorted(slots) and seen_partial
+    eng.remove(slots[1])
+    assert eng.finished() == sorted(s for s in slots if s != slots[1])
+    eng.free()
