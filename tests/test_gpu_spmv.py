@@ -597,8 +597,18 @@ def test_hll_spmv_host(psb, alpha, beta):
     d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
     cases.append((psb.HllMat.from_csr_device(n, n, len(ja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 32,
                                              perm.data_ptr()), n))
+    # rectangular: more columns than rows, and fewer
+    for nr, nc in ((5000, 5517), (5000, 4700)):
+        rows = [np.unique(np.append(rng.choice(nc, 5, replace=False), min(i, nc - 1))) + 1 for i in range(nr)]
+        ja = np.concatenate(rows).astype(np.int32)
+        irp = np.concatenate([[1], 1 + np.cumsum([len(r) for r in rows])]).astype(np.int32)
+        va = rng.standard_normal(len(ja))
+        d = [torch.from_numpy(a).cuda() for a in (irp, ja, va)]
+        cases.append((psb.HllMat.from_csr_device(nr, nc, len(ja), d[0].data_ptr(), d[1].data_ptr(),
+                                                 d[2].data_ptr(), 32), (nr, nc)))
     for A, n in cases:
-        x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+        nr, nc = n if isinstance(n, tuple) else (n, n)
+        x, y0 = rng.uniform(-1, 1, nc), rng.uniform(-1, 1, nr)
         X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
         A.spmv(alpha, X, beta, Y)
         want = Y.get_vect()
@@ -610,7 +620,7 @@ def test_hll_spmv_host(psb, alpha, beta):
             yp = torch.from_numpy(y0.copy()).pin_memory()
             A.spmv_host(alpha, xp, beta, yp, chunks=chunks)
             assert np.array_equal(yp.numpy(), want), (n, chunks, "pinned")
-        if beta == 0.0:  # y = A y in place, pageable and page-locked
+        if beta == 0.0 and nr == nc:  # y = A y in place, pageable and page-locked
             yy = x.copy()
             A.spmv_host(alpha, yy, 0.0, yy)
             assert np.array_equal(yy, want)
