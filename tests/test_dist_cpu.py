@@ -173,10 +173,12 @@ class _HostCGOps:
 
         import oracle as O
         from psblas3_b200 import dist as D
-        send = torch.from_numpy(x[self.plan.send_idx - 1].copy())
-        recv = torch.zeros(sum(self.plan.recv_counts), dtype=torch.float64)
-        D.halo_exchange(send, recv, self.plan)
-        x[self.nl:] = recv.numpy()
+        import torch.distributed as dist
+        if dist.is_initialized():  # every rank takes part in the all-to-all
+            send = torch.from_numpy(x[self.plan.send_idx - 1].copy())
+            recv = torch.zeros(sum(self.plan.recv_counts), dtype=torch.float64)
+            D.halo_exchange(send, recv, self.plan)
+            x[self.nl:] = recv.numpy()
         t = O.csr_csmv(*self.part.ad, alpha, x, beta, np.asarray(y[:self.nl]), nc=self.ncol)
         y[:self.nl] = O.csr_csmv(*self.part.and_, alpha, x, 1.0, t, nc=self.ncol)
 
@@ -274,3 +276,31 @@ def test_gloo_distributed_cg(world, single):
     assert got[0][4] == (2 + it if single else 1 + 2 * it)
     x = np.concatenate([g[5] for g in sorted(got, key=lambda g: g[0])])
     assert np.max(np.abs(x - xo)) <= 1e-8 * np.max(np.abs(xo))
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_dist_cg_one_rank_stop_tests(single):
+    """One rank, no process group: istop 3 (||r|| against ||r0||) within +-2
+    iterations of the oracle's serial CG from a nonzero x0, and itmax ends
+    the solve at exactly itmax iterations with the error of the last one."""
+    import numpy as np
+
+    import oracle as O
+    from psblas3_b200 import dist as D
+    irp, ja, va, b, dinv = _cg_system()
+    n = len(irp) - 1
+    part = D.local_part(irp, ja, va, 0, n)
+    plan = D.exchange_plan(0, [(0, n)], [part.halo])
+    ops = _HostCGOps(part, plan, dinv)
+    solver = D.dist_cg1 if single else D.dist_cg
+    x0 = np.random.default_rng(9).uniform(-1, 1, n)
+    x = ops.new(ext=True)
+    x[:n] = x0
+    it, err = solver(ops, b.copy(), x, eps=1e-8, itmax=500, istop=3, allreduce=lambda v: [float(t) for t in v])
+    xo, ito, erro = O.krylov("CG", irp, ja, va, b, x0=x0, dinv=dinv, eps=1e-8, itmax=500, istop=3)
+    assert abs(it - ito) <= 2 and err <= 1e-8
+    x = ops.new(ext=True)
+    it, err = solver(ops, b.copy(), x, eps=1e-14, itmax=5, allreduce=lambda v: [float(t) for t in v])
+    _, ito, erro = O.krylov("CG", irp, ja, va, b, dinv=dinv, eps=1e-14, itmax=5)
+    assert it == 5 == ito
+    assert abs(err - erro) <= 1e-6 * erro
