@@ -630,3 +630,34 @@ def test_hll_spmv_host(psb, alpha, beta):
                 A.spmv_host(alpha, yp, 0.0, yp)
                 assert np.array_equal(yp.numpy(), want)
         A.free()
+
+
+def test_device_build_random_matrices(psb):
+    """Seeded random matrices (rectangular, empty rows, after psb_d_fix_coo):
+    the device CSR -> HLL build gives the CPU converter's arrays byte for
+    byte for hack sizes 32 and 64, and the device product (exact mode) the
+    CPU csmv's bits."""
+    import torch
+    for seed in range(12):
+        rng = np.random.default_rng(2000 + seed)
+        nr, nc = int(rng.integers(1, 300)), int(rng.integers(1, 300))
+        nz = max(1, int(nr * nc * float(rng.uniform(0.0, 0.1))))
+        ia, ja, va = O.coo_fix(nr, rng.integers(1, nr + 1, nz), rng.integers(1, nc + 1, nz), rng.standard_normal(nz))
+        irp, cja, cva = O.csr_from_coo(nr, ia, ja, va)
+        x, y0 = rng.uniform(-1, 1, nc), rng.uniform(-1, 1, nr)
+        want = O.csr_csmv(irp, cja, cva, -1.5, x, 0.5, y0, nc=nc)
+        for hksz in (32, 64):
+            h = O.hll_from_coo(nr, ia, ja, va, hksz)
+            d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (irp, cja, cva)]
+            A = psb.HllMat.from_csr_device(nr, nc, len(cja), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), hksz)
+            g = A.read()
+            for k in ("hkoffs", "irn", "ja"):
+                assert np.array_equal(g[k], h[k]), (seed, hksz, k)
+            assert np.array_equal(g["val"].view(np.uint64), h["val"].view(np.uint64)), (seed, hksz)
+            has = np.array([np.any(cja[irp[r] - 1:irp[r + 1] - 1] == r + 1) for r in range(nr)], bool)
+            assert np.array_equal(g["idiag"][has], h["idiag"][has])
+            A.set_wide_split(False)
+            X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+            A.spmv(-1.5, X, 0.5, Y)
+            assert np.array_equal(Y.get_vect(), want), (seed, hksz)
+            A.free()

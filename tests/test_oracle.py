@@ -241,3 +241,57 @@ def test_oracle_fcg_and_rgmres():
     assert abs(c.value ** 2 + s.value ** 2 - 1.0) <= 1e-15
     with pytest.raises(ValueError):
         O.krylov("RGMRES", irp, ja, va, b, istop=1)
+
+
+def _random_coo(draw_seed, nr, nc, density, dup):
+    rng = np.random.default_rng(draw_seed)
+    nz = int(nr * nc * density)
+    ia = rng.integers(1, nr + 1, nz)
+    ja = rng.integers(1, nc + 1, nz)
+    if dup and nz:  # repeat some entries: coo_fix adds them
+        k = rng.integers(0, nz, max(1, nz // 5))
+        ia, ja = np.concatenate([ia, ia[k]]), np.concatenate([ja, ja[k]])
+    val = rng.standard_normal(len(ia))
+    return ia, ja, val
+
+
+def test_random_matrices_formats_agree():
+    """Seeded random matrices (rectangular, empty rows, duplicate entries,
+    hack sizes 1 .. 64): after psb_d_fix_coo every format's csmv gives the
+    CSR csmv's bits, and the HLL layout keeps the reference's invariants --
+    hack width = its longest row, padding value 0 repeating the row's last
+    column (the hack's first COO column for an empty row), idiag = 1-based
+    diagonal position where the row has one."""
+    for seed in range(40):
+        rng = np.random.default_rng(1000 + seed)
+        nr, nc = int(rng.integers(1, 90)), int(rng.integers(1, 90))
+        ia, ja, val = _random_coo(seed, nr, nc, float(rng.uniform(0.0, 0.3)), bool(seed % 2))
+        ia, ja, val = O.coo_fix(nr, ia, ja, val)
+        assert np.all(np.diff(ia.astype(np.int64) * (nc + 1) + ja) > 0)  # sorted, no duplicates left
+        irp, cja, cval = O.csr_from_coo(nr, ia, ja, val)
+        x, y0 = rng.uniform(-1, 1, nc), rng.uniform(-1, 1, nr)
+        a, b = float(rng.choice([1.0, -1.0, 2.5])), float(rng.choice([0.0, 1.0, -0.5]))
+        yc = O.csr_csmv(irp, cja, cval, a, x, b, y0, nc=nc)
+        lens = np.diff(irp)
+        for hksz in (1, 4, 32, 64):
+            h = O.hll_from_coo(nr, ia, ja, val, hksz)
+            assert np.array_equal(h["irn"], lens)
+            assert np.array_equal(O.hll_csmv(h, nr, a, x, b, y0, nc=nc), yc), (seed, hksz)
+            for k in range(len(h["hkoffs"]) - 1):
+                rows = np.arange(k * hksz, min(nr, (k + 1) * hksz))
+                w = (h["hkoffs"][k + 1] - h["hkoffs"][k]) // hksz
+                assert w == (lens[rows].max() if len(rows) else 0)
+                blk_j = h["ja"][h["hkoffs"][k]:h["hkoffs"][k + 1]].reshape(w, hksz)
+                blk_v = h["val"][h["hkoffs"][k]:h["hkoffs"][k + 1]].reshape(w, hksz)
+                for li, r in enumerate(rows):
+                    n_r = lens[r]
+                    row_j = cja[irp[r] - 1:irp[r + 1] - 1]
+                    assert np.array_equal(blk_j[:n_r, li], row_j)
+                    assert np.all(blk_v[n_r:, li] == 0.0)
+                    if n_r:
+                        assert np.all(blk_j[n_r:, li] == row_j[-1])
+                    d = np.nonzero(row_j == r + 1)[0]
+                    if len(d):
+                        assert h["idiag"][r] == d[0] + 1
+        e = O.ell_from_coo(nr, ia, ja, val)
+        assert np.array_equal(O.ell_csmv(e, nr, a, x, b, y0, nc=nc), yc), seed
