@@ -661,3 +661,31 @@ def test_device_build_random_matrices(psb):
             A.spmv(-1.5, X, 0.5, Y)
             assert np.array_equal(Y.get_vect(), want), (seed, hksz)
             A.free()
+
+
+def test_random_matrices_ell_csr_products(psb):
+    """Seeded random rectangular matrices with empty rows: the ELL (host
+    arrays of the CPU converter) and CSR device products give the CPU csmv's
+    bits; CSR rows longer than a block (none here) would be the only
+    tolerance case."""
+    for seed in range(12):
+        rng = np.random.default_rng(3000 + seed)
+        nr, nc = int(rng.integers(1, 400)), int(rng.integers(1, 400))
+        nz = max(1, int(nr * nc * float(rng.uniform(0.0, 0.08))))
+        ia, ja, va = O.coo_fix(nr, rng.integers(1, nr + 1, nz), rng.integers(1, nc + 1, nz), rng.standard_normal(nz))
+        irp, cja, cva = O.csr_from_coo(nr, ia, ja, va)
+        x, y0 = rng.uniform(-1, 1, nc), rng.uniform(-1, 1, nr)
+        for a, b in ((1.0, 0.0), (-1.5, 0.5)):
+            want = O.csr_csmv(irp, cja, cva, a, x, b, y0, nc=nc)
+            Cm = psb.CsrMat(nr, irp, cja, cva, cols=nc)
+            X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+            Cm.spmv(a, X, b, Y)
+            assert np.array_equal(Y.get_vect(), want), (seed, "csr", a, b)
+            Cm.free()
+            e = O.ell_from_coo(nr, ia, ja, va)
+            E = psb.EllMat.from_host_ell(nr, e["nzm"], e["irn"], e["ja"], e["val"], e["idiag"], e["ldv"],
+                                         nnz=len(cja))
+            X, Y = psb.DVect.bld(x), psb.DVect.bld(y0)
+            E.spmv(a, X, b, Y)
+            assert np.array_equal(Y.get_vect(), want), (seed, "ell", a, b)
+            E.free()
