@@ -249,3 +249,35 @@ def test_repeated_solves_replay_kept_graph(psb, method):
     it_a, err_a = psb.psb_krylov(method, A, P, B, X, eps=1e-10, itmax=2000)
     it_b, err_b = psb.psb_krylov(method, A, P, B, X2, eps=1e-10, itmax=2000)
     assert (it_a, err_a) == (it_b, err_b) and np.array_equal(X.get_vect(), X2.get_vect())
+
+
+@pytest.mark.parametrize("fmt", ["HLL", "ELL", "CSR"])
+def test_random_systems_cg_bicgstab(psb, fmt):
+    """Seeded random diagonally dominant systems (rows of 0 .. 12 random
+    off-diagonal entries, the diagonal their absolute sum plus 1): CG on the
+    symmetric ones (A + A^T), BiCGSTAB on the nonsymmetric ones, DIAG: the
+    device solver and the oracle reach the tolerance within +-2 iterations
+    and agree on x."""
+    for seed in range(4):
+        rng = np.random.default_rng(4000 + seed)
+        n = int(rng.integers(200, 3000))
+        k = rng.integers(0, 13, n)
+        ia = np.repeat(np.arange(1, n + 1), k)
+        ja = rng.integers(1, n + 1, len(ia))
+        va = rng.standard_normal(len(ia))
+        for sym, method in ((True, "CG"), (False, "BICGSTAB")):
+            ii, jj, vv = (np.concatenate([ia, ja]), np.concatenate([ja, ia]), np.concatenate([va, va])) if sym \
+                else (ia, ja, va)
+            keep = ii != jj
+            ii, jj, vv = ii[keep], jj[keep], vv[keep]
+            absum = np.bincount(ii - 1, weights=np.abs(vv), minlength=n)
+            ii = np.concatenate([ii, np.arange(1, n + 1)])
+            jj = np.concatenate([jj, np.arange(1, n + 1)])
+            vv = np.concatenate([vv, absum + 1.0])
+            fi, fj, fv = O.coo_fix(n, ii, jj, vv)
+            irp, cja, cva = O.csr_from_coo(n, fi, fj, fv)
+            b = rng.uniform(-1, 1, n)
+            (x, it, err), (xo, ito, erro) = _solve_both(psb, method, irp, cja, cva, b, fmt=fmt, eps=1e-9)
+            assert abs(it - ito) <= 2, (seed, method, it, ito)
+            assert err <= 1e-9 and erro <= 1e-9
+            assert np.max(np.abs(x - xo)) <= 1e-7 * max(1.0, np.max(np.abs(xo)))
