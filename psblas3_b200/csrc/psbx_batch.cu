@@ -1172,9 +1172,16 @@ int psbx_batch_add(void *eng, void *hllMat, const double *d_b, double *d_x, cons
   Eng *e = (Eng *)eng;
   HllDevice *m = (HllDevice *)hllMat;
   if (!e || !m || !d_b || !d_x || !slot) return SPGPU_UNSUPPORTED;
-  if (m->elemType != SPGPU_TYPE_DOUBLE || m->hackSize != 32 || m->perm || m->baseIndex != 1) return SPGPU_UNSUPPORTED;
+  if (m->elemType != SPGPU_TYPE_DOUBLE || m->hackSize != 32 || m->perm || m->baseIndex != 1) {
+    psbx_set_error("psbx_batch_add: the matrix must be an FP64 HLL of hack size 32, index base 1, "
+                   "without a row permutation");
+    return SPGPU_UNSUPPORTED;
+  }
   // rows of 8 right-hand sides move as 16-byte vectors
-  if (e->K > 1 && (((uintptr_t)d_b | (uintptr_t)d_x) & 15)) return SPGPU_UNSUPPORTED;
+  if (e->K > 1 && (((uintptr_t)d_b | (uintptr_t)d_x) & 15)) {
+    psbx_set_error("psbx_batch_add: with several right-hand sides b and x must be 16-byte aligned");
+    return SPGPU_UNSUPPORTED;
+  }
   if (!m->cM32) {
     int rc = psbx_hll_make_single(m);
     if (rc) return rc;

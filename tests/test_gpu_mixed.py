@@ -97,3 +97,52 @@ def test_mixed_cg_itmax_and_errors(psb):
     assert abs(_true_rel_res(irp, ja, va, b, X.get_vect()) - err) <= 1e-12
     with pytest.raises(PsbxError):
         psb.psb_mixed_cg(A, P, psb.DVect.bld(b), X, delta=1.5)
+
+
+def _random_spd(seed):
+    """Symmetric, diagonally dominant: rows of 0 .. 12 random off-diagonal
+    entries mirrored, diagonal = absolute row sum + 1 (1-based CSR)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(500, 5000))
+    k = rng.integers(0, 13, n)
+    ia = np.repeat(np.arange(1, n + 1), k)
+    ja = rng.integers(1, n + 1, len(ia))
+    va = rng.standard_normal(len(ia))
+    ii, jj, vv = np.concatenate([ia, ja]), np.concatenate([ja, ia]), np.concatenate([va, va])
+    keep = ii != jj
+    ii, jj, vv = ii[keep], jj[keep], vv[keep]
+    absum = np.bincount(ii - 1, weights=np.abs(vv), minlength=n)
+    ii = np.concatenate([ii, np.arange(1, n + 1)])
+    jj = np.concatenate([jj, np.arange(1, n + 1)])
+    vv = np.concatenate([vv, absum + 1.0])
+    fi, fj, fv = O.coo_fix(n, ii, jj, vv)
+    return O.csr_from_coo(n, fi, fj, fv)
+
+
+def test_mixed_cg_random_systems(psb):
+    """Seeded random SPD systems, in stored order and with the rows in length
+    order (permuted layout): the mixed solve reaches ||b - Ax|| <= 1e-10 ||b||
+    (checked in FP64 on the host) and the batch engine (stored order; it
+    takes no permuted layout), one and eight right-hand sides, does too."""
+    import torch
+    for seed in range(4):
+        irp, ja, va = _random_spd(5000 + seed)
+        for perm in (True, False):  # the engine takes the stored order (the last one)
+            n, A, P, b = _setup(psb, irp, ja, va, seed=seed, perm=perm)
+            B, X = psb.DVect.bld(b), psb.DVect(n)
+            it, err, nref = psb.psb_mixed_cg(A, P, B, X, eps=1e-10, itmax=5000)
+            assert err <= 1e-10 and _true_rel_res(irp, ja, va, b, X.get_vect()) <= 1.01e-10, (seed, perm)
+        A.make_single()
+        for k in (1, 8):
+            rhs = np.random.default_rng(seed).uniform(-1, 1, (n, k))
+            db = torch.from_numpy(np.ascontiguousarray(rhs.reshape(-1))).cuda()
+            dx = torch.zeros_like(db)
+            eng = psb.BatchSolver(1, n, k)
+            s = eng.add(A, db, dx, P.dv.data_ptr, eps=1e-10)
+            eng.run()
+            st, outer, its, errs = eng.poll(s)
+            x = dx.cpu().numpy().reshape(n, k)
+            assert st == 1, (seed, k, st)
+            for j in range(k):
+                assert _true_rel_res(irp, ja, va, rhs[:, j], x[:, j]) <= 1.01e-10, (seed, k, j)
+            eng.free()
