@@ -866,6 +866,7 @@ def c5_serving(psb, gen, rate=2000.0, window=60.0, pool_each=16, seed=0, replays
 def run_ours(args):
     world, rank, local = dist_setup()
     import torch
+    local = local_device(local)
     torch.cuda.set_device(local)
     from psblas3_b200 import gen, psb
     from psblas3_b200._lib import check, lib
